@@ -1,0 +1,381 @@
+#!/usr/bin/env python3
+"""Benchmark: BFV homomorphic-multiplication kernel chain on B200.
+
+Workload (one step): a batch of P ciphertext pairs at nphi = 8192, |Q| = 5,
+|B| = 6, t = 256 -- basis extension Q -> Q u B of the four input polynomials,
+DGT tensor product (3 outputs), HPS t/Q scale-and-round back to Q.  Inputs
+and outputs are in the DGT domain (cuPoly's poly_t state RNSSTATE).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One JSON line is printed by rank 0.  `value` is whole-job hom-mul/s with the
+inputs resident in HBM (batched form, device-timed, max over ranks);
+`e2e` repeats it through the C ABI with pinned host buffers and the
+host<->device copies inside the timed region; `plain` is the per-call form
+(one cp_bfv_mul per pair); `polymul` is the batched DGT polymul/s of the
+nphi = 4096, k = 2 configuration.  With --impl reference the C oracle (the
+CPU restatement of the reference path; cuPoly itself cannot be built here) is
+timed on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NPHI, K_Q, K_B, T_PLAIN = 8192, 5, 6, 256
+WORKLOAD = "BFV homomorphic-multiply kernel chain (nphi=8192, k=5, kl=6, t=256)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=128, help="ciphertext pairs per step (batched form)")
+    ap.add_argument("--plain-pairs", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only: no collective on the data path)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._th = threading.Thread(target=self._run, daemon=True)
+        self._th.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and
+                          s[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (the oracle's C restatement of the reference path)
+# ---------------------------------------------------------------------------
+def cpu_bfv_rate(budget_s: float, pairs_per_call: int = 4):
+    import numpy as np
+
+    from oracle import coracle, pyoracle
+    from tests.common import random_poly_residues
+
+    Q, B = pyoracle.bases(K_Q, K_B)
+    rows = [np.stack([random_poly_residues(31 + 4 * i + j, Q, NPHI) for i in range(pairs_per_call)])
+            for j in range(4)]
+    coracle.bfv_mul(*[r[:1] for r in rows], Q, B, T_PLAIN)  # warm-up
+    done, t0 = 0, time.perf_counter()
+    while True:
+        coracle.bfv_mul(*rows, Q, B, T_PLAIN)
+        done += pairs_per_call
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    return done / el, done, el, coracle.num_threads()
+
+
+def run_reference(args, D: Dist):
+    """--impl reference: the CPU restatement timed on the host cores, rank 0 only."""
+    if D.rank != 0:
+        return
+    from oracle import coracle
+
+    coracle.lib()
+    cores = coracle.num_threads()
+    per_step = 4
+    import numpy as np
+
+    from oracle import pyoracle
+    from tests.common import random_poly_residues
+
+    Q, B = pyoracle.bases(K_Q, K_B)
+    rows = [np.stack([random_poly_residues(31 + 4 * i + j, Q, NPHI) for i in range(per_step)]) for j in range(4)]
+    for _ in range(args.warmup):
+        coracle.bfv_mul(*rows, Q, B, T_PLAIN)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        coracle.bfv_mul(*rows, Q, B, T_PLAIN)
+    el = time.perf_counter() - t0
+    v = per_step * args.steps / el
+    line = {
+        "impl": "reference", "metric": "BFV mul/s", "value": round(v, 3), "unit": "hom-mul/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el * 1e3 / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs_per_step": per_step, "nphi": NPHI, "k": K_Q, "kl": K_B,
+                   "t": T_PLAIN},
+        "cpu_baseline": {"value": round(v, 3), "unit": "hom-mul/s", "cores": cores, "kind": "port",
+                         "sample": "%d pairs per step, C restatement (oracle/cpoly_oracle.c), OpenMP" % per_step},
+        "e2e": {"value": round(v, 3), "unit": "hom-mul/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "cuPoly needs NTL/GMP/gtest and cannot be built here; the oracle's C port of its path is timed",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, D: Dist):
+    import torch
+
+    from cupoly_b200.engine import FORWARD, QBase, UNIFORM, Engine
+
+    torch.cuda.set_device(D.local)
+    dev_index = D.local
+    e = Engine(K_Q, K_B, NPHI, T_PLAIN)
+    P = args.pairs
+    seed = 0xC0FFEE + 1000003 * D.rank
+    ins = []
+    for j in range(4):
+        x = e.empty(QBase, P)
+        e.sample(x, QBase, UNIFORM, seed, 4096 * j, npolys=P, to_dgt=True)
+        ins.append(x)
+    c = e.empty(QBase, 3 * P)
+    ws = e.bfv_mul_batch_workspace(P)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+
+    def step():
+        e.bfv_mul_batch(c, *ins, P, ws)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev_index) as clk:
+        D.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        D.barrier()
+    ms = D.max(ev0.elapsed_time(ev1))
+    value = D.world * P * args.steps / (ms / 1e3)
+    launches_per_step = 10  # 5 DGT + 2 base conversions + 2 tensor + 1 scaling (nphi <= 16384)
+
+    # ---- e2e: C ABI with pinned host buffers, copies inside the timed region ----
+    hin = [torch.empty_like(x, device="cpu").pin_memory() for x in ins]
+    for h, x in zip(hin, ins):
+        h.copy_(x)
+    hout = torch.empty_like(c, device="cpu").pin_memory()
+    din = [torch.empty_like(x) for x in ins]
+
+    def e2e_step():
+        for d, h in zip(din, hin):
+            d.copy_(h, non_blocking=True)
+        e.bfv_mul_batch(c, *din, P, ws)
+        hout.copy_(c, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    D.barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = D.max(ev0.elapsed_time(ev1))
+    h2d = sum(h.numel() * 8 for h in hin)
+    d2h = hout.numel() * 8
+
+    # ---- plain per-call form: one cp_bfv_mul per pair ----
+    PP = min(args.plain_pairs, P)
+    outs = [e.empty(QBase) for _ in range(3)]
+
+    def plain_step():
+        for i in range(PP):
+            e.bfv_mul(*outs, *[x[i:i + 1] for x in ins])
+
+    plain_step()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    plain_steps = max(1, args.steps // 4)
+    for _ in range(plain_steps):
+        plain_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = ev0.elapsed_time(ev1)
+    plain_value = PP * plain_steps / (plain_ms / 1e3)
+
+    # ---- dominant kernel: forward DGT over the step's 4P x |B| residues ----
+    import json as _json
+    peaks = {}
+    try:
+        peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    xb = e.empty(1, 4 * P)
+    xb.zero_()
+    reps = 20
+    e.dgt(xb, 1, FORWARD)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(reps):
+        e.dgt(xb, 1, FORWARD)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    dgt_ms = ev0.elapsed_time(ev1) / reps
+    dgt_bytes = 2 * 16 * e.N * 4 * P * K_B  # read + write every Gaussian element once
+    achieved = dgt_bytes / (dgt_ms / 1e3) / 1e9
+
+    # ---- polymul/s of the nphi = 4096, k = 2 configuration (batched) ----
+    e1 = Engine(2, 3, 4096, 256)
+    NPm = 1024
+    pa, pb, pc = e1.empty(QBase, NPm), e1.empty(QBase, NPm), e1.empty(QBase, NPm)
+    e1.sample(pa, QBase, UNIFORM, seed, 1, npolys=NPm, to_dgt=False)
+    e1.sample(pb, QBase, UNIFORM, seed, 2 + NPm, npolys=NPm, to_dgt=False)
+    from cupoly_b200.engine import INVERSE
+
+    ta, tb = torch.empty_like(pa), torch.empty_like(pb)
+
+    def polymul_step():  # coefficient domain in and out: 3 transforms + pointwise
+        ta.copy_(pa)
+        tb.copy_(pb)
+        e1.dgt(ta, QBase, FORWARD)
+        e1.dgt(tb, QBase, FORWARD)
+        e1.mul_batch(pc, ta, tb, QBase)
+        e1.dgt(pc, QBase, INVERSE)
+
+    polymul_step()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(5):
+        polymul_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    polymul_value = NPm * 5 / (ev0.elapsed_time(ev1) / 1e3)
+
+    cpu = None
+    if D.rank == 0 and not args.no_cpu_baseline:
+        rate, done, el, cores = cpu_bfv_rate(10.0)
+        cpu = {"value": round(rate, 3), "unit": "hom-mul/s", "cores": cores, "kind": "port",
+               "sample": "%d pairs in %.1f s (nphi=8192, k=5) through oracle/cpoly_oracle.c, OpenMP" % (done, el)}
+
+    if D.rank == 0:
+        line = {
+            "metric": "BFV mul/s", "value": round(value, 2), "unit": "hom-mul/s", "n_gpus": D.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded uniform residues mod q_i (Philox), DGT domain",
+            "config": {"workload": WORKLOAD + ", batched form", "pairs_per_step": P, "nphi": NPHI, "k": K_Q,
+                       "kl": K_B, "t": T_PLAIN, "parallelism": "replicas x%d" % D.world,
+                       "l2": "inputs larger than L2 (%.0f MB read per step)" % (4 * P * K_Q * e.N * 16 / 1e6)},
+            "e2e": {"value": round(D.world * P * args.steps / (e2e_ms / 1e3), 2), "unit": "hom-mul/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "plain": {"value": round(plain_value, 2), "unit": "hom-mul/s",
+                      "form": "one cp_bfv_mul call per pair (cuPoly's per-call composition)", "pairs": PP},
+            "batched_over_plain": round(value / D.world / plain_value, 2),
+            "polymul": ({"value": round(polymul_value, 1), "unit": "polymul/s",
+                         "config": "nphi=4096, k=2, batch 1024"} if polymul_value else None),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                         "kernel": "k_dgt_fwd (forward DGT, %d residues of N=%d per launch, timed alone)" %
+                                   (4 * P * K_B, e.N),
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback"},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": launches_per_step * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    D = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, D)
+        else:
+            run_ours(args, D)
+    finally:
+        D.close()
+
+
+if __name__ == "__main__":
+    main()

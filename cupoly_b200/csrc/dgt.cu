@@ -1,0 +1,96 @@
+// Host launchers of the DGT kernels (replaces cuPoly's
+// DGTEngine::execute_dgt and its runDGT dispatch, src/cuda/dgt.cu:107-205,
+// 1069-1094).
+#include "dgt_kernels.cuh"
+#include "launch.cuh"
+
+namespace cpoly {
+
+namespace {
+
+template <int LOGNC, int LOGR>
+int run_cta(const Engine& e, ulonglong2* data, int nres, int rid_off, int npolys, long long poly_stride,
+            bool inverse, bool twist, cudaStream_t st) {
+  constexpr int T = (1 << LOGNC) >> LOGR;
+  constexpr int smem = dgt_smem_bytes<LOGNC, LOGR>();
+  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc};
+  const int S = e.plan.S;
+  const long long blocks = (long long)npolys * nres << S;
+  if (blocks <= 0) return 0;
+  if (blocks > 0x7fffffffLL) {
+    set_error("dgt: grid too large");
+    return 1;
+  }
+  if (!inverse) {
+    static std::atomic<unsigned long long> done{0};
+    if (int rc = ensure_smem(k_dgt_fwd<LOGNC, LOGR>, smem, done)) return rc;
+    k_dgt_fwd<LOGNC, LOGR><<<(unsigned)blocks, T, smem, st>>>(data, A, nres, rid_off, poly_stride, S, twist ? 1 : 0);
+  } else {
+    static std::atomic<unsigned long long> done{0};
+    if (int rc = ensure_smem(k_dgt_inv<LOGNC, LOGR>, smem, done)) return rc;
+    k_dgt_inv<LOGNC, LOGR><<<(unsigned)blocks, T, smem, st>>>(data, A, nres, rid_off, poly_stride, S, twist ? 1 : 0);
+  }
+  return check_launch("dgt");
+}
+
+using RunFn = int (*)(const Engine&, ulonglong2*, int, int, int, long long, bool, bool, cudaStream_t);
+
+// (logNc, effective logR) -> instantiation.
+RunFn pick(int logNc, int logR) {
+#define CP_CASE(A, B) \
+  if (logNc == A && logR == B) return &run_cta<A, B>;
+  CP_CASE(1, 1) CP_CASE(2, 2) CP_CASE(3, 3) CP_CASE(4, 4) CP_CASE(4, 3)
+  CP_CASE(5, 4) CP_CASE(5, 3) CP_CASE(6, 4) CP_CASE(6, 3) CP_CASE(7, 4) CP_CASE(7, 3)
+  CP_CASE(8, 4) CP_CASE(8, 3) CP_CASE(9, 4) CP_CASE(9, 3) CP_CASE(10, 4) CP_CASE(10, 3)
+  CP_CASE(11, 4) CP_CASE(11, 3) CP_CASE(12, 4) CP_CASE(12, 3) CP_CASE(13, 4) CP_CASE(13, 3)
+#undef CP_CASE
+  return nullptr;
+}
+
+}  // namespace
+
+int launch_dgt(const Engine& e, void* data_v, int base, int npolys, long long poly_stride, bool inverse,
+               cudaStream_t st) {
+  if (base == 3) return 0;  // TBase: no transform (cuPoly dgt.cu:1087-1088)
+  const int nres = e.n_residues(base);
+  if (nres < 0) {
+    set_error("dgt: unknown base");
+    return 1;
+  }
+  const int rid_off = e.rid_offset(base);
+  ulonglong2* data = reinterpret_cast<ulonglong2*>(data_v);
+  if (poly_stride == 0) poly_stride = (long long)nres * e.N;
+  RunFn fn = pick(e.plan.logNc, e.plan.logR);
+  if (!fn) {
+    set_error("dgt: no kernel for this size");
+    return 3;
+  }
+  const int S = e.plan.S;
+  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc};
+  const int Nc = 1 << e.plan.logNc;
+  const long long split_blocks = (long long)npolys * nres * (Nc / 256);
+  if (!inverse) {
+    if (S > 0) {
+      if (S == 1)
+        k_dgt_split<1, false><<<(unsigned)split_blocks, 256, 0, st>>>(data, A, nres, rid_off, poly_stride,
+                                                                       e.plan.logNc, e.plan.logR);
+      else
+        k_dgt_split<2, false><<<(unsigned)split_blocks, 256, 0, st>>>(data, A, nres, rid_off, poly_stride,
+                                                                       e.plan.logNc, e.plan.logR);
+      int rc = check_launch("dgt split");
+      if (rc) return rc;
+    }
+    return fn(e, data, nres, rid_off, npolys, poly_stride, false, S == 0, st);
+  }
+  int rc = fn(e, data, nres, rid_off, npolys, poly_stride, true, S == 0, st);
+  if (rc || S == 0) return rc;
+  if (S == 1)
+    k_dgt_split<1, true><<<(unsigned)split_blocks, 256, 0, st>>>(data, A, nres, rid_off, poly_stride, e.plan.logNc,
+                                                                  e.plan.logR);
+  else
+    k_dgt_split<2, true><<<(unsigned)split_blocks, 256, 0, st>>>(data, A, nres, rid_off, poly_stride, e.plan.logNc,
+                                                                  e.plan.logR);
+  return check_launch("dgt split");
+}
+
+}  // namespace cpoly

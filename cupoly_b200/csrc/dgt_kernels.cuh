@@ -1,0 +1,411 @@
+// Discrete Galois transform kernels for sm_100a.
+//
+// Replaces cuPoly's hdgt_tr / hidgt / hidgt_tr / dgt / idgt kernels
+// (cuPoly src/cuda/dgt.cu:681-1067).  The transform computed is the same:
+// forward = twist by xi^n, then the N-point DFT with w_N = g^((p-1)/N),
+// output in bit-reversed order (X[brev(pos)] at pos); inverse = exact
+// inverse including N^-1.  cuPoly's two-pass Na x Nb split produces exactly
+// this order, so the DGT-domain bytes agree for the same xi.
+//
+// Structure (one CTA per residue of one polynomial, N <= 8192 GIs):
+//  * the residue stays in shared memory for the whole transform: one HBM
+//    read and one HBM write per transform (cuPoly: two of each);
+//  * each thread keeps 2^LOGR Gaussian elements in registers and runs a
+//    radix-2^LOGR DIF (inverse: DIT) over one contiguous bit field of the
+//    index per pass; passes exchange through padded shared memory;
+//  * between passes the per-element twiddle w_M^(L brev(pos)) comes from a
+//    per-pass table laid out in access order, so global reads coalesce;
+//  * every constant multiply is a Shoup product with a precomputed quotient.
+// For N > 8192 an element-wise radix-2^S stage (twist + top S bits) runs
+// first (forward) or last (inverse) and the CTA kernel handles the
+// 2^S sub-transforms.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "engine.cuh"
+
+namespace cpoly {
+
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+
+template <int LOGNC, int LOGR>
+struct PassCfg {
+  static constexpr int NP = (LOGNC + LOGR - 1) / LOGR;
+  static constexpr int W0 = LOGNC - (NP - 1) * LOGR;
+  __host__ __device__ static constexpr int width(int i) { return i == 0 ? W0 : LOGR; }
+  __host__ __device__ static constexpr int field(int i) { return LOGNC - W0 - i * LOGR; }
+};
+
+// In-register 2^W-point Gentleman-Sande DIF (natural in, bit-reversed out).
+// rad[j] = w_R^j, R = 2^LOGR; the 2^W-point root is w_R^(2^(LOGR-W)).
+template <int W, int LOGR>
+__device__ __forceinline__ void dif_regs(uint64_t* xr, uint64_t* xi, const ulonglong2* rad, uint64_t p) {
+#pragma unroll
+  for (int s = 0; s < W; ++s) {
+    const int m = (1 << W) >> (s + 1);
+#pragma unroll
+    for (int i = 0; i < (1 << W); ++i) {
+      if ((i & m) == 0) {
+        const int j = i & (m - 1);
+        const uint64_t ar = xr[i], ai = xi[i], br = xr[i + m], bi = xi[i + m];
+        xr[i] = add_mod(ar, br, p);
+        xi[i] = add_mod(ai, bi, p);
+        if (j == 0) {
+          xr[i + m] = sub_mod(ar, br, p);
+          xi[i + m] = sub_mod(ai, bi, p);
+        } else {
+          const ulonglong2 w = rad[(j << s) << (LOGR - W)];
+          xr[i + m] = shoup_mul(ar + p - br, w.x, w.y, p);
+          xi[i + m] = shoup_mul(ai + p - bi, w.x, w.y, p);
+        }
+      }
+    }
+  }
+}
+
+// In-register 2^W-point Cooley-Tukey DIT with inverse roots (bit-reversed in,
+// natural out), unscaled.
+template <int W, int LOGR>
+__device__ __forceinline__ void dit_regs(uint64_t* xr, uint64_t* xi, const ulonglong2* rad, uint64_t p) {
+  constexpr int R = 1 << LOGR;
+#pragma unroll
+  for (int s = W - 1; s >= 0; --s) {
+    const int m = (1 << W) >> (s + 1);
+#pragma unroll
+    for (int i = 0; i < (1 << W); ++i) {
+      if ((i & m) == 0) {
+        const int j = i & (m - 1);
+        const uint64_t ar = xr[i], ai = xi[i];
+        uint64_t br = xr[i + m], bi = xi[i + m];
+        if (j != 0) {
+          const ulonglong2 w = rad[R - ((j << s) << (LOGR - W))];
+          br = shoup_mul(br, w.x, w.y, p);
+          bi = shoup_mul(bi, w.x, w.y, p);
+        }
+        xr[i] = add_mod(ar, br, p);
+        xi[i] = add_mod(ai, bi, p);
+        xr[i + m] = sub_mod(ar, br, p);
+        xi[i + m] = sub_mod(ai, bi, p);
+      }
+    }
+  }
+}
+
+// One middle/late forward pass (I >= 1), full radix 2^LOGR, data in smem.
+template <int LOGNC, int LOGR, int I>
+__device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* tab,
+                                           const DgtTableLayout& L, uint64_t p) {
+  using C = PassCfg<LOGNC, LOGR>;
+  if constexpr (I < C::NP) {
+    constexpr int PF = C::field(I);
+    constexpr int R = 1 << LOGR;
+    const int c = threadIdx.x;
+    const int Lw = c & ((1 << PF) - 1);
+    const int base = ((c >> PF) << (PF + LOGR)) + Lw;
+    uint64_t xr[R], xi[R];
+#pragma unroll
+    for (int v = 0; v < R; ++v) {
+      const ulonglong2 a = sdat[pad16(base + (v << PF))];
+      xr[v] = a.x;
+      xi[v] = a.y;
+    }
+    dif_regs<LOGR, LOGR>(xr, xi, srad, p);
+    if constexpr (PF > 0) {
+      const ulonglong2* tw = tab + L.off_fwd[I] + Lw;
+#pragma unroll
+      for (int v = 1; v < R; ++v) {
+        const ulonglong2 w = __ldg(tw + (v << PF));
+        xr[v] = shoup_mul(xr[v], w.x, w.y, p);
+        xi[v] = shoup_mul(xi[v], w.x, w.y, p);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
+    __syncthreads();
+    fwd_passes<LOGNC, LOGR, I + 1>(sdat, srad, tab, L, p);
+  }
+}
+
+template <int LOGNC, int LOGR, int I>
+__device__ __forceinline__ void inv_passes(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* tab,
+                                           const DgtTableLayout& L, uint64_t p) {
+  using C = PassCfg<LOGNC, LOGR>;
+  if constexpr (I >= 1) {
+    constexpr int PF = C::field(I);
+    constexpr int R = 1 << LOGR;
+    const int c = threadIdx.x;
+    const int Lw = c & ((1 << PF) - 1);
+    const int base = ((c >> PF) << (PF + LOGR)) + Lw;
+    uint64_t xr[R], xi[R];
+#pragma unroll
+    for (int v = 0; v < R; ++v) {
+      const ulonglong2 a = sdat[pad16(base + (v << PF))];
+      xr[v] = a.x;
+      xi[v] = a.y;
+    }
+    if constexpr (PF > 0) {
+      const ulonglong2* tw = tab + L.off_inv[I] + Lw;
+#pragma unroll
+      for (int v = 1; v < R; ++v) {
+        const ulonglong2 w = __ldg(tw + (v << PF));
+        xr[v] = shoup_mul(xr[v], w.x, w.y, p);
+        xi[v] = shoup_mul(xi[v], w.x, w.y, p);
+      }
+    }
+    dit_regs<LOGR, LOGR>(xr, xi, srad, p);
+#pragma unroll
+    for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
+    __syncthreads();
+    inv_passes<LOGNC, LOGR, I - 1>(sdat, srad, tab, L, p);
+  }
+}
+
+// Shared-memory bytes of one CTA.
+template <int LOGNC, int LOGR>
+constexpr int dgt_smem_bytes() {
+  return ((1 << LOGNC) + ((1 << LOGNC) >> 4) + (1 << LOGR)) * 16;
+}
+
+// Forward transform of 2^LOGNC elements per CTA, in place.
+// blockIdx.x = (poly * nres + r) * 2^S + h; element block h of residue r.
+// Occupancy hint: at most 128 registers per thread for the CTA sizes used.
+template <int LOGNC, int LOGR>
+constexpr int dgt_min_blocks() {
+  return (512 >> (LOGNC - LOGR)) > 0 ? ((512 >> (LOGNC - LOGR)) < 32 ? (512 >> (LOGNC - LOGR)) : 32) : 1;
+}
+
+template <int LOGNC, int LOGR>
+__global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
+    k_dgt_fwd(ulonglong2* __restrict__ data, DgtArgs A, int nres, int rid_off, long long poly_stride, int S,
+              int twist) {
+  constexpr int NC = 1 << LOGNC, R = 1 << LOGR, T = NC >> LOGR;
+  using C = PassCfg<LOGNC, LOGR>;
+  extern __shared__ ulonglong2 smem[];
+  ulonglong2* sdat = smem;
+  ulonglong2* srad = smem + NC + (NC >> 4);
+  const int tid = threadIdx.x;
+  const int h = blockIdx.x & ((1 << S) - 1);
+  const int pr = blockIdx.x >> S;
+  const int r = pr % nres;
+  const int poly = pr / nres;
+  const int rid = rid_off + r;
+  const uint64_t p = A.mc[rid].p;
+  const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
+  ulonglong2* x = data + poly * poly_stride + ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
+  for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
+  __syncthreads();
+  {
+    constexpr int W = C::W0, PF = LOGNC - C::W0, G = 1 << (LOGR - C::W0);
+    uint64_t xr[R], xi[R];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const int Lw = tid + g * T;
+#pragma unroll
+      for (int v = 0; v < (1 << W); ++v) {
+        const int idx = Lw + (v << PF);
+        const ulonglong2 a = x[idx];
+        uint64_t ar = a.x, ai = a.y;
+        if (twist) {
+          const ulonglong2 tr = __ldg(tab + A.L.off_twist + 2 * idx);
+          const ulonglong2 ti = __ldg(tab + A.L.off_twist + 2 * idx + 1);
+          gi_mul_const(ar, ai, tr.x, tr.y, ti.x, ti.y, p);
+        }
+        xr[g * (1 << W) + v] = ar;
+        xi[g * (1 << W) + v] = ai;
+      }
+      dif_regs<W, LOGR>(xr + g * (1 << W), xi + g * (1 << W), srad, p);
+      if constexpr (PF > 0) {
+        const ulonglong2* tw = tab + A.L.off_fwd[0] + Lw;
+#pragma unroll
+        for (int v = 1; v < (1 << W); ++v) {
+          const ulonglong2 w = __ldg(tw + (v << PF));
+          xr[g * (1 << W) + v] = shoup_mul(xr[g * (1 << W) + v], w.x, w.y, p);
+          xi[g * (1 << W) + v] = shoup_mul(xi[g * (1 << W) + v], w.x, w.y, p);
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < (1 << W); ++v)
+        sdat[pad16(Lw + (v << PF))] = make_ulonglong2(xr[g * (1 << W) + v], xi[g * (1 << W) + v]);
+    }
+    __syncthreads();
+  }
+  fwd_passes<LOGNC, LOGR, 1>(sdat, srad, tab, A.L, p);
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const int idx = tid + j * T;
+    x[idx] = sdat[pad16(idx)];
+  }
+}
+
+// Inverse transform of 2^LOGNC elements per CTA, in place; untwist (with
+// N^-1) applied when `untwist` is set (S == 0).
+template <int LOGNC, int LOGR>
+__global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
+    k_dgt_inv(ulonglong2* __restrict__ data, DgtArgs A, int nres, int rid_off, long long poly_stride, int S,
+              int untwist) {
+  constexpr int NC = 1 << LOGNC, R = 1 << LOGR, T = NC >> LOGR;
+  using C = PassCfg<LOGNC, LOGR>;
+  extern __shared__ ulonglong2 smem[];
+  ulonglong2* sdat = smem;
+  ulonglong2* srad = smem + NC + (NC >> 4);
+  const int tid = threadIdx.x;
+  const int h = blockIdx.x & ((1 << S) - 1);
+  const int pr = blockIdx.x >> S;
+  const int r = pr % nres;
+  const int poly = pr / nres;
+  const int rid = rid_off + r;
+  const uint64_t p = A.mc[rid].p;
+  const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
+  ulonglong2* x = data + poly * poly_stride + ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
+  for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const int idx = tid + j * T;
+    sdat[pad16(idx)] = x[idx];
+  }
+  __syncthreads();
+  inv_passes<LOGNC, LOGR, C::NP - 1>(sdat, srad, tab, A.L, p);
+  {
+    constexpr int W = C::W0, PF = LOGNC - C::W0, G = 1 << (LOGR - C::W0);
+    uint64_t xr[1 << W], xi[1 << W];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const int Lw = tid + g * T;
+#pragma unroll
+      for (int v = 0; v < (1 << W); ++v) {
+        const ulonglong2 a = sdat[pad16(Lw + (v << PF))];
+        xr[v] = a.x;
+        xi[v] = a.y;
+      }
+      if constexpr (PF > 0) {
+        const ulonglong2* tw = tab + A.L.off_inv[0] + Lw;
+#pragma unroll
+        for (int v = 1; v < (1 << W); ++v) {
+          const ulonglong2 w = __ldg(tw + (v << PF));
+          xr[v] = shoup_mul(xr[v], w.x, w.y, p);
+          xi[v] = shoup_mul(xi[v], w.x, w.y, p);
+        }
+      }
+      dit_regs<W, LOGR>(xr, xi, srad, p);
+#pragma unroll
+      for (int v = 0; v < (1 << W); ++v) {
+        const int idx = Lw + (v << PF);
+        uint64_t ar = xr[v], ai = xi[v];
+        if (untwist) {
+          const ulonglong2 tr = __ldg(tab + A.L.off_untwist + 2 * idx);
+          const ulonglong2 ti = __ldg(tab + A.L.off_untwist + 2 * idx + 1);
+          gi_mul_const(ar, ai, tr.x, tr.y, ti.x, ti.y, p);
+        }
+        x[idx] = make_ulonglong2(ar, ai);
+      }
+    }
+  }
+}
+
+// Element-wise top stage for N = 2^S * Nc (forward: twist + radix-2^S DIF
+// over the top S bits + twiddle; inverse: twiddle + radix-2^S DIT + untwist).
+template <int S, bool INV>
+__global__ void __launch_bounds__(256)
+    k_dgt_split(ulonglong2* __restrict__ data, DgtArgs A, int nres, int rid_off, long long poly_stride, int logNc,
+                int logR) {
+  const int Nc = 1 << logNc;
+  const int chunks = Nc / 256;
+  const int pr = blockIdx.x / chunks;
+  const int Lw = (blockIdx.x % chunks) * 256 + threadIdx.x;
+  const int r = pr % nres;
+  const int poly = pr / nres;
+  const int rid = rid_off + r;
+  const uint64_t p = A.mc[rid].p;
+  const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
+  ulonglong2* x = data + poly * poly_stride + ((size_t)r << (logNc + S));
+  constexpr int K = 1 << S;
+  uint64_t xr[K], xi[K];
+  const int R = 1 << logR;
+  if (!INV) {
+#pragma unroll
+    for (int hh = 0; hh < K; ++hh) {
+      const int n = Lw + hh * Nc;
+      const ulonglong2 a = x[n];
+      uint64_t ar = a.x, ai = a.y;
+      const ulonglong2 tr = __ldg(tab + A.L.off_twist + 2 * n);
+      const ulonglong2 ti = __ldg(tab + A.L.off_twist + 2 * n + 1);
+      gi_mul_const(ar, ai, tr.x, tr.y, ti.x, ti.y, p);
+      xr[hh] = ar;
+      xi[hh] = ai;
+    }
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int m = K >> (s + 1);
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if ((i & m) == 0) {
+          const int j = i & (m - 1);
+          const uint64_t ar = xr[i], ai = xi[i], br = xr[i + m], bi = xi[i + m];
+          xr[i] = add_mod(ar, br, p);
+          xi[i] = add_mod(ai, bi, p);
+          if (j == 0) {
+            xr[i + m] = sub_mod(ar, br, p);
+            xi[i + m] = sub_mod(ai, bi, p);
+          } else {
+            const ulonglong2 w = __ldg(tab + A.L.off_rad + ((j << s) * (R >> S)));
+            xr[i + m] = shoup_mul(ar + p - br, w.x, w.y, p);
+            xi[i + m] = shoup_mul(ai + p - bi, w.x, w.y, p);
+          }
+        }
+    }
+#pragma unroll
+    for (int pos = 0; pos < K; ++pos) {
+      uint64_t ar = xr[pos], ai = xi[pos];
+      if (pos) {
+        const ulonglong2 w = __ldg(tab + A.L.off_split_fwd + pos * Nc + Lw);
+        ar = shoup_mul(ar, w.x, w.y, p);
+        ai = shoup_mul(ai, w.x, w.y, p);
+      }
+      x[Lw + pos * Nc] = make_ulonglong2(ar, ai);
+    }
+  } else {
+#pragma unroll
+    for (int pos = 0; pos < K; ++pos) {
+      const ulonglong2 a = x[Lw + pos * Nc];
+      uint64_t ar = a.x, ai = a.y;
+      if (pos) {
+        const ulonglong2 w = __ldg(tab + A.L.off_split_inv + pos * Nc + Lw);
+        ar = shoup_mul(ar, w.x, w.y, p);
+        ai = shoup_mul(ai, w.x, w.y, p);
+      }
+      xr[pos] = ar;
+      xi[pos] = ai;
+    }
+#pragma unroll
+    for (int s = S - 1; s >= 0; --s) {
+      const int m = K >> (s + 1);
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if ((i & m) == 0) {
+          const int j = i & (m - 1);
+          const uint64_t ar = xr[i], ai = xi[i];
+          uint64_t br = xr[i + m], bi = xi[i + m];
+          if (j != 0) {
+            const ulonglong2 w = __ldg(tab + A.L.off_rad + R - ((j << s) * (R >> S)));
+            br = shoup_mul(br, w.x, w.y, p);
+            bi = shoup_mul(bi, w.x, w.y, p);
+          }
+          xr[i] = add_mod(ar, br, p);
+          xi[i] = add_mod(ai, bi, p);
+          xr[i + m] = sub_mod(ar, br, p);
+          xi[i + m] = sub_mod(ai, bi, p);
+        }
+    }
+#pragma unroll
+    for (int hh = 0; hh < K; ++hh) {
+      const int n = Lw + hh * Nc;
+      uint64_t ar = xr[hh], ai = xi[hh];
+      const ulonglong2 tr = __ldg(tab + A.L.off_untwist + 2 * n);
+      const ulonglong2 ti = __ldg(tab + A.L.off_untwist + 2 * n + 1);
+      gi_mul_const(ar, ai, tr.x, tr.y, ti.x, ti.y, p);
+      x[n] = make_ulonglong2(ar, ai);
+    }
+  }
+}
+
+}  // namespace cpoly

@@ -1,0 +1,118 @@
+// Internal engine state: parameters and device-resident tables of one
+// (nphi, k, kl, t) instance.
+//
+// Replaces cuPoly's process-wide singletons CUDAEngine / DGTEngine and their
+// __constant__ tables (cuPoly src/cuda/cudaengine.cu:22-101,
+// src/cuda/dgt.cu:20-33, precompute :1337-1673 and dgt.cu:1694-1982).  Each
+// engine owns its own tables, so any number of parameter sets coexist.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "modarith.cuh"
+
+namespace cpoly {
+
+constexpr int kMaxLogNc = 13;   // largest transform kept whole in one CTA (8192 GIs, 136 KB smem)
+constexpr int kMaxPasses = 8;
+constexpr int kMaxResidues = 96; // |Q| + |B| limit of one engine
+
+// Radix plan of the in-CTA transform of size 2^logNc.  Passes run from the
+// top index bits down; pass i covers bits [p[i], p[i] + w[i]).
+struct DgtPlan {
+  int logN = 0;     // full transform size (N = nphi / 2)
+  int logNc = 0;    // size handled inside one CTA
+  int S = 0;        // split bits handled by the element-wise split stage
+  int logR = 0;     // register radix
+  int npass = 0;
+  int w[kMaxPasses] = {0};
+  int p[kMaxPasses] = {0};
+};
+
+DgtPlan make_plan(int logN, int logR);
+
+// Offsets (in 16-byte entries) inside one residue's table block.
+struct DgtTableLayout {
+  int off_rad = 0;                      // R entries: w_R^j (w, w')
+  int off_fwd[kMaxPasses] = {0};        // per pass: 2^(p+w) entries
+  int off_inv[kMaxPasses] = {0};
+  int off_split_fwd = 0;                // N entries (only if S > 0)
+  int off_split_inv = 0;
+  int off_twist = 0;                    // 2N entries: (xr, xr'), (xi, xi')
+  int off_untwist = 0;                  // 2N entries, includes N^-1
+  int stride = 0;                       // entries per residue block
+};
+
+// Arguments of the DGT kernels (passed by value).
+struct DgtArgs {
+  const ulonglong2* tab;   // table block of residue 0 of the engine
+  int stride;              // entries per residue block
+  DgtTableLayout L;
+  const ModConst* mc;      // per engine residue
+};
+
+// Mixed-radix conversion constants of one (source base -> targets) pair.
+// Source base: n primes s_0..s_{n-1}; targets: K moduli m_0..m_{K-1}.
+struct MrcTables {
+  int n = 0, K = 0;
+  // inv[i*(i-1)/2 + l] = s_l^-1 mod s_i (and companion), l < i
+  std::vector<uint64_t> inv, inv_s;
+  // horner[j*n + i] = s_i mod m_j (and companion), i < n - 1
+  std::vector<uint64_t> hor, hor_s;
+  // digits of (prod(s) - 1) / 2, for the centred lift
+  std::vector<uint64_t> half_digits;
+  // prod(s) mod m_j (and companion)
+  std::vector<uint64_t> P_mod, P_mod_s;
+};
+
+struct Engine {
+  int device = 0;
+  int nphi = 0, N = 0, logN = 0;
+  int k = 0, kl = 0;
+  uint64_t t = 0;
+  std::vector<uint64_t> primes;   // Q then B
+  std::vector<ModConst> mconst;
+  std::vector<std::pair<uint64_t, uint64_t>> xi;  // Gaussian root of i used for the twist, per residue
+  DgtPlan plan;
+  DgtTableLayout layout;
+
+  // device allocations
+  ModConst* d_mc = nullptr;
+  ulonglong2* d_tab = nullptr;     // (k + kl) residue blocks
+  uint64_t* d_hps = nullptr;       // packed HPS/MRC constants
+  size_t hps_words = 0;
+  // word offsets inside d_hps
+  struct HpsOffsets {
+    int qb_inv, qb_inv_s, qb_hor, qb_hor_s, qb_half;           // Q -> B
+    int bq_inv, bq_inv_s, bq_hor, bq_hor_s;                    // B -> Q
+    int qt_hor, qt_hor_s;                                      // Q -> t
+    int q_mod_b, q_mod_b_s;        // Q mod b_j
+    int qinv_b, qinv_b_s;          // Q^-1 mod b_j
+    int t_q, t_q_s;                // t mod q_i
+    int t_b, t_b_s;                // t mod b_j
+    int q_mod_t, q_mod_t_s;        // Q mod t
+    int qinv_t, qinv_t_s;          // Q^-1 mod t
+    int xi_q, xi_q_s;              // (Q/q_i)^-1 mod q_i
+    int rho_q, rho_q_s;            // (Q/q_i) mod q_i
+  } ho{};
+  uint64_t t_shoup_one = 0;        // floor(2^64 / t)
+  uint64_t h_q_mod_t = 0, h_qinv_t = 0, h_qinv_t_s = 0;  // Q mod t, Q^-1 mod t
+  int* d_err = nullptr;            // device-side error flag (sampler rejection exhaustion)
+
+  int n_residues(int base) const;
+  int rid_offset(int base) const;
+};
+
+// thread-local error reporting
+void set_error(const std::string& msg);
+const char* last_error();
+
+// table construction (tables.cu)
+int build_tables(Engine& e);
+void free_tables(Engine& e);
+
+}  // namespace cpoly

@@ -1,0 +1,51 @@
+// Launch helpers shared by the kernel files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <string>
+
+#include "engine.cuh"
+
+namespace cpoly {
+
+// Status codes of the C ABI (mirrored in include/cupoly_b200.h).
+enum : int {
+  CP_OK_ = 0,
+  CP_ERR_INVALID_ = 1,
+  CP_ERR_CUDA_ = 2,
+  CP_ERR_UNSUPPORTED_ = 3,
+  CP_ERR_OOM_ = 4,
+  CP_ERR_TIMEOUT_ = 5,
+};
+
+inline int cuda_fail(const char* what, cudaError_t err = cudaGetLastError()) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(err));
+  return CP_ERR_CUDA_;
+}
+
+inline int check_launch(const char* what) {
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(what, err);
+  return CP_OK_;
+}
+
+// Raise a kernel's dynamic shared-memory limit once per device.
+template <typename K>
+inline int ensure_smem(K kernel, int bytes, std::atomic<unsigned long long>& done_mask) {
+  if (bytes <= 48 * 1024) return CP_OK_;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ULL << (dev & 63);
+  if (done_mask.load() & bit) return CP_OK_;
+  cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (err != cudaSuccess) return cuda_fail("cudaFuncSetAttribute", err);
+  done_mask.fetch_or(bit);
+  return CP_OK_;
+}
+
+// Kernel entry points implemented in the .cu files.
+int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly_stride, bool inverse,
+               cudaStream_t st);
+
+}  // namespace cpoly

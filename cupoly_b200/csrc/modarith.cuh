@@ -1,0 +1,154 @@
+// Modular arithmetic for 63-bit primes on sm_100a.
+//
+// Replaces cuPoly's Barrett `mod`/`mulmod`/`addmod`/`submod` and the
+// Gaussian-integer helpers (cuPoly src/cuda/dgt.cu:285-675,
+// include/cuPoly/cuda/dgt.h:74-82).  Every result is canonical in [0, p).
+//
+// p < 2^63, so a + b < 2^64 for reduced a, b but 4p > 2^64: lazy [0, 4p)
+// butterflies are impossible and every add/sub is corrected immediately.
+//
+//  * shoup_mul(a, w, w', p): a * w mod p for a constant w with
+//    w' = floor(w 2^64 / p); valid for any a < 2^64 (Shoup / Harvey).
+//  * mont_redc(hi:lo): (hi:lo) * 2^-64 mod p for hi:lo < p 2^64 (Montgomery).
+//  * mul_mod(a, b): exact a * b mod p = REDC(a b) * (2^64 mod p), the second
+//    factor applied with shoup_mul.
+#pragma once
+#include <cstdint>
+
+#ifndef CP_HD
+#define CP_HD __host__ __device__ __forceinline__
+#endif
+
+namespace cpoly {
+
+// Per-residue constants, one entry per prime of an engine (Q then B).
+struct ModConst {
+  uint64_t p;       // the prime
+  uint64_t pneg;    // -p^-1 mod 2^64
+  uint64_t r1;      // 2^64 mod p
+  uint64_t r1s;     // shoup companion of r1
+};
+
+CP_HD uint64_t mulhi64(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+  return __umul64hi(a, b);
+#else
+  return (uint64_t)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+CP_HD uint64_t add_mod(uint64_t a, uint64_t b, uint64_t p) {
+  uint64_t s = a + b;
+  return s >= p ? s - p : s;
+}
+
+CP_HD uint64_t sub_mod(uint64_t a, uint64_t b, uint64_t p) {
+  uint64_t d = a - b;
+  return a < b ? d + p : d;
+}
+
+CP_HD uint64_t neg_mod(uint64_t a, uint64_t p) { return a == 0 ? 0 : p - a; }
+
+// a * w mod p, w < p constant, ws = floor(w * 2^64 / p); any a < 2^64.
+CP_HD uint64_t shoup_mul(uint64_t a, uint64_t w, uint64_t ws, uint64_t p) {
+  uint64_t q = mulhi64(a, ws);
+  uint64_t r = a * w - q * p;  // in [0, 2p)
+  return r >= p ? r - p : r;
+}
+
+// Montgomery reduction of hi:lo < p * 2^64 -> hi:lo * 2^-64 mod p.
+CP_HD uint64_t mont_redc(uint64_t hi, uint64_t lo, uint64_t p, uint64_t pneg) {
+  uint64_t m = lo * pneg;
+  uint64_t t = hi + mulhi64(m, p) + (lo != 0);
+  return t >= p ? t - p : t;
+}
+
+// a * b * 2^-64 mod p for a * b < p * 2^64.
+CP_HD uint64_t mont_mul(uint64_t a, uint64_t b, uint64_t p, uint64_t pneg) {
+  return mont_redc(mulhi64(a, b), a * b, p, pneg);
+}
+
+// Exact a * b mod p for a, b < p.
+CP_HD uint64_t mul_mod(uint64_t a, uint64_t b, const ModConst& m) {
+  return shoup_mul(mont_mul(a, b, m.p, m.pneg), m.r1, m.r1s, m.p);
+}
+
+// 128-bit accumulate helpers (hi:lo += a * b).
+CP_HD void mac128(uint64_t& hi, uint64_t& lo, uint64_t a, uint64_t b) {
+  uint64_t pl = a * b, ph = mulhi64(a, b);
+  lo += pl;
+  hi += ph + (lo < pl);
+}
+
+// Gaussian integer (re + im i) mod p: exact product, result canonical.
+// re = a0 b0 + a1 (p - b1), im = a0 b1 + a1 b0, each < 2 p^2 < p 2^64,
+// reduced by one Montgomery step and corrected by 2^64 mod p.
+CP_HD void gi_mul(uint64_t& cr, uint64_t& ci, uint64_t a0, uint64_t a1, uint64_t b0,
+                  uint64_t b1, const ModConst& m) {
+  uint64_t rh = 0, rl = 0, ih = 0, il = 0;
+  mac128(rh, rl, a0, b0);
+  mac128(rh, rl, a1, b1 == 0 ? 0 : m.p - b1);
+  mac128(ih, il, a0, b1);
+  mac128(ih, il, a1, b0);
+  uint64_t r = mont_redc(rh, rl, m.p, m.pneg);
+  uint64_t i = mont_redc(ih, il, m.p, m.pneg);
+  cr = shoup_mul(r, m.r1, m.r1s, m.p);
+  ci = shoup_mul(i, m.r1, m.r1s, m.p);
+}
+
+// Same product without the 2^64 correction: returns a*b*2^-64 (Montgomery
+// domain).  Used where the correction folds into a later constant.
+CP_HD void gi_mul_mont(uint64_t& cr, uint64_t& ci, uint64_t a0, uint64_t a1, uint64_t b0,
+                       uint64_t b1, const ModConst& m) {
+  uint64_t rh = 0, rl = 0, ih = 0, il = 0;
+  mac128(rh, rl, a0, b0);
+  mac128(rh, rl, a1, b1 == 0 ? 0 : m.p - b1);
+  mac128(ih, il, a0, b1);
+  mac128(ih, il, a1, b0);
+  cr = mont_redc(rh, rl, m.p, m.pneg);
+  ci = mont_redc(ih, il, m.p, m.pneg);
+}
+
+// Gaussian times a Gaussian constant with Shoup companions (4 shoup products).
+CP_HD void gi_mul_const(uint64_t& xr, uint64_t& xi, uint64_t wr, uint64_t wrs, uint64_t wi,
+                        uint64_t wis, uint64_t p) {
+  uint64_t a = shoup_mul(xr, wr, wrs, p);
+  uint64_t b = shoup_mul(xi, wi, wis, p);
+  uint64_t c = shoup_mul(xr, wi, wis, p);
+  uint64_t d = shoup_mul(xi, wr, wrs, p);
+  xr = sub_mod(a, b, p);
+  xi = add_mod(c, d, p);
+}
+
+// ---------------------------------------------------------------------------
+// Host-side helpers (table construction)
+// ---------------------------------------------------------------------------
+inline uint64_t h_mulmod(uint64_t a, uint64_t b, uint64_t p) {
+  return (uint64_t)((unsigned __int128)a * b % p);
+}
+inline uint64_t h_powmod(uint64_t a, uint64_t e, uint64_t p) {
+  uint64_t r = 1 % p;
+  a %= p;
+  while (e) {
+    if (e & 1) r = h_mulmod(r, a, p);
+    a = h_mulmod(a, a, p);
+    e >>= 1;
+  }
+  return r;
+}
+inline uint64_t h_invmod(uint64_t a, uint64_t p) { return h_powmod(a, p - 2, p); }
+inline uint64_t h_shoup(uint64_t w, uint64_t p) {
+  return (uint64_t)(((unsigned __int128)w << 64) / p);
+}
+inline ModConst h_modconst(uint64_t p) {
+  ModConst m;
+  m.p = p;
+  uint64_t inv = 1;  // Newton iteration for p^-1 mod 2^64
+  for (int i = 0; i < 7; ++i) inv *= 2 - p * inv;
+  m.pneg = (uint64_t)0 - inv;
+  m.r1 = (uint64_t)(((unsigned __int128)1 << 64) % p);
+  m.r1s = h_shoup(m.r1, p);
+  return m;
+}
+
+}  // namespace cpoly

@@ -1,0 +1,375 @@
+// Host-side construction of an engine's device tables.
+//
+// Replaces cuPoly's DGTEngine::init / compute_gjk / compute_nthroot
+// (src/cuda/dgt.cu:1501-1982) and CUDAEngine::precompute
+// (src/cuda/cudaengine.cu:1337-1673).  All constants are computed here from
+// the primes and their primitive roots with 128-bit integer arithmetic; no
+// multi-precision library is needed because the HPS step is done by exact
+// mixed-radix conversion, whose constants are single-word residues.
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <thread>
+
+#include "engine.cuh"
+#include "prime_table.h"
+
+namespace cpoly {
+
+namespace {
+thread_local std::string g_last_error;
+
+uint64_t omega(uint64_t p, uint64_t g, uint64_t n) { return h_powmod(g, (p - 1) / n, p); }
+
+int brev(int x, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; ++i) {
+    r = (r << 1) | (x & 1);
+    x >>= 1;
+  }
+  return r;
+}
+
+// Gaussian arithmetic on the host.
+struct G {
+  uint64_t re, im;
+};
+G gmul(G a, G b, uint64_t p) {
+  uint64_t r = (uint64_t)(((unsigned __int128)a.re * b.re + (unsigned __int128)a.im * (b.im ? p - b.im : 0)) % p);
+  uint64_t i = (uint64_t)(((unsigned __int128)a.re * b.im + (unsigned __int128)a.im * b.re) % p);
+  return {r, i};
+}
+G gpow(G a, uint64_t e, uint64_t p) {
+  G r{1, 0};
+  while (e) {
+    if (e & 1) r = gmul(r, a, p);
+    a = gmul(a, a, p);
+    e >>= 1;
+  }
+  return r;
+}
+
+// Extended Euclid inverse of a modulo m (m need not be prime); 0 if none.
+uint64_t inv_general(uint64_t a, uint64_t m) {
+  __int128 t = 0, nt = 1, r = m, nr = a % m;
+  while (nr != 0) {
+    __int128 q = r / nr;
+    __int128 tmp = t - q * nt;
+    t = nt;
+    nt = tmp;
+    tmp = r - q * nr;
+    r = nr;
+    nr = tmp;
+  }
+  if (r != 1) return 0;
+  if (t < 0) t += m;
+  return (uint64_t)t;
+}
+
+uint64_t shoup_general(uint64_t w, uint64_t m) {
+  return (uint64_t)(((unsigned __int128)w << 64) / m);
+}
+
+// Mixed-radix digits of the value with residues r_i over primes s_i.
+std::vector<uint64_t> mrc_digits(const std::vector<uint64_t>& r, const std::vector<uint64_t>& s) {
+  size_t n = s.size();
+  std::vector<uint64_t> d(n);
+  for (size_t i = 0; i < n; ++i) {
+    uint64_t y = r[i] % s[i];
+    for (size_t l = 0; l < i; ++l) {
+      uint64_t dl = d[l] % s[i];
+      y = (y + s[i] - dl) % s[i];
+      y = h_mulmod(y, h_invmod(s[l] % s[i], s[i]), s[i]);
+    }
+    d[i] = y;
+  }
+  return d;
+}
+
+void parallel_for(int n, const std::function<void(int)>& f) {
+  unsigned hw = std::thread::hardware_concurrency();
+  int nt = (int)std::min<unsigned>(hw ? hw : 1, 16);
+  if (n < 2 || nt < 2) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  std::atomic<int> next{0};
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&]() {
+      for (int i = next++; i < n; i = next++) f(i);
+    });
+  for (auto& x : th) x.join();
+}
+}  // namespace
+
+uint64_t primitive_root_of(uint64_t p) {
+  for (int i = 0; i < kNumPrimes; ++i)
+    if (kPrimes[i] == p) return kPrimitiveRoots[i];
+  return 0;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+int Engine::n_residues(int base) const {
+  switch (base) {
+    case 0: return k;          // Q
+    case 1: return kl;         // B
+    case 2: return k + kl;     // QB
+    case 3: return 1;          // T
+    default: return -1;
+  }
+}
+int Engine::rid_offset(int base) const { return base == 1 ? k : 0; }
+
+DgtPlan make_plan(int logN, int logR) {
+  DgtPlan P;
+  P.logN = logN;
+  P.logNc = logN < kMaxLogNc ? logN : kMaxLogNc;
+  P.S = logN - P.logNc;
+  P.logR = logR < P.logNc ? logR : P.logNc;
+  P.npass = (P.logNc + P.logR - 1) / P.logR;
+  P.w[0] = P.logNc - (P.npass - 1) * P.logR;
+  P.p[0] = P.logNc - P.w[0];
+  for (int i = 1; i < P.npass; ++i) {
+    P.w[i] = P.logR;
+    P.p[i] = P.p[i - 1] - P.logR;
+  }
+  return P;
+}
+
+int build_tables(Engine& e) {
+  const int nres = e.k + e.kl;
+  const int N = e.N;
+  const int Nc = 1 << e.plan.logNc;
+  const int R = 1 << e.plan.logR;
+  const DgtPlan& P = e.plan;
+  DgtTableLayout& L = e.layout;
+  int off = 0;
+  L.off_rad = off;
+  off += R;
+  for (int i = 0; i < P.npass; ++i) {
+    if (P.p[i] > 0) {
+      L.off_fwd[i] = off;
+      off += 1 << (P.p[i] + P.w[i]);
+      L.off_inv[i] = off;
+      off += 1 << (P.p[i] + P.w[i]);
+    }
+  }
+  if (P.S > 0) {
+    L.off_split_fwd = off;
+    off += N;
+    L.off_split_inv = off;
+    off += N;
+  }
+  L.off_twist = off;
+  off += 2 * N;
+  L.off_untwist = off;
+  off += 2 * N;
+  L.stride = (off + 1) & ~1;
+
+  std::vector<ulonglong2> tab((size_t)L.stride * nres);
+  parallel_for(nres, [&](int r) {
+    const uint64_t p = e.primes[r];
+    ulonglong2* T = tab.data() + (size_t)r * L.stride;
+    const uint64_t gen = primitive_root_of(p);
+    const uint64_t wN = omega(p, gen, (uint64_t)N);
+    const uint64_t wNi = h_invmod(wN, p);
+    // powers of w_N and w_N^-1
+    std::vector<uint64_t> pw(N), pwi(N);
+    pw[0] = pwi[0] = 1;
+    for (int i = 1; i < N; ++i) {
+      pw[i] = h_mulmod(pw[i - 1], wN, p);
+      pwi[i] = h_mulmod(pwi[i - 1], wNi, p);
+    }
+    auto put = [&](int idx, uint64_t w) { T[idx] = make_ulonglong2(w, h_shoup(w, p)); };
+    for (int j = 0; j < R; ++j) put(L.off_rad + j, pw[(size_t)j * (N / R)]);
+    for (int i = 0; i < P.npass; ++i) {
+      if (P.p[i] == 0) continue;
+      const int pp = P.p[i], ww = P.w[i];
+      const int M = 1 << (pp + ww);
+      const int step = N / M;  // w_M = w_N^step
+      for (int pos = 0; pos < (1 << ww); ++pos) {
+        const int kk = brev(pos, ww);
+        for (int Lw = 0; Lw < (1 << pp); ++Lw) {
+          const size_t e_ = (size_t)Lw * kk % M * step;
+          put(L.off_fwd[i] + pos * (1 << pp) + Lw, pw[e_]);
+          put(L.off_inv[i] + pos * (1 << pp) + Lw, pwi[e_]);
+        }
+      }
+    }
+    if (P.S > 0) {
+      for (int pos = 0; pos < (1 << P.S); ++pos) {
+        const int kk = brev(pos, P.S);
+        for (int Lw = 0; Lw < Nc; ++Lw) {
+          const size_t e_ = (size_t)Lw * kk % N;
+          put(L.off_split_fwd + pos * Nc + Lw, pw[e_]);
+          put(L.off_split_inv + pos * Nc + Lw, pwi[e_]);
+        }
+      }
+    }
+    // twist by xi^n and untwist by xi^-n * N^-1
+    G xi{e.xi[r].first, e.xi[r].second};
+    G xii = gpow(xi, 4 * (uint64_t)N - 1, p);
+    const uint64_t ninv = h_invmod((uint64_t)N, p);
+    G a{1, 0}, b{ninv, 0};
+    for (int n = 0; n < N; ++n) {
+      put(L.off_twist + 2 * n, a.re);
+      put(L.off_twist + 2 * n + 1, a.im);
+      put(L.off_untwist + 2 * n, b.re);
+      put(L.off_untwist + 2 * n + 1, b.im);
+      a = gmul(a, xi, p);
+      b = gmul(b, xii, p);
+    }
+  });
+
+  // ---------------- HPS / mixed-radix constants ----------------
+  std::vector<uint64_t> Q(e.primes.begin(), e.primes.begin() + e.k);
+  std::vector<uint64_t> B(e.primes.begin() + e.k, e.primes.end());
+  std::vector<uint64_t> H;  // packed words
+  auto mark = [&]() { return (int)H.size(); };
+  auto push_pair = [&](uint64_t w, uint64_t m, std::vector<uint64_t>& vals, std::vector<uint64_t>& comp) {
+    vals.push_back(w);
+    comp.push_back(shoup_general(w, m));
+  };
+  auto append = [&](const std::vector<uint64_t>& v) {
+    int o = mark();
+    H.insert(H.end(), v.begin(), v.end());
+    return o;
+  };
+  // MRC inverse constants of a base s: inv[i*(i-1)/2 + l] = s_l^-1 mod s_i
+  auto mrc_inv = [&](const std::vector<uint64_t>& s, std::vector<uint64_t>& v, std::vector<uint64_t>& c) {
+    for (size_t i = 1; i < s.size(); ++i)
+      for (size_t l = 0; l < i; ++l) push_pair(h_invmod(s[l] % s[i], s[i]), s[i], v, c);
+  };
+  // Horner constants: hor[j*(n-1) + i] = s_i mod m_j
+  auto horner = [&](const std::vector<uint64_t>& s, const std::vector<uint64_t>& m, std::vector<uint64_t>& v,
+                    std::vector<uint64_t>& c) {
+    for (size_t j = 0; j < m.size(); ++j)
+      for (size_t i = 0; i + 1 < s.size(); ++i) push_pair(s[i] % m[j], m[j], v, c);
+  };
+  auto prod_mod = [&](const std::vector<uint64_t>& s, uint64_t m) {
+    uint64_t r = 1 % m;
+    for (auto x : s) r = h_mulmod(r, x % m, m);
+    return r;
+  };
+  {
+    std::vector<uint64_t> v, c;
+    mrc_inv(Q, v, c);
+    e.ho.qb_inv = append(v);
+    e.ho.qb_inv_s = append(c);
+  }
+  {
+    std::vector<uint64_t> v, c;
+    horner(Q, B, v, c);
+    e.ho.qb_hor = append(v);
+    e.ho.qb_hor_s = append(c);
+  }
+  {
+    std::vector<uint64_t> half(Q.size());
+    for (size_t i = 0; i < Q.size(); ++i) half[i] = (Q[i] - 1) / 2;  // (Q-1)/2 mod q_i
+    e.ho.qb_half = append(mrc_digits(half, Q));
+  }
+  {
+    std::vector<uint64_t> v, c;
+    mrc_inv(B, v, c);
+    e.ho.bq_inv = append(v);
+    e.ho.bq_inv_s = append(c);
+  }
+  {
+    std::vector<uint64_t> v, c;
+    horner(B, Q, v, c);
+    e.ho.bq_hor = append(v);
+    e.ho.bq_hor_s = append(c);
+  }
+  {
+    std::vector<uint64_t> v, c;
+    horner(Q, std::vector<uint64_t>{e.t}, v, c);
+    e.ho.qt_hor = append(v);
+    e.ho.qt_hor_s = append(c);
+  }
+  {
+    std::vector<uint64_t> v, c, v2, c2, v3, c3, v4, c4;
+    for (auto b : B) {
+      uint64_t qm = prod_mod(Q, b);
+      push_pair(qm, b, v, c);
+      push_pair(h_invmod(qm, b), b, v2, c2);
+      push_pair(e.t % b, b, v4, c4);
+    }
+    for (auto q : Q) push_pair(e.t % q, q, v3, c3);
+    e.ho.q_mod_b = append(v);
+    e.ho.q_mod_b_s = append(c);
+    e.ho.qinv_b = append(v2);
+    e.ho.qinv_b_s = append(c2);
+    e.ho.t_q = append(v3);
+    e.ho.t_q_s = append(c3);
+    e.ho.t_b = append(v4);
+    e.ho.t_b_s = append(c4);
+  }
+  {
+    uint64_t qt = prod_mod(Q, e.t);
+    uint64_t qi = inv_general(qt, e.t);
+    std::vector<uint64_t> v{qt}, c{shoup_general(qt, e.t)}, v2{qi}, c2{shoup_general(qi, e.t)};
+    e.ho.q_mod_t = append(v);
+    e.ho.q_mod_t_s = append(c);
+    e.ho.qinv_t = append(v2);
+    e.ho.qinv_t_s = append(c2);
+    e.t_shoup_one = shoup_general(1 % e.t, e.t);
+    e.h_q_mod_t = qt;
+    e.h_qinv_t = qi;
+    e.h_qinv_t_s = shoup_general(qi, e.t);
+  }
+  {
+    std::vector<uint64_t> v, c, v2, c2;
+    for (size_t i = 0; i < Q.size(); ++i) {
+      uint64_t qq = 1 % Q[i];
+      for (size_t l = 0; l < Q.size(); ++l)
+        if (l != i) qq = h_mulmod(qq, Q[l] % Q[i], Q[i]);
+      push_pair(h_invmod(qq, Q[i]), Q[i], v, c);
+      push_pair(qq, Q[i], v2, c2);
+    }
+    e.ho.xi_q = append(v);
+    e.ho.xi_q_s = append(c);
+    e.ho.rho_q = append(v2);
+    e.ho.rho_q_s = append(c2);
+  }
+  e.hps_words = H.size();
+
+  // ---------------- upload ----------------
+  cudaError_t err;
+  if ((err = cudaMalloc(&e.d_tab, tab.size() * sizeof(ulonglong2))) != cudaSuccess ||
+      (err = cudaMalloc(&e.d_mc, e.mconst.size() * sizeof(ModConst))) != cudaSuccess ||
+      (err = cudaMalloc(&e.d_hps, (H.size() + 1) * sizeof(uint64_t))) != cudaSuccess ||
+      (err = cudaMalloc(&e.d_err, sizeof(int))) != cudaSuccess) {
+    set_error(std::string("cudaMalloc failed for engine tables: ") + cudaGetErrorString(err));
+    free_tables(e);
+    return 4;
+  }
+  if ((err = cudaMemcpy(e.d_tab, tab.data(), tab.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (err = cudaMemcpy(e.d_mc, e.mconst.data(), e.mconst.size() * sizeof(ModConst), cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (err = cudaMemcpy(e.d_hps, H.data(), H.size() * sizeof(uint64_t), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (err = cudaMemset(e.d_err, 0, sizeof(int))) != cudaSuccess) {
+    set_error(std::string("table upload failed: ") + cudaGetErrorString(err));
+    free_tables(e);
+    return 2;
+  }
+  return 0;
+}
+
+void free_tables(Engine& e) {
+  if (e.d_tab) cudaFree(e.d_tab);
+  if (e.d_mc) cudaFree(e.d_mc);
+  if (e.d_hps) cudaFree(e.d_hps);
+  if (e.d_err) cudaFree(e.d_err);
+  e.d_err = nullptr;
+  e.d_tab = nullptr;
+  e.d_mc = nullptr;
+  e.d_hps = nullptr;
+}
+
+}  // namespace cpoly

@@ -1,0 +1,519 @@
+"""cuPoly's polynomial API, re-created over the C ABI.
+
+Mirrors the names, argument meaning and state machine of cuPoly 0.3.5
+(include/cuPoly/arithmetic/polynomial.h, cudaengine.h, dgt.h, sampler.h,
+context.h) so that code written against cuPoly reads the same:
+
+    CUDAEngine.init(k, k + 1, nphi, t)
+    ctx = Context()
+    Sampler.init(ctx)
+    a, b, c = poly_t(), poly_t(), poly_t()
+    Sampler.sample(ctx, a, UNIFORM); Sampler.sample(ctx, b, UNIFORM)
+    poly_mul(ctx, c, a, b)
+    poly_get_coeff(ctx, c, 0)
+
+Coefficients on the host are Python integers (cuPoly: NTL ZZ).  A poly_t
+keeps cuPoly's lazy host/device state machine (polynomial.h:39-66): device
+data is in the DGT domain while the status is RNSSTATE or BOTHSTATE.
+Errors raise (cuPoly: assert / std::runtime_error / exit(1)).
+"""
+from __future__ import annotations
+
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from .engine import (ADD, ADDADD, BBase, BINARY, DESTROY_INPUTS, DISCRETE_GAUSSIAN, FORWARD, GAUSSIAN,
+                     HAMMINGWEIGHT, INVERSE, MUL, MULMUL, NARROW, QBBase, QBase, SUB, TBase, TERNARY, UNIFORM, ZO,
+                     Engine, from_u64, to_u64)
+
+HOSTSTATE, RNSSTATE, BOTHSTATE = 0, 1, 2
+HAMMINGWEIGHT_H = 64
+GAUSSIAN_STD_DEVIATION = 3.2
+SEED = 42
+
+__all__ = [
+    "CUDAEngine", "DGTEngine", "Context", "Sampler", "poly_t", "QBase", "BBase", "QBBase", "TBase", "FORWARD",
+    "INVERSE", "ADD", "SUB", "MUL", "MULMUL", "ADDADD", "DISCRETE_GAUSSIAN", "HAMMINGWEIGHT", "NARROW", "ZO",
+    "BINARY", "UNIFORM", "TERNARY", "GAUSSIAN", "HOSTSTATE", "RNSSTATE", "BOTHSTATE",
+]
+
+
+def _prod(xs):
+    r = 1
+    for x in xs:
+        r *= x
+    return r
+
+
+class CUDAEngine:
+    """Process-wide default engine (cuPoly include/cuPoly/cuda/cudaengine.h:59-123)."""
+
+    engine: Optional[Engine] = None
+    is_init = False
+    N = 0
+    t = 0
+    RNSPrimes: List[int] = []
+    RNSBPrimes: List[int] = []
+    RNSProduct = 1
+    RNSBProduct = 1
+    RNSMpi: List[int] = []
+    RNSInvMpi: List[int] = []
+
+    @classmethod
+    def init(cls, k: int, kl: int, M: int, t: int, log_radix: int = 0):
+        """init(k, kl, M, t): M is the ring degree nphi (cuPoly cudaengine.cu:1691-1731)."""
+        if cls.is_init:
+            cls.destroy()
+        cls.engine = Engine(k, kl if kl > 0 else k + 1, M, t, log_radix)
+        cls.N = M >> 1
+        cls.t = t
+        cls.RNSPrimes = list(cls.engine.Q)
+        cls.RNSBPrimes = list(cls.engine.B)
+        cls.RNSProduct = _prod(cls.RNSPrimes)
+        cls.RNSBProduct = _prod(cls.RNSBPrimes)
+        cls.RNSMpi = [cls.RNSProduct // p for p in cls.RNSPrimes]
+        cls.RNSInvMpi = [pow(m % p, -1, p) for m, p in zip(cls.RNSMpi, cls.RNSPrimes)]
+        cls.is_init = True
+
+    @classmethod
+    def destroy(cls):
+        if cls.engine is not None:
+            torch.cuda.synchronize()
+            cls.engine.close()
+        cls.engine = None
+        cls.is_init = False
+
+    @classmethod
+    def get_n_residues(cls, base: int) -> int:
+        assert cls.is_init
+        return cls.engine.n_residues(base)
+
+
+def _E() -> Engine:
+    if not CUDAEngine.is_init:
+        raise RuntimeError("CUDAEngine is not initialised")
+    return CUDAEngine.engine
+
+
+class Context:
+    """One stream plus scratch (cuPoly include/cuPoly/arithmetic/context.h:34-109)."""
+
+    def __init__(self):
+        e = _E()
+        self.stream = torch.cuda.Stream()
+        with torch.cuda.stream(self.stream):
+            self.workspace = e.workspace()
+            self.d_aux_coefs = e.empty(QBBase)
+
+    def get_stream(self):
+        return self.stream
+
+
+class poly_t:
+    """cuPoly's polynomial struct (polynomial.h:55-66)."""
+
+    def __init__(self):
+        self.init = False
+        self.coefs: List[int] = []
+        self.d_coefs: Optional[torch.Tensor] = None
+        self.status = BOTHSTATE
+        self.base = QBase
+
+
+class DGTEngine:
+    """cuPoly include/cuPoly/cuda/dgt.h:106-283 (static members)."""
+
+    @staticmethod
+    def execute_dgt(data: torch.Tensor, base: int, direction: int, ctx: Context):
+        _E().dgt(data, base, direction, npolys=1, stream=ctx.stream)
+
+    @staticmethod
+    def execute_add_dgt(c, a, b, base, stream):
+        _E().add(c, a, b, base, stream)
+
+    @staticmethod
+    def execute_sub_dgt(c, a, b, base, stream):
+        _E().sub(c, a, b, base, stream)
+
+    @staticmethod
+    def execute_double_add_dgt(c1, a1, b1, c2, a2, b2, base, stream):
+        _E().double_add(c1, a1, b1, c2, a2, b2, base, stream)
+
+    @staticmethod
+    def execute_dr2_dgt(c21, c22, c23, c01, c02, c11, c12, base, stream):
+        _E().dr2(c21, c22, c23, c01, c02, c11, c12, base, stream)
+
+    @staticmethod
+    def execute_mul_dgt_gi(c, a, b, base, stream):
+        _E().mul(c, a, b, base, stream)
+
+    @staticmethod
+    def execute_mul_dgt_u64(c, a, b, base, stream):
+        _E().mul_u64(c, a, b, base, stream)
+
+    @staticmethod
+    def execute_muladd_dgt(d, a, b, c, base, stream):
+        _E().muladd(d, a, b, c, base, stream)
+
+
+# ---------------------------------------------------------------------------
+# state machine (polynomial.cu:45-188)
+# ---------------------------------------------------------------------------
+def poly_get_residues_size(base: int) -> int:
+    return CUDAEngine.N * CUDAEngine.get_n_residues(base) * 16
+
+
+def poly_init(ctx: Context, a: poly_t, base: int = QBase):
+    if a.init:
+        return
+    e = _E()
+    a.base = base
+    with torch.cuda.stream(ctx.stream):
+        a.d_coefs = e.zeros(base)
+    a.coefs = [0] * (2 * CUDAEngine.N)
+    a.status = BOTHSTATE
+    a.init = True
+
+
+def poly_free(ctx: Context, a: poly_t):
+    if a is None or not a.init:
+        return
+    ctx.stream.synchronize()
+    a.coefs = []
+    a.d_coefs = None
+    a.init = False
+
+
+def poly_clear(ctx: Context, a: poly_t):
+    poly_init(ctx, a)
+    a.coefs = []
+    with torch.cuda.stream(ctx.stream):
+        a.d_coefs.zero_()
+    a.status = BOTHSTATE
+
+
+def _residues_of(coefs: List[int], primes: List[int], N: int) -> np.ndarray:
+    nphi = 2 * N
+    c = list(coefs[:nphi]) + [0] * max(0, nphi - len(coefs))
+    out = np.empty((len(primes), N, 2), dtype=np.uint64)
+    for r, p in enumerate(primes):
+        row = np.array([x % p for x in c], dtype=np.uint64)
+        out[r, :, 0] = row[:N]
+        out[r, :, 1] = row[N:]
+    return out
+
+
+def poly_crt(ctx: Context, a: poly_t) -> np.ndarray:
+    """Host residues of the coefficients (cuPoly polynomial.cu:190-221)."""
+    assert a.base in (QBase, QBBase)
+    return _residues_of(a.coefs, _E().base_primes(a.base), CUDAEngine.N)
+
+
+def poly_icrt(ctx: Context, a: poly_t, h: np.ndarray):
+    """CRT recombination into coefficients in [0, Q) (polynomial.cu:223-296)."""
+    N = CUDAEngine.N
+    if a.base == TBase:
+        a.coefs = [int(v) for v in np.concatenate([h[0, :, 0], h[0, :, 1]])]
+        return
+    if a.base != QBase:
+        raise RuntimeError("Unknown base")
+    Q = CUDAEngine.RNSProduct
+    acc = [0] * (2 * N)
+    for r, p in enumerate(CUDAEngine.RNSPrimes):
+        Mi, inv = CUDAEngine.RNSMpi[r], CUDAEngine.RNSInvMpi[r]
+        row = np.concatenate([h[r, :, 0], h[r, :, 1]]).tolist()
+        for i, x in enumerate(row):
+            if x:
+                acc[i] += (x * inv % p) * Mi
+    a.coefs = [x % Q for x in acc]
+
+
+def poly_copy_to_device(ctx: Context, a: poly_t):
+    if a.status in (RNSSTATE, BOTHSTATE):
+        return
+    e = _E()
+    with torch.cuda.stream(ctx.stream):
+        a.d_coefs = from_u64(poly_crt(ctx, a)[None])
+    e.dgt(a.d_coefs, a.base, FORWARD, stream=ctx.stream)
+    ctx.stream.synchronize()
+    a.status = BOTHSTATE
+
+
+def poly_copy_to_host(ctx: Context, a: poly_t):
+    if a.status in (HOSTSTATE, BOTHSTATE):
+        return
+    e = _E()
+    with torch.cuda.stream(ctx.stream):
+        aux = a.d_coefs.clone()
+    e.dgt(aux, a.base, INVERSE, stream=ctx.stream)
+    ctx.stream.synchronize()
+    poly_icrt(ctx, a, to_u64(aux[0]))
+    a.status = BOTHSTATE
+
+
+def poly_copy(ctx: Context, b: poly_t, a: poly_t):
+    poly_init(ctx, b, a.base)
+    if a.status in (RNSSTATE, BOTHSTATE):
+        with torch.cuda.stream(ctx.stream):
+            b.d_coefs = a.d_coefs.clone()
+        b.base = a.base
+        b.status = RNSSTATE
+    else:
+        b.coefs = list(a.coefs)
+        b.status = HOSTSTATE
+
+
+def poly_set_coeff(ctx: Context, a: poly_t, index: int, c: int):
+    if not a.init:
+        poly_init(ctx, a)
+    poly_copy_to_host(ctx, a)
+    if c < 0:
+        c = CUDAEngine.RNSProduct + c
+    if index >= len(a.coefs):
+        a.coefs.extend([0] * (index + 1 - len(a.coefs)))
+    a.coefs[index] = c
+    a.status = HOSTSTATE
+
+
+def poly_get_coeff(ctx: Context, a: poly_t, index: int) -> int:
+    assert a.init
+    poly_copy_to_host(ctx, a)
+    return a.coefs[index] if index < len(a.coefs) else 0
+
+
+def poly_get_deg(ctx: Context, a: poly_t) -> int:
+    if a.status == RNSSTATE:
+        poly_copy_to_host(ctx, a)
+    c = a.coefs
+    d = len(c) - 1
+    while d >= 0 and c[d] == 0:
+        d -= 1
+    return d
+
+
+def poly_are_equal(ctx: Context, a: poly_t, b: poly_t) -> bool:
+    if poly_get_deg(ctx, a) != poly_get_deg(ctx, b):
+        return False
+    Q = CUDAEngine.RNSProduct
+    return all(poly_get_coeff(ctx, a, i) % Q == poly_get_coeff(ctx, b, i) % Q
+               for i in range(poly_get_deg(ctx, a) + 1))
+
+
+def poly_to_string(ctx: Context, a: poly_t) -> str:
+    return "".join("%d, " % poly_get_coeff(ctx, a, i) for i in range(poly_get_deg(ctx, a) + 1))
+
+
+# ---------------------------------------------------------------------------
+# arithmetic (polynomial.cu:802-1153)
+# ---------------------------------------------------------------------------
+def _prep(ctx, out: poly_t, base: int, *ins: poly_t):
+    for x in ins:
+        assert x.init
+        poly_copy_to_device(ctx, x)
+    poly_init(ctx, out, base)
+    if out.d_coefs is None or out.d_coefs.shape[1] != CUDAEngine.get_n_residues(base):
+        with torch.cuda.stream(ctx.stream):
+            out.d_coefs = _E().zeros(base)
+
+
+def _done(out: poly_t, base: int):
+    out.status = RNSSTATE
+    out.base = base
+
+
+def poly_add(ctx, c, a, b):
+    assert a.base == b.base
+    _prep(ctx, c, a.base, a, b)
+    _E().add(c.d_coefs, a.d_coefs, b.d_coefs, a.base, ctx.stream)
+    _done(c, a.base)
+
+
+def poly_sub(ctx, c, a, b):
+    assert a.base == b.base
+    _prep(ctx, c, a.base, a, b)
+    _E().sub(c.d_coefs, a.d_coefs, b.d_coefs, a.base, ctx.stream)
+    _done(c, a.base)
+
+
+def poly_double_add(ctx, c1, a1, b1, c2, a2, b2):
+    assert a1.base == b1.base == a2.base == b2.base
+    _prep(ctx, c1, a1.base, a1, b1, a2, b2)
+    _prep(ctx, c2, a1.base)
+    _E().double_add(c1.d_coefs, a1.d_coefs, b1.d_coefs, c2.d_coefs, a2.d_coefs, b2.d_coefs, a1.base, ctx.stream)
+    _done(c1, a1.base)
+    _done(c2, a1.base)
+
+
+def poly_mul(ctx, c, a, b):
+    assert a.base == b.base
+    _prep(ctx, c, a.base, a, b)
+    _E().mul(c.d_coefs, a.d_coefs, b.d_coefs, a.base, ctx.stream)
+    _done(c, a.base)
+
+
+def poly_mul_add(ctx, d, a, b, c):
+    assert a.base == b.base == c.base
+    _prep(ctx, d, a.base, a, b, c)
+    _E().muladd(d.d_coefs, a.d_coefs, b.d_coefs, c.d_coefs, a.base, ctx.stream)
+    _done(d, a.base)
+
+
+def poly_dr2(ctx, ct21, ct22, ct23, ct01, ct02, ct11, ct12):
+    assert ct01.base == ct02.base == ct11.base == ct12.base
+    base = ct01.base
+    _prep(ctx, ct21, base, ct01, ct02, ct11, ct12)
+    _prep(ctx, ct22, base)
+    _prep(ctx, ct23, base)
+    _E().dr2(ct21.d_coefs, ct22.d_coefs, ct23.d_coefs, ct01.d_coefs, ct02.d_coefs, ct11.d_coefs, ct12.d_coefs,
+             base, ctx.stream)
+    for x in (ct21, ct22, ct23):
+        _done(x, base)
+
+
+def _op_int(ctx, b, a, x, op):
+    _prep(ctx, b, a.base, a)
+    _E().op_by_int(b.d_coefs, a.d_coefs, a.base, x, op, ctx.stream)
+    _done(b, a.base)
+
+
+def poly_mul_int(ctx, b, a, x):
+    _op_int(ctx, b, a, x, MUL)
+
+
+def poly_add_int(ctx, b, a, x):
+    _op_int(ctx, b, a, x, ADD)
+
+
+def poly_sub_int(ctx, b, a, x):
+    _op_int(ctx, b, a, x, SUB)
+
+
+def poly_double_mul_int(ctx, b1, a1, b2, a2, x1, x2):
+    _prep(ctx, b1, a1.base, a1, a2)
+    _prep(ctx, b2, a1.base)
+    _E().double_op_by_int(b1.d_coefs, a1.d_coefs, b2.d_coefs, a2.d_coefs, a1.base, x1, x2, MULMUL, ctx.stream)
+    _done(b1, a1.base)
+    _done(b2, a1.base)
+
+
+def poly_double_add_int(ctx, b1, a1, b2, a2, x1, x2):
+    _prep(ctx, b1, a1.base, a1, a2)
+    _prep(ctx, b2, a1.base)
+    _E().double_op_by_int(b1.d_coefs, a1.d_coefs, b2.d_coefs, a2.d_coefs, a1.base, x1, x2, ADDADD, ctx.stream)
+    _done(b1, a1.base)
+    _done(b2, a1.base)
+
+
+def poly_negate(ctx, a):
+    poly_copy_to_device(ctx, a)
+    _E().negate(a.d_coefs, a.d_coefs, a.base, ctx.stream)
+    a.status = RNSSTATE
+
+
+# ---------------------------------------------------------------------------
+# HPS (polynomial.cu:310-527)
+# ---------------------------------------------------------------------------
+def poly_simple_scaling_tDivQ(ctx, b, a):
+    assert a.base == QBase
+    poly_copy_to_device(ctx, a)
+    poly_init(ctx, b)
+    with torch.cuda.stream(ctx.stream):
+        b.d_coefs = _E().zeros(TBase)
+    _E().poly_simple_scaling_tdivq(b.d_coefs, a.d_coefs, ctx.stream)
+    b.status = RNSSTATE
+    b.base = TBase
+
+
+def poly_complex_scaling_tDivQ(ctx, b_Q, a_Q, a_B):
+    """Destroys a_Q and a_B like cuPoly (polynomial.h:346-347)."""
+    assert a_Q.base == QBase and a_B.base == BBase
+    poly_copy_to_device(ctx, a_Q)
+    poly_copy_to_device(ctx, a_B)
+    _prep(ctx, b_Q, QBase)
+    _E().poly_complex_scaling_tdivq(b_Q.d_coefs, a_Q.d_coefs, a_B.d_coefs, DESTROY_INPUTS, ctx.stream)
+    # cuPoly leaves the inputs inverse-transformed but still flagged RNSSTATE
+    _done(b_Q, QBase)
+
+
+def poly_basis_extension_Q_to_B(ctx, a_B, a_Q):
+    assert a_Q.base == QBase
+    poly_copy_to_device(ctx, a_Q)
+    _prep(ctx, a_B, BBase)
+    _E().poly_basis_extension_q_to_b(a_B.d_coefs, a_Q.d_coefs, ctx.stream)
+    _done(a_B, BBase)
+
+
+def poly_basis_extension_Q_to_QB(ctx, b, a):
+    assert a.base == QBase
+    poly_copy_to_device(ctx, a)
+    _prep(ctx, b, QBBase)
+    _E().poly_basis_extension_q_to_qb(b.d_coefs, a.d_coefs, ctx.stream)
+    _done(b, QBBase)
+
+
+def poly_basis_extension_B_to_Q(ctx, a_Q, a_B):
+    assert a_B.base == BBase
+    poly_copy_to_device(ctx, a_B)
+    _prep(ctx, a_Q, QBase)
+    _E().poly_basis_extension_b_to_q(a_Q.d_coefs, a_B.d_coefs, ctx.stream)
+    _done(a_Q, QBase)
+
+
+def _xi_rho(ctx, c: List[poly_t], a: poly_t, rho: bool):
+    e = _E()
+    poly_copy_to_device(ctx, a)
+    with torch.cuda.stream(ctx.stream):
+        out = e.empty(QBase, e.k)
+    (e.rho if rho else e.xi)(out, a.d_coefs, ctx.stream)
+    for i in range(e.k):
+        poly_init(ctx, c[i])
+        c[i].d_coefs = out[i:i + 1]
+        _done(c[i], QBase)
+
+
+def poly_xi_bfv(ctx, c: List[poly_t], a: poly_t):
+    """c[i] has residue i equal to a_i (Q/q_i)^-1 mod q_i (cuPoly polynomial.cu:612-650)."""
+    _xi_rho(ctx, c, a, False)
+
+
+def poly_rho_bfv(ctx, c: List[poly_t], a: poly_t):
+    """c[i] has residue i equal to a_i (Q/q_i) mod q_i (cuPoly polynomial.cu:652-693)."""
+    _xi_rho(ctx, c, a, True)
+
+
+# ---------------------------------------------------------------------------
+# Sampler (sampler.h:53-101)
+# ---------------------------------------------------------------------------
+class Sampler:
+    seed = SEED
+    _counter = 0
+
+    @classmethod
+    def init(cls, ctx: Context):
+        cls._counter = 0
+
+    @classmethod
+    def reset(cls, ctx: Context):
+        cls._counter = 0
+
+    @classmethod
+    def destroy(cls):
+        pass
+
+    @classmethod
+    def sample(cls, ctx: Context, p: Optional[poly_t] = None, kind: int = UNIFORM):
+        """sample(ctx, p, kind) fills p; sample(ctx, kind) returns a new poly_t."""
+        if isinstance(p, int):
+            p, kind = None, p
+        ret = p is None
+        if p is None:
+            p = poly_t()
+        poly_init(ctx, p)
+        e = _E()
+        sid = cls._counter
+        cls._counter += 1
+        e.sample(p.d_coefs, p.base, kind, cls.seed, sid, npolys=1, to_dgt=True, stream=ctx.stream)
+        p.status = RNSSTATE
+        return p if ret else None

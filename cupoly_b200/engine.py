@@ -1,0 +1,230 @@
+"""Engine objects over the C ABI, with device buffers held in torch tensors.
+
+``Engine`` is one (nphi, k, kl, t) parameter set with its own device tables;
+any number of engines coexist (cuPoly allows one per process).  Buffers are
+int64 tensors of shape ``(npolys, nres, N, 2)`` whose bytes are cuPoly's
+GaussianInteger layout (the bit patterns are uint64 residues).  torch is
+used only for device memory and streams; every computation is a call into
+``libcupoly_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call
+
+QBase, BBase, QBBase, TBase = 0, 1, 2, 3
+FORWARD, INVERSE = 0, 1
+ADD, SUB, MUL, MULMUL, ADDADD = 0, 1, 2, 3, 4
+(DISCRETE_GAUSSIAN, HAMMINGWEIGHT, NARROW, ZO, BINARY, UNIFORM, TERNARY, GAUSSIAN) = range(8)
+DESTROY_INPUTS = 1
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def to_u64(t: torch.Tensor) -> np.ndarray:
+    """Copy a device buffer to a host numpy uint64 array of the same shape."""
+    return t.detach().cpu().numpy().view(np.uint64)
+
+
+def from_u64(a: np.ndarray, device="cuda") -> torch.Tensor:
+    """Copy a host uint64 array to a device int64 tensor (same bytes)."""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return torch.from_numpy(a.view(np.int64)).to(device)
+
+
+class Engine:
+    """One parameter set: ring degree nphi, |Q| = k, |B| = kl, plaintext modulus t."""
+
+    def __init__(self, k: int, kl: int = 0, nphi: int = 4096, t: int = 256, log_radix: int = 0):
+        if not torch.cuda.is_available():
+            raise RuntimeError("cupoly_b200 needs a CUDA device")
+        _lib.lib()
+        h = C.c_void_p()
+        call("cp_engine_create", C.byref(h), k, kl, nphi, t, log_radix)
+        self._h = h
+        self.k = k
+        self.kl = kl if kl > 0 else k + 1
+        self.nphi = nphi
+        self.N = nphi // 2
+        self.t = t
+        buf = (C.c_uint64 * (self.k + self.kl))()
+        _lib.lib().cp_engine_primes(h, buf, self.k + self.kl)
+        self.primes: List[int] = [int(x) for x in buf]
+        self.Q = self.primes[: self.k]
+        self.B = self.primes[self.k:]
+        self._ws: Optional[torch.Tensor] = None
+
+    # ---- lifecycle ----
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.lib().cp_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def n_residues(self, base: int) -> int:
+        return {QBase: self.k, BBase: self.kl, QBBase: self.k + self.kl, TBase: 1}[base]
+
+    def base_primes(self, base: int) -> List[int]:
+        return {QBase: self.Q, BBase: self.B, QBBase: self.primes, TBase: [self.t]}[base]
+
+    # ---- memory ----
+    def empty(self, base: int = QBase, npolys: int = 1) -> torch.Tensor:
+        return torch.empty((npolys, self.n_residues(base), self.N, 2), dtype=torch.int64, device="cuda")
+
+    def zeros(self, base: int = QBase, npolys: int = 1) -> torch.Tensor:
+        return torch.zeros((npolys, self.n_residues(base), self.N, 2), dtype=torch.int64, device="cuda")
+
+    def workspace(self) -> torch.Tensor:
+        if self._ws is None:
+            n = _lib.lib().cp_workspace_bytes(self._h)
+            self._ws = torch.empty(((n + 15) // 16, 2), dtype=torch.int64, device="cuda")
+        return self._ws
+
+    # ---- roots ----
+    def set_nthroot(self, xi: Sequence[Sequence[int]]):
+        arr = (C.c_uint64 * (2 * len(xi)))(*[int(v) for pair in xi for v in pair])
+        call("cp_engine_set_nthroot", self._h, arr)
+
+    def get_nthroot(self):
+        n = self.k + self.kl
+        arr = (C.c_uint64 * (2 * n))()
+        call("cp_engine_get_nthroot", self._h, arr)
+        return [(int(arr[2 * i]), int(arr[2 * i + 1])) for i in range(n)]
+
+    def check(self, stream=None):
+        call("cp_engine_check", self._h, _stream(stream))
+
+    # ---- DGT ----
+    def dgt(self, x: torch.Tensor, base: int, direction: int, npolys: Optional[int] = None, stream=None):
+        n = x.shape[0] if npolys is None else npolys
+        call("cp_dgt", self._h, _ptr(x), base, direction, n, 0, _stream(stream))
+        return x
+
+    # ---- pointwise ----
+    def add(self, c, a, b, base, stream=None):
+        call("cp_add", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
+
+    def sub(self, c, a, b, base, stream=None):
+        call("cp_sub", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
+
+    def double_add(self, c1, a1, b1, c2, a2, b2, base, stream=None):
+        call("cp_double_add", self._h, _ptr(c1), _ptr(a1), _ptr(b1), _ptr(c2), _ptr(a2), _ptr(b2), base,
+             _stream(stream))
+
+    def mul(self, c, a, b, base, stream=None):
+        call("cp_mul", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
+
+    def mul_batch(self, c, a, b, base, npolys=None, stream=None):
+        n = c.shape[0] if npolys is None else npolys
+        call("cp_mul_batch", self._h, _ptr(c), _ptr(a), _ptr(b), base, n, _stream(stream))
+
+    def mul_u64(self, c, a, b, base, stream=None):
+        call("cp_mul_u64", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
+
+    def muladd(self, d, a, b, c, base, stream=None):
+        call("cp_muladd", self._h, _ptr(d), _ptr(a), _ptr(b), _ptr(c), base, _stream(stream))
+
+    def dr2(self, c21, c22, c23, c01, c02, c11, c12, base, stream=None):
+        call("cp_dr2", self._h, _ptr(c21), _ptr(c22), _ptr(c23), _ptr(c01), _ptr(c02), _ptr(c11), _ptr(c12),
+             base, _stream(stream))
+
+    def negate(self, b, a, base, stream=None):
+        call("cp_negate", self._h, _ptr(b), _ptr(a), base, _stream(stream))
+
+    def op_by_int(self, b, a, base, x, op, stream=None):
+        call("cp_op_by_int", self._h, _ptr(b), _ptr(a), base, int(x), op, _stream(stream))
+
+    def double_op_by_int(self, b1, a1, b2, a2, base, x1, x2, op, stream=None):
+        call("cp_double_op_by_int", self._h, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), base, int(x1), int(x2), op,
+             _stream(stream))
+
+    # ---- HPS (coefficient domain) ----
+    def basis_ext_q_to_b(self, out_b, in_q, npolys=1, stream=None):
+        call("cp_basis_ext_q_to_b", self._h, _ptr(out_b), _ptr(in_q), npolys, _stream(stream))
+
+    def basis_ext_b_to_q(self, out_q, in_b, npolys=1, stream=None):
+        call("cp_basis_ext_b_to_q", self._h, _ptr(out_q), _ptr(in_b), npolys, _stream(stream))
+
+    def complex_scaling(self, out_b, in_q, in_b, npolys=1, stream=None):
+        call("cp_complex_scaling", self._h, _ptr(out_b), _ptr(in_q), _ptr(in_b), npolys, _stream(stream))
+
+    def simple_scaling(self, out_t, in_q, stream=None):
+        call("cp_simple_scaling", self._h, _ptr(out_t), _ptr(in_q), _stream(stream))
+
+    def xi(self, out, a, stream=None):
+        call("cp_xi", self._h, _ptr(out), _ptr(a), _stream(stream))
+
+    def rho(self, out, a, stream=None):
+        call("cp_rho", self._h, _ptr(out), _ptr(a), _stream(stream))
+
+    # ---- composite (DGT domain) ----
+    def poly_basis_extension_q_to_b(self, out_b, in_q, stream=None):
+        call("cp_poly_basis_extension_q_to_b", self._h, _ptr(out_b), _ptr(in_q), _ptr(self.workspace()),
+             _stream(stream))
+
+    def poly_basis_extension_q_to_qb(self, out_qb, in_q, stream=None):
+        call("cp_poly_basis_extension_q_to_qb", self._h, _ptr(out_qb), _ptr(in_q), _ptr(self.workspace()),
+             _stream(stream))
+
+    def poly_basis_extension_b_to_q(self, out_q, in_b, stream=None):
+        call("cp_poly_basis_extension_b_to_q", self._h, _ptr(out_q), _ptr(in_b), _ptr(self.workspace()),
+             _stream(stream))
+
+    def poly_complex_scaling_tdivq(self, out_q, in_q, in_b, flags=0, stream=None):
+        call("cp_poly_complex_scaling_tdivq", self._h, _ptr(out_q), _ptr(in_q), _ptr(in_b), flags,
+             _ptr(self.workspace()), _stream(stream))
+
+    def poly_simple_scaling_tdivq(self, out_t, in_q, stream=None):
+        call("cp_poly_simple_scaling_tdivq", self._h, _ptr(out_t), _ptr(in_q), _ptr(self.workspace()),
+             _stream(stream))
+
+    def bfv_mul(self, c0, c1, c2, a0, a1, b0, b1, stream=None):
+        call("cp_bfv_mul", self._h, _ptr(c0), _ptr(c1), _ptr(c2), _ptr(a0), _ptr(a1), _ptr(b0), _ptr(b1),
+             _ptr(self.workspace()), _stream(stream))
+
+    def bfv_mul_batch_workspace(self, npairs: int) -> torch.Tensor:
+        n = _lib.lib().cp_bfv_mul_batch_workspace_bytes(self._h, npairs)
+        return torch.empty(((n + 15) // 16, 2), dtype=torch.int64, device="cuda")
+
+    def bfv_mul_batch(self, c, a0, a1, b0, b1, npairs, workspace, stream=None):
+        """c: (3 * npairs, k, N, 2); inputs (npairs, k, N, 2), all DGT domain."""
+        call("cp_bfv_mul_batch", self._h, _ptr(c), _ptr(a0), _ptr(a1), _ptr(b0), _ptr(b1), npairs, _ptr(workspace),
+             _stream(stream))
+
+    # ---- sampler ----
+    def sample(self, out, base, kind, seed, stream_id, npolys=None, to_dgt=True, stream=None):
+        n = out.shape[0] if npolys is None else npolys
+        call("cp_sample", self._h, _ptr(out), base, kind, int(seed), int(stream_id), n, 1 if to_dgt else 0,
+             _stream(stream))
+
+    # ---- host helpers (folded layout) ----
+    def fold(self, coeffs_per_residue: np.ndarray) -> np.ndarray:
+        """(nres, nphi) uint64 coefficient rows -> (nres, N, 2) folded layout."""
+        a = np.asarray(coeffs_per_residue, dtype=np.uint64)
+        return np.stack([a[:, : self.N], a[:, self.N:]], axis=-1)
+
+    def unfold(self, x: np.ndarray) -> np.ndarray:
+        """(..., nres, N, 2) folded -> (..., nres, nphi) coefficient rows."""
+        return np.concatenate([x[..., 0], x[..., 1]], axis=-1)

@@ -1,0 +1,162 @@
+/*
+ * cupoly_b200 -- C ABI of the B200-native cyclotomic-polynomial engine.
+ *
+ * This is the drop-in boundary for cuPoly's hot path (pdroalves/cupoly 0.3.5):
+ * the hierarchical DGT, RNS pointwise arithmetic, HPS basis extension and
+ * t/Q scaling, and the sampler.  Every entry point takes plain pointers,
+ * sizes and a CUDA stream (as void*); none allocates device memory except
+ * cp_engine_create.  Status codes are returned; the message of the last
+ * failure on the calling thread is available from cp_last_error().
+ *
+ * Data layout (cuPoly include/cuPoly/settings.h:70-80,
+ * src/arithmetic/polynomial.cu:206-217): a polynomial over a base with nres
+ * primes is `uint64_t[nres][N][2]` (N = nphi / 2 Gaussian elements per
+ * residue; element j of residue r holds (a_j mod p_r, a_{j+N} mod p_r)).
+ * Values are canonical in [0, p_r).  "DGT domain" buffers hold the forward
+ * transform in cuPoly's order (bit-reversed twisted DFT).
+ *
+ * Bases (cuPoly `enum bases`, settings.h:37): CP_QBASE = the first k primes,
+ * CP_BBASE = the next kl primes, CP_QBBASE = Q followed by B, CP_TBASE = the
+ * plaintext modulus t (one residue).
+ */
+#ifndef CUPOLY_B200_H
+#define CUPOLY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define CP_OK 0
+#define CP_ERR_INVALID 1     /* bad argument (cuPoly: assert / runtime_error) */
+#define CP_ERR_CUDA 2        /* CUDA runtime error (cuPoly: cudaCheckError -> exit) */
+#define CP_ERR_UNSUPPORTED 3 /* size/parameter outside the compiled range */
+#define CP_ERR_OOM 4         /* device allocation failed */
+#define CP_ERR_DEVICE 5      /* a kernel reported an error through the engine's flag */
+
+/* ---- enums (values equal cuPoly's) ---- */
+enum cp_base { CP_QBASE = 0, CP_BBASE = 1, CP_QBBASE = 2, CP_TBASE = 3 };
+enum cp_direction { CP_FORWARD = 0, CP_INVERSE = 1 };                 /* dgt_direction, settings.h:41 */
+enum cp_op { CP_ADD = 0, CP_SUB = 1, CP_MUL = 2, CP_MULMUL = 3, CP_ADDADD = 4 }; /* add_mode_t, settings.h:33 */
+enum cp_distribution {                                                  /* pdistributions, sampler.h:38-47 */
+  CP_DISCRETE_GAUSSIAN = 0, /* |nearbyint(3.2 Z)|, |x| <= 19 (cuPoly BFV semantics) */
+  CP_HAMMINGWEIGHT = 1,     /* exactly min(64, nphi) coefficients in {-1, +1} */
+  CP_NARROW = 2,            /* uniform {0, 1, 2} */
+  CP_ZO = 3,                /* i.i.d. -1 : 1/4, 0 : 1/2, +1 : 1/4 */
+  CP_BINARY = 4,            /* uniform {0, 1} */
+  CP_UNIFORM = 5,           /* uniform mod q_i, independent per residue */
+  CP_TERNARY = 6,           /* uniform {-1, 0, +1} (secrets) */
+  CP_GAUSSIAN = 7           /* discrete Gaussian, sigma = 3.19, |x| <= 19, signed (errors) */
+};
+/* flags of the composite scaling calls */
+#define CP_DESTROY_INPUTS 1u /* inverse-transform the inputs in place, as cuPoly does (polynomial.h:346-347) */
+
+typedef struct cp_engine cp_engine;
+
+/* ---- library ---- */
+const char* cp_version(void);
+const char* cp_last_error(void);
+
+/* ---- engine: replaces CUDAEngine::init(k, kl, M, t) / destroy() / get_n_residues(base)
+ *      (cuPoly include/cuPoly/cuda/cudaengine.h:65-123, src/cuda/cudaengine.cu:1691-1779)
+ *      and DGTEngine::init (src/cuda/dgt.cu:1694-1982).  nphi is the ring degree
+ *      (cuPoly's M), 2 <= nphi <= 65536 a power of two; kl <= 0 selects k + 1;
+ *      any t >= 2 coprime to Q (cuPoly requires a power of two).  The engine is
+ *      created on the current CUDA device.  log_radix in {3, 4} picks the DGT
+ *      register radix (0 = default). */
+int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int log_radix);
+int cp_engine_destroy(cp_engine* e);
+int cp_engine_n_residues(const cp_engine* e, int base);
+int cp_engine_nphi(const cp_engine* e);
+/* primes of the engine, Q then B (cuPoly CUDAEngine::RNSPrimes / RNSBPrimes) */
+int cp_engine_primes(const cp_engine* e, uint64_t* out, int capacity);
+/* Replace the Gaussian root xi (xi^N = i) of every residue, e.g. with cuPoly's
+ * NTHROOT[p][N] table (src/arithmetic/coprimes.cu:868), so that DGT-domain
+ * bytes match cuPoly's; xi is uint64_t[nres_QB][2].  Default: the canonical
+ * root ((u + u^-1)/2, (u - u^-1)/(2 s)), u = g^((p-1)/(4N)), s = g^((p-1)/4). */
+int cp_engine_set_nthroot(cp_engine* e, const uint64_t* xi);
+int cp_engine_get_nthroot(const cp_engine* e, uint64_t* xi_out);
+/* bytes of scratch the composite calls below need */
+size_t cp_workspace_bytes(const cp_engine* e);
+/* read and clear the engine's device error flag (synchronises `stream`) */
+int cp_engine_check(const cp_engine* e, void* stream);
+
+/* ---- DGT: replaces DGTEngine::execute_dgt(data, base, direction, ctx)
+ *      (src/cuda/dgt.cu:1069-1094).  In place on npolys consecutive polynomials
+ *      of the base (poly_stride = 0 means densely packed). */
+int cp_dgt(const cp_engine* e, void* data, int base, int direction, int npolys, int64_t poly_stride, void* stream);
+
+/* ---- pointwise, DGT domain: replace DGTEngine::execute_{add,sub,double_add,
+ *      mul_dgt_gi,mul_dgt_u64,muladd,dr2}_dgt (src/cuda/dgt.cu:1096-1499) ---- */
+int cp_add(const cp_engine* e, void* c, const void* a, const void* b, int base, void* stream);
+int cp_sub(const cp_engine* e, void* c, const void* a, const void* b, int base, void* stream);
+int cp_double_add(const cp_engine* e, void* c1, const void* a1, const void* b1, void* c2, const void* a2,
+                  const void* b2, int base, void* stream);
+int cp_mul(const cp_engine* e, void* c, const void* a, const void* b, int base, void* stream);
+int cp_mul_u64(const cp_engine* e, void* c, const void* a, const uint64_t* b, int base, void* stream);
+/* cp_mul over npolys densely packed polynomials (no counterpart in cuPoly) */
+int cp_mul_batch(const cp_engine* e, void* c, const void* a, const void* b, int base, int npolys, void* stream);
+int cp_muladd(const cp_engine* e, void* d, const void* a, const void* b, const void* c, int base, void* stream);
+int cp_dr2(const cp_engine* e, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
+           const void* c12, int base, void* stream);
+/* replace CUDAEngine::execute_polynomial_negate / _op_by_int / _double_op_by_int
+ * (src/cuda/cudaengine.cu:115-302); op is a cp_op */
+int cp_negate(const cp_engine* e, void* b, const void* a, int base, void* stream);
+int cp_op_by_int(const cp_engine* e, void* b, const void* a, int base, uint64_t x, int op, void* stream);
+int cp_double_op_by_int(const cp_engine* e, void* b1, const void* a1, void* b2, const void* a2, int base,
+                        uint64_t x1, uint64_t x2, int op, void* stream);
+
+/* ---- HPS, coefficient domain: replace CUDAEngine::execute_polynomial_basis_ext_Q_to_B /
+ *      _B_to_Q / _complex_scaling / _simple_scaling (src/cuda/cudaengine.cu:304-798).
+ *      Exact: X mod m for the unique X in [0, Q) (resp. [0, B)); round(t X / Q). */
+int cp_basis_ext_q_to_b(const cp_engine* e, void* out_b, const void* in_q, int npolys, void* stream);
+int cp_basis_ext_b_to_q(const cp_engine* e, void* out_q, const void* in_b, int npolys, void* stream);
+int cp_complex_scaling(const cp_engine* e, void* out_b, const void* in_q, const void* in_b, int npolys,
+                       void* stream);
+int cp_simple_scaling(const cp_engine* e, void* out_t, const void* in_q, void* stream);
+/* replace CUDAEngine::execute_xi_rns / execute_rho_bfv_rns (src/cuda/cudaengine.cu:992-1062):
+ * out is k polynomials over Q; polynomial i has residue i set, the rest zero */
+int cp_xi(const cp_engine* e, void* out, const void* in, void* stream);
+int cp_rho(const cp_engine* e, void* out, const void* in, void* stream);
+
+/* ---- composite polynomial calls, DGT domain in and out: replace
+ *      poly_basis_extension_Q_to_B / _Q_to_QB / _B_to_Q, poly_complex_scaling_tDivQ,
+ *      poly_simple_scaling_tDivQ (src/arithmetic/polynomial.cu:310-527).
+ *      `workspace` holds cp_workspace_bytes(e) bytes of device memory. */
+int cp_poly_basis_extension_q_to_b(const cp_engine* e, void* out_b, const void* in_q, void* workspace,
+                                   void* stream);
+int cp_poly_basis_extension_q_to_qb(const cp_engine* e, void* out_qb, const void* in_q, void* workspace,
+                                    void* stream);
+int cp_poly_basis_extension_b_to_q(const cp_engine* e, void* out_q, const void* in_b, void* workspace,
+                                   void* stream);
+int cp_poly_complex_scaling_tdivq(const cp_engine* e, void* out_q, void* in_q, void* in_b, unsigned flags,
+                                  void* workspace, void* stream);
+int cp_poly_simple_scaling_tdivq(const cp_engine* e, void* out_t, const void* in_q, void* workspace, void* stream);
+
+/* ---- BFV homomorphic multiplication kernel chain (BASELINE configuration 2's
+ *      step): (c0, c1, c2) = round(t/Q * (a0 + a1 s)(b0 + b1 s)) in Q, all DGT domain.
+ *      cp_bfv_mul is the plain per-call composition of the calls above, in cuPoly's
+ *      order (src/arithmetic/polynomial.cu:350-527, 951-999). ---- */
+int cp_bfv_mul(const cp_engine* e, void* c0, void* c1, void* c2, const void* a0, const void* a1, const void* b0,
+               const void* b1, void* workspace, void* stream);
+/* Batched form of the same chain: npairs ciphertext pairs per call, each input
+ * uint64_t[npairs][k][N][2] (DGT domain), output c = uint64_t[3][npairs][k][N][2]
+ * (c0 of every pair, then c1, then c2).  No counterpart in cuPoly (one
+ * parameter set and one polynomial per call there). */
+size_t cp_bfv_mul_batch_workspace_bytes(const cp_engine* e, int npairs);
+int cp_bfv_mul_batch(const cp_engine* e, void* c, const void* a0, const void* a1, const void* b0, const void* b1,
+                     int npairs, void* workspace, void* stream);
+
+/* ---- sampler: replaces Sampler::sample(ctx, p, kind) (src/cuda/sampler.cu:576-645).
+ *      npolys consecutive polynomials over `base` with stream ids stream_id ..
+ *      stream_id + npolys - 1; to_dgt != 0 applies the forward DGT (cuPoly does). */
+int cp_sample(const cp_engine* e, void* out, int base, int kind, uint64_t seed, uint32_t stream_id, int npolys,
+              int to_dgt, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUPOLY_B200_H */

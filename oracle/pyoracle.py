@@ -1,0 +1,457 @@
+"""Pure-Python big-integer oracle for cuPoly's hot path -- TEST INFRASTRUCTURE ONLY.
+
+Every function restates one piece of cuPoly (pdroalves/cupoly 0.3.5) from its
+mathematics; the citation in each docstring is the reference file:line the
+behaviour follows.  Nothing here is imported by the product package.
+
+Conventions (cuPoly ``include/cuPoly/settings.h:70-80``,
+``src/arithmetic/polynomial.cu:206-217``):
+  * a ring element has ``nphi`` coefficients, ``N = nphi // 2``;
+  * one residue is a list of N Gaussian integers ``(re, im)`` with
+    ``re = a_j mod p`` and ``im = a_{j+N} mod p`` ("folded" encoding);
+  * a polynomial over a base is residue-major: ``[nres][N]``.
+"""
+from __future__ import annotations
+
+import os
+import re as _re
+from functools import lru_cache
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_PRIME_HEADER = os.path.join(_HERE, "..", "cupoly_b200", "csrc", "prime_table.h")
+_CDT_HEADER = os.path.join(_HERE, "..", "cupoly_b200", "csrc", "cdt_table.h")
+
+
+# ----------------------------------------------------------------------------
+# Parameters
+# ----------------------------------------------------------------------------
+def _load_prime_table():
+    src = open(_PRIME_HEADER).read()
+    p = _re.search(r"kPrimes\[kNumPrimes\]\s*=\s*\{([^}]*)\}", src).group(1)
+    g = _re.search(r"kPrimitiveRoots\[kNumPrimes\]\s*=\s*\{([^}]*)\}", src).group(1)
+    primes = [int(x.strip().rstrip("ULL")) for x in p.split(",") if x.strip()]
+    roots = [int(x) for x in g.split(",") if x.strip()]
+    return primes, roots
+
+
+PRIMES, PROOTS = _load_prime_table()
+PROOT = dict(zip(PRIMES, PROOTS))
+
+
+def bases(k: int, kl: int):
+    """Q = first k primes, B = next kl primes (cuPoly ``src/cuda/cudaengine.cu:1265-1290``)."""
+    return PRIMES[:k], PRIMES[k:k + kl]
+
+
+def prod(xs):
+    r = 1
+    for x in xs:
+        r *= x
+    return r
+
+
+# ----------------------------------------------------------------------------
+# Gaussian-integer arithmetic mod p (cuPoly ``src/cuda/dgt.cu:527-570``)
+# ----------------------------------------------------------------------------
+def gi_add(a, b, p):
+    return ((a[0] + b[0]) % p, (a[1] + b[1]) % p)
+
+
+def gi_sub(a, b, p):
+    return ((a[0] - b[0]) % p, (a[1] - b[1]) % p)
+
+
+def gi_mul(a, b, p):
+    """(a0 + a1 i)(b0 + b1 i) mod p; cuPoly computes it with Karatsuba (dgt.cu:547-570)."""
+    return ((a[0] * b[0] - a[1] * b[1]) % p, (a[0] * b[1] + a[1] * b[0]) % p)
+
+
+def gi_pow(a, e, p):
+    r = (1, 0)
+    while e:
+        if e & 1:
+            r = gi_mul(r, a, p)
+        a = gi_mul(a, a, p)
+        e >>= 1
+    return r
+
+
+def gi_scale(a, w, p):
+    return (a[0] * w % p, a[1] * w % p)
+
+
+# ----------------------------------------------------------------------------
+# Roots
+# ----------------------------------------------------------------------------
+def omega(p: int, n: int) -> int:
+    """Primitive n-th root of unity PROOT^((p-1)/n).
+
+    cuPoly derives every DGT twiddle from the tabulated primitive root:
+    stage twiddles from g = PROOT^((p-1)/(2S)) (``dgt.cu:1532-1533``) and the
+    inter-pass twiddles from PROOT^((p-1)/N) (``dgt.cu:1920-1932``).
+    """
+    assert (p - 1) % n == 0
+    return pow(PROOT[p], (p - 1) // n, p)
+
+
+def canonical_xi(p: int, n: int):
+    """A Gaussian xi with xi^n = i, chosen canonically.
+
+    Z_p[i] is isomorphic to Z_p x Z_p through a+bi -> (a + b s, a - b s)
+    with s = PROOT^((p-1)/4).  With u = PROOT^((p-1)/(4n)) (so u^n = s),
+    the pair (u, u^-1) maps back to xi = ((u + u^-1)/2, (u - u^-1)/(2s)).
+    The family is consistent: canonical_xi(p, 2n)^2 == canonical_xi(p, n).
+    cuPoly instead uses tabulated roots (``NTHROOT``, ``coprimes.cu:868``);
+    any xi with xi^n = i gives the same coefficient-domain results.
+    """
+    assert (p - 1) % (4 * n) == 0
+    s = pow(PROOT[p], (p - 1) // 4, p)
+    u = pow(PROOT[p], (p - 1) // (4 * n), p)
+    ui = pow(u, p - 2, p)
+    inv2 = (p + 1) // 2
+    re = (u + ui) * inv2 % p
+    im = (u - ui) * inv2 % p * pow(s, p - 2, p) % p
+    return (re, im)
+
+
+def brev(x: int, bits: int) -> int:
+    r = 0
+    for _ in range(bits):
+        r = (r << 1) | (x & 1)
+        x >>= 1
+    return r
+
+
+def hdgt_split(N: int):
+    """(Na, Nb) factorisation of cuPoly's hierarchical DGT (``include/cuPoly/cuda/dgt.h:41-50``)."""
+    return {1024: (32, 32), 2048: (64, 32), 4096: (64, 64), 8192: (128, 64),
+            16384: (128, 128), 32768: (256, 128)}.get(N)
+
+
+# ----------------------------------------------------------------------------
+# DGT: bit-exact restatement of cuPoly's kernels
+# ----------------------------------------------------------------------------
+def _gs_dif(x, p, S):
+    """In-place S-point Gentleman-Sande DIF (``dgt.cu:681-714, 757-777``).
+
+    Stage s pairs (i, i+m), m = S >> (s+1), and multiplies the difference by
+    w_S^(j 2^s) with j = i mod m; w_S = PROOT^((p-1)/S).  Output is in
+    bit-reversed order.
+    """
+    w = omega(p, S)
+    logS = S.bit_length() - 1
+    for s in range(logS):
+        m = S >> (s + 1)
+        for cid in range(S // 2):
+            j = cid * 2 * m // S
+            i = j + (cid % (S // (2 * m))) * 2 * m
+            a, b = x[i], x[i + m]
+            x[i] = gi_add(a, b, p)
+            x[i + m] = gi_scale(gi_sub(a, b, p), pow(w, j << s, p), p)
+
+
+def _ct_dit_inv(x, p, S):
+    """In-place S-point Cooley-Tukey inverse with inverse twiddles, unscaled (``dgt.cu:716-753, 782-805``)."""
+    wi = pow(omega(p, S), p - 2, p)
+    logS = S.bit_length() - 1
+    for s in range(logS - 1, -1, -1):
+        m = S >> (s + 1)
+        for cid in range(S // 2):
+            j = cid * 2 * m // S
+            i = j + (cid % (S // (2 * m))) * 2 * m
+            a, b = x[i], gi_scale(x[i + m], pow(wi, j << s, p), p)
+            x[i] = gi_add(a, b, p)
+            x[i + m] = gi_sub(a, b, p)
+
+
+def dgt_forward_ref(x, p, xi=None):
+    """cuPoly's forward DGT of one residue (``dgt.cu:819-908``, dispatch ``:107-205``).
+
+    For N >= 1024 it is the two-pass hierarchical transform with N = Na*Nb:
+    pass 1 (``hdgt_tr<Nb>``) twists column b by xi^(t Na + b) and runs an
+    Nb-point DIF, writing tmp[b Nb + t]; pass 2 (``hdgt_tr<Na>``) multiplies
+    tmp[t Nb + c] by g_N^(t brev_Nb(c)) and runs an Na-point DIF, writing
+    out[c Na + t].  For N <= 512 it is one twisted N-point DIF (``dgt<N>``).
+    """
+    N = len(x)
+    xi = canonical_xi(p, N) if xi is None else xi
+    split = hdgt_split(N)
+    if split is None:
+        y = [gi_mul(x[n], gi_pow(xi, n, p), p) for n in range(N)]
+        _gs_dif(y, p, N)
+        return y
+    Na, Nb = split
+    gN = omega(p, N)
+    lb = Nb.bit_length() - 1
+    tmp = [None] * N
+    for b in range(Na):
+        col = [gi_mul(x[t * Na + b], gi_pow(xi, t * Na + b, p), p) for t in range(Nb)]
+        _gs_dif(col, p, Nb)
+        for t in range(Nb):
+            tmp[t + b * Nb] = col[t]
+    out = [None] * N
+    for c in range(Nb):
+        col = [gi_scale(tmp[t * Nb + c], pow(gN, t * brev(c, lb), p), p) for t in range(Na)]
+        _gs_dif(col, p, Na)
+        for t in range(Na):
+            out[t + c * Na] = col[t]
+    return out
+
+
+def dgt_inverse_ref(X, p, xi=None):
+    """cuPoly's inverse DGT of one residue (``dgt.cu:917-1006``; tables ``:1879-1960``).
+
+    Pass 1 (``hidgt<Na>``): contiguous rows c, Na-point CT inverse, times
+    g_N^-(brev_Nb(c) t) (Na Nb)^-1.  Pass 2 (``hidgt_tr<Nb>``): columns of
+    stride Na, Nb-point CT inverse, times xi^-(t Na + b).  For N <= 512 the
+    single-block inverse folds N^-1 into the untwist (``dgt.cu:1654-1662``).
+    """
+    N = len(X)
+    xi = canonical_xi(p, N) if xi is None else xi
+    xii = gi_pow(xi, 4 * N - 1, p)  # xi has order 4N
+    ninv = pow(N, p - 2, p)
+    split = hdgt_split(N)
+    if split is None:
+        y = list(X)
+        _ct_dit_inv(y, p, N)
+        return [gi_scale(gi_mul(y[n], gi_pow(xii, n, p), p), ninv, p) for n in range(N)]
+    Na, Nb = split
+    gNi = pow(omega(p, N), p - 2, p)
+    lb = Nb.bit_length() - 1
+    tmp = [None] * N
+    for c in range(Nb):
+        row = list(X[c * Na:(c + 1) * Na])
+        _ct_dit_inv(row, p, Na)
+        for t in range(Na):
+            tmp[c * Na + t] = gi_scale(row[t], pow(gNi, brev(c, lb) * t, p) * ninv % p, p)
+    out = [None] * N
+    for b in range(Na):
+        col = [tmp[t * Na + b] for t in range(Nb)]
+        _ct_dit_inv(col, p, Nb)
+        for t in range(Nb):
+            out[t * Na + b] = gi_mul(col[t], gi_pow(xii, t * Na + b, p), p)
+    return out
+
+
+def dgt_forward_direct(x, p, xi=None):
+    """O(N^2) definition: out[pos] = sum_n x[n] xi^n w_N^(n brev(pos)).
+
+    The DGT domain of cuPoly is the twisted DFT of the folded signal stored in
+    bit-reversed order, independent of the Na x Nb split.
+    """
+    N = len(x)
+    xi = canonical_xi(p, N) if xi is None else xi
+    w = omega(p, N)
+    bits = N.bit_length() - 1
+    tw = [gi_mul(x[n], gi_pow(xi, n, p), p) for n in range(N)]
+    out = []
+    for pos in range(N):
+        k = brev(pos, bits)
+        acc = (0, 0)
+        for n in range(N):
+            acc = gi_add(acc, gi_scale(tw[n], pow(w, n * k % N, p), p), p)
+        out.append(acc)
+    return out
+
+
+# ----------------------------------------------------------------------------
+# Folding, polynomial products
+# ----------------------------------------------------------------------------
+def fold(coeffs, p, N):
+    """a_j -> (a_j mod p, a_{j+N} mod p) (``polynomial.cu:206-217``)."""
+    c = list(coeffs) + [0] * (2 * N - len(coeffs))
+    return [(c[j] % p, c[j + N] % p) for j in range(N)]
+
+
+def unfold(res):
+    N = len(res)
+    return [res[j][0] for j in range(N)] + [res[j][1] for j in range(N)]
+
+
+def negacyclic_mul_schoolbook(a, b, p):
+    """c = a*b mod (x^n + 1, p): the definition cuPoly's tests check against NTL
+    (``tests/unit_tests/test_bfv_mode.cu:1180-1208``)."""
+    n = len(a)
+    c = [0] * n
+    for i, ai in enumerate(a):
+        if ai == 0:
+            continue
+        for j, bj in enumerate(b):
+            k = i + j
+            if k < n:
+                c[k] += ai * bj
+            else:
+                c[k - n] -= ai * bj
+    return [x % p for x in c]
+
+
+def polymul_dgt(a, b, p, xi=None):
+    """fold -> forward DGT x2 -> pointwise GIMul -> inverse DGT -> unfold."""
+    N = len(a) // 2
+    A = dgt_forward_ref(fold(a, p, N), p, xi)
+    B = dgt_forward_ref(fold(b, p, N), p, xi)
+    C = [gi_mul(x, y, p) for x, y in zip(A, B)]
+    return unfold(dgt_inverse_ref(C, p, xi))
+
+
+# ----------------------------------------------------------------------------
+# CRT and the exact HPS definitions
+# ----------------------------------------------------------------------------
+def crt(residues, primes):
+    """The unique X in [0, prod(primes)) with X = r_i mod p_i."""
+    M = prod(primes)
+    x = 0
+    for r, p in zip(residues, primes):
+        Mi = M // p
+        x += r * pow(Mi % p, p - 2, p) % p * Mi
+    return x % M
+
+
+def basis_extension_exact(xs, src, dst):
+    """X mod d_j for X = crt(xs, src) in [0, prod(src)).
+
+    cuPoly computes this with a floating-point correction v
+    (``src/cuda/cudaengine.cu:483-649, 659-796``); its tests assert the exact
+    value (``tests/unit_tests/test_bfv_mode.cu:640-730``).
+    """
+    X = crt(xs, src)
+    return [X % d for d in dst]
+
+
+def complex_scaling_exact(xq, yb, Q, B, t):
+    """round(t X / Q) mod b_j for X = crt(xq ++ yb, Q ++ B) in [0, Q B).
+
+    cuPoly's HPS complex scaling (``src/cuda/cudaengine.cu:382-469``) targets
+    this value; t X / Q is never a half-integer because Q is odd.
+    """
+    Qp = prod(Q)
+    X = crt(list(xq) + list(yb), list(Q) + list(B))
+    r = (2 * t * X + Qp) // (2 * Qp)
+    return [r % b for b in B]
+
+
+def complex_scaling_tdivq_exact(xq, yb, Q, B, t):
+    """((round(t X / Q) mod B) mod q_i): ``poly_complex_scaling_tDivQ`` (``polynomial.cu:350-404``)."""
+    Qp, Bp = prod(Q), prod(B)
+    X = crt(list(xq) + list(yb), list(Q) + list(B))
+    r = (2 * t * X + Qp) // (2 * Qp) % Bp
+    return [r % q for q in Q]
+
+
+def simple_scaling_exact(xq, Q, t):
+    """round(t X / Q) mod t for X = crt(xq, Q) (``cudaengine.cu:323-380``; test ``test_bfv_mode.cu:938-983``)."""
+    Qp = prod(Q)
+    X = crt(xq, Q)
+    return (2 * t * X + Qp) // (2 * Qp) % t
+
+
+# ----------------------------------------------------------------------------
+# Sampler: Philox4x32-10 and the distributions of the device sampler
+# ----------------------------------------------------------------------------
+_M = 0xFFFFFFFF
+
+
+def philox4x32_10(ctr, key):
+    """Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11, "Parallel random numbers:
+    as easy as 1, 2, 3").  Returns four 32-bit words."""
+    c0, c1, c2, c3 = ctr
+    k0, k1 = key
+    for _ in range(10):
+        p0 = 0xD2511F53 * c0
+        p1 = 0xCD9E8D57 * c2
+        hi0, lo0 = p0 >> 32, p0 & _M
+        hi1, lo1 = p1 >> 32, p1 & _M
+        c0, c1, c2, c3 = (hi1 ^ c1 ^ k0) & _M, lo1, (hi0 ^ c3 ^ k1) & _M, lo0
+        k0 = (k0 + 0x9E3779B9) & _M
+        k1 = (k1 + 0xBB67AE85) & _M
+    return c0, c1, c2, c3
+
+
+def load_cdt(name):
+    """Read one cumulative table (uint64 thresholds) from cdt_table.h."""
+    src = open(_CDT_HEADER).read()
+    m = _re.search(name + r"\[\]\s*=\s*\{([^}]*)\}", src)
+    return [int(x.strip().rstrip("ULL")) for x in m.group(1).split(",") if x.strip()]
+
+
+# Distribution kinds of the device sampler (values of enum cp_distribution).
+DISCRETE_GAUSSIAN, HAMMINGWEIGHT, NARROW, ZO, BINARY, UNIFORM, TERNARY, GAUSSIAN = range(8)
+
+
+def _cdt_lookup(u63, cdt):
+    return sum(1 for t in cdt if u63 >= t)
+
+
+def sample_small(kind, c, sid, seed):
+    """Signed value of coefficient c for the residue-independent kinds.
+
+    Restates the device sampler: Philox4x32-10 with key (seed_lo, seed_hi) and
+    counter (c, draw, stream id, kind).  cuPoly's kinds (src/cuda/sampler.cu:
+    73-493): NARROW {0,1,2}, BINARY {0,1}, DISCRETE_GAUSSIAN |round(3.2 Z)|;
+    ZO is i.i.d. (cuPoly fixes exactly half the coefficients nonzero).
+    """
+    k0, k1 = seed & _M, (seed >> 32) & _M
+    if kind in (NARROW, TERNARY):
+        for d in range(8):
+            for w in philox4x32_10((c, d, sid, kind), (k0, k1)):
+                if w != 0xFFFFFFFF:
+                    x = w % 3
+                    return -1 if (kind == TERNARY and x == 2) else x
+        raise RuntimeError("rejection limit")
+    r = philox4x32_10((c, 0, sid, kind), (k0, k1))
+    u63 = ((r[1] & 0x7FFFFFFF) << 32) | r[0]
+    if kind == BINARY:
+        return r[0] & 1
+    if kind == ZO:
+        b = r[0] & 3
+        return 0 if b < 2 else (1 if b == 2 else -1)
+    if kind == DISCRETE_GAUSSIAN:
+        return _cdt_lookup(u63, load_cdt("kCdtFolded"))
+    if kind == GAUSSIAN:
+        m = _cdt_lookup(u63, load_cdt("kCdtSigned"))
+        return -m if (r[2] & 1) else m
+    raise ValueError(kind)
+
+
+def sample_uniform(c, r, p, sid, seed):
+    """Uniform residue mod p of coefficient c in residue r (rejection on 63 bits)."""
+    k0, k1 = seed & _M, (seed >> 32) & _M
+    for d in range(8):
+        q = philox4x32_10((c, r * 8 + d, sid, UNIFORM), (k0, k1))
+        u0 = ((q[1] & 0x7FFFFFFF) << 32) | q[0]
+        u1 = ((q[3] & 0x7FFFFFFF) << 32) | q[2]
+        if u0 < p:
+            return u0
+        if u1 < p:
+            return u1
+    raise RuntimeError("rejection limit")
+
+
+def sample_hamming(nphi, sid, seed, h=64):
+    """{position: +-1} with exactly min(h, nphi) entries (cuPoly HAMMINGWEIGHT_H = 64, settings.h:43)."""
+    k0, k1 = seed & _M, (seed >> 32) & _M
+    lg = nphi.bit_length() - 1
+    out = {}
+    for i in range(min(h, nphi)):
+        for d in range(1024):
+            q = philox4x32_10((i, d, sid, HAMMINGWEIGHT), (k0, k1))
+            pos = (q[0] >> (32 - lg)) if lg else 0
+            if pos not in out:
+                out[pos] = -1 if (q[1] & 1) else 1
+                break
+    return out
+
+
+def sample_poly(kind, primes, nphi, sid, seed):
+    """(nres, nphi) coefficient rows the device sampler produces."""
+    rows = []
+    if kind == UNIFORM:
+        return [[sample_uniform(c, r, p, sid, seed) for c in range(nphi)] for r, p in enumerate(primes)]
+    if kind == HAMMINGWEIGHT:
+        hw = sample_hamming(nphi, sid, seed)
+        vals = [hw.get(c, 0) for c in range(nphi)]
+    else:
+        vals = [sample_small(kind, c, sid, seed) for c in range(nphi)]
+    for p in primes:
+        rows.append([v % p for v in vals])
+    return rows

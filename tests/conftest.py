@@ -1,0 +1,23 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); run with -m gpu")
+
+
+@pytest.fixture(scope="session")
+def gpu():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU test run without a CUDA device"
+    import cupoly_b200
+
+    cupoly_b200.native_library()
+    return torch.device("cuda:0")

@@ -1,0 +1,64 @@
+"""The C ABI library loads, exports every declared symbol, and rejects invalid
+arguments with status codes (cuPoly: assert / runtime_error / exit) -- no GPU."""
+import ctypes as C
+import subprocess
+
+import pytest
+
+import cupoly_b200
+from cupoly_b200 import _lib
+
+
+def test_library_loads_and_versions():
+    L = cupoly_b200.native_library()
+    assert L.cp_version().startswith(b"cupoly_b200")
+
+
+def test_every_header_symbol_is_exported():
+    names = _lib.header_functions()
+    assert len(names) >= 30
+    L = _lib.lib()
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(_lib.SIGNATURES), set(names) ^ set(_lib.SIGNATURES)
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert set(names) <= exported
+
+
+def test_no_torch_dependency_in_native_library():
+    out = subprocess.run(["ldd", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    assert "torch" not in out and "c10" not in out
+
+
+@pytest.mark.parametrize("args, fragment", [
+    ((0, 1, 4096, 256, 0), "k must be"),
+    ((25, 1, 4096, 256, 0), "k must be"),
+    ((2, 25, 4096, 256, 0), "kl must be"),
+    ((2, 3, 3000, 256, 0), "power of two"),
+    ((2, 3, 131072, 256, 0), "power of two"),
+    ((2, 3, 4096, 1, 0), "t must be"),
+    ((2, 3, 4096, 256, 5), "log_radix"),
+])
+def test_engine_create_rejects_bad_parameters(args, fragment):
+    L = _lib.lib()
+    h = C.c_void_p()
+    rc = L.cp_engine_create(C.byref(h), *args)
+    assert rc == 1 and not h.value
+    assert fragment in L.cp_last_error().decode()
+
+
+def test_null_engine_calls_fail_cleanly():
+    L = _lib.lib()
+    assert L.cp_dgt(None, None, 0, 0, 1, 0, None) == 1
+    assert L.cp_add(None, None, None, None, 0, None) == 1
+    assert L.cp_bfv_mul(None, None, None, None, None, None, None, None, None, None) == 1
+    assert L.cp_engine_n_residues(None, 0) == -1
+    assert L.cp_workspace_bytes(None) == 0
+    assert L.cp_engine_destroy(None) == 0
+
+
+def test_status_error_raises():
+    with pytest.raises(_lib.CupolyError) as ei:
+        _lib.call("cp_add", None, None, None, None, 0, None)
+    assert ei.value.code == 1

@@ -1,0 +1,193 @@
+"""Pointwise arithmetic and cuPoly's TestArithmetic / TestRNS ports on the GPU.
+
+The reference's parameter grid is (logq2, nphi) with k = ceil(logq2 / 63),
+kl = k + 1, t = 256 (tests/unit_tests/test_bfv_mode.cu:1492-1508)."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import coracle as CO
+from oracle import pyoracle as O
+from tests.common import fold, random_poly_residues, unfold
+
+pytestmark = pytest.mark.gpu
+
+GRID = [(30, 32), (120, 32), (340, 32), (120, 256), (30, 2048), (340, 2048), (170, 4096), (340, 8192)]
+
+
+def _ref_engine(logq2, nphi):
+    from cupoly_b200 import cupoly as cp
+    k = math.ceil(logq2 / 63)
+    cp.CUDAEngine.init(k, k + 1, nphi, 256)
+    ctx = cp.Context()
+    cp.Sampler.init(ctx)
+    return cp, ctx
+
+
+def _gi_mul(a, b, p):
+    """Exact Gaussian product of folded arrays (numpy object ints)."""
+    ar, ai = a[..., 0].astype(object), a[..., 1].astype(object)
+    br, bi = b[..., 0].astype(object), b[..., 1].astype(object)
+    return np.stack([(ar * br - ai * bi) % p, (ar * bi + ai * br) % p], -1).astype(np.uint64)
+
+
+def test_pointwise_ops_vs_exact(gpu):
+    from cupoly_b200.engine import ADD, MUL, MULMUL, ADDADD, SUB, Engine, from_u64, to_u64
+    e = Engine(3, 4, 2048, 256)
+    for base in (0, 1, 2):
+        primes = e.base_primes(base)
+        P = np.array(primes, dtype=object)[:, None]
+        xs = [fold(random_poly_residues(10 * base + i, primes, 2048))[None] for i in range(4)]
+        a, b, c, d = (from_u64(x) for x in xs)
+        A, Bv, Cv, D = (x[0].astype(object) for x in xs)
+        out, out2, out3 = e.empty(base), e.empty(base), e.empty(base)
+
+        e.add(out, a, b, base)
+        assert np.array_equal(to_u64(out)[0], ((A + Bv) % P[..., None]).astype(np.uint64))
+        e.sub(out, a, b, base)
+        assert np.array_equal(to_u64(out)[0], ((A - Bv) % P[..., None]).astype(np.uint64))
+        e.mul(out, a, b, base)
+        ref_mul = np.stack([_gi_mul(xs[0][0, r], xs[1][0, r], p) for r, p in enumerate(primes)])
+        assert np.array_equal(to_u64(out)[0], ref_mul)
+        e.muladd(out, a, b, c, base)
+        assert np.array_equal(to_u64(out)[0], ((ref_mul.astype(object) + Cv) % P[..., None]).astype(np.uint64))
+        e.dr2(out, out2, out3, a, b, c, d, base)
+        r21 = np.stack([_gi_mul(xs[0][0, r], xs[2][0, r], p) for r, p in enumerate(primes)])
+        r22 = np.stack([(_gi_mul(xs[0][0, r], xs[3][0, r], p).astype(object) +
+                         _gi_mul(xs[1][0, r], xs[2][0, r], p).astype(object)) % p for r, p in enumerate(primes)])
+        r23 = np.stack([_gi_mul(xs[1][0, r], xs[3][0, r], p) for r, p in enumerate(primes)])
+        assert np.array_equal(to_u64(out)[0], r21)
+        assert np.array_equal(to_u64(out2)[0], r22.astype(np.uint64))
+        assert np.array_equal(to_u64(out3)[0], r23)
+        e.double_add(out, a, b, out2, c, d, base)
+        assert np.array_equal(to_u64(out)[0], ((A + Bv) % P[..., None]).astype(np.uint64))
+        assert np.array_equal(to_u64(out2)[0], ((Cv + D) % P[..., None]).astype(np.uint64))
+        e.negate(out, a, base)
+        assert np.array_equal(to_u64(out)[0], ((-A) % P[..., None]).astype(np.uint64))
+        for x in (0, 7, 2 ** 64 - 1):
+            e.op_by_int(out, a, base, x, ADD)
+            exp = A.copy()
+            exp[..., 0] = (exp[..., 0] + x) % P
+            assert np.array_equal(to_u64(out)[0], exp.astype(np.uint64))
+            e.op_by_int(out, a, base, x, SUB)
+            exp = A.copy()
+            exp[..., 0] = (exp[..., 0] - x) % P
+            assert np.array_equal(to_u64(out)[0], exp.astype(np.uint64))
+            e.op_by_int(out, a, base, x, MUL)
+            assert np.array_equal(to_u64(out)[0], ((A * x) % P[..., None]).astype(np.uint64))
+        e.double_op_by_int(out, a, out2, b, base, 5, 9, MULMUL)
+        assert np.array_equal(to_u64(out)[0], ((A * 5) % P[..., None]).astype(np.uint64))
+        assert np.array_equal(to_u64(out2)[0], ((Bv * 9) % P[..., None]).astype(np.uint64))
+        e.double_op_by_int(out, a, out2, b, base, 5, 9, ADDADD)
+        exp = A.copy()
+        exp[..., 0] = (exp[..., 0] + 5) % P
+        assert np.array_equal(to_u64(out)[0], exp.astype(np.uint64))
+        u64 = random_poly_residues(99, primes, 1024)  # (nres, N) multipliers
+        bu = from_u64(u64)
+        e.mul_u64(out, a, bu, base)
+        assert np.array_equal(to_u64(out)[0], ((A * u64.astype(object)[..., None]) % P[..., None]).astype(np.uint64))
+
+
+@pytest.mark.parametrize("nphi,k", [(2048, 2), (4096, 2), (8192, 5), (16384, 3), (32768, 2), (65536, 1)])
+def test_polymul_vs_oracle(gpu, nphi, k):
+    """forward DGT x2, pointwise, inverse: the negacyclic product per prime."""
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine, from_u64, to_u64
+    e = Engine(k, 0, nphi, 256)
+    a = random_poly_residues(1, e.Q, nphi)
+    b = random_poly_residues(2, e.Q, nphi)
+    ta, tb = from_u64(fold(a)[None]), from_u64(fold(b)[None])
+    e.dgt(ta, 0, FORWARD)
+    e.dgt(tb, 0, FORWARD)
+    tc = e.empty(0)
+    e.mul(tc, ta, tb, 0)
+    e.dgt(tc, 0, INVERSE)
+    c = unfold(to_u64(tc))[0]
+    assert np.array_equal(c, CO.polymul(a[None], b[None], e.Q)[0])
+    if nphi == 2048:
+        assert c[0].tolist() == O.negacyclic_mul_schoolbook(a[0].tolist(), b[0].tolist(), e.Q[0])
+
+
+@pytest.mark.parametrize("logq2,nphi", GRID)
+def test_reference_arithmetic(gpu, logq2, nphi):
+    """cuPoly TestArithmetic.{Add, Sub, Mul, MulAdd, MulByInt, SetCoeff} and TestRNS.RNS."""
+    cp, ctx = _ref_engine(logq2, nphi)
+    q = cp.CUDAEngine.RNSProduct
+    a, b, c, d, s = cp.poly_t(), cp.poly_t(), cp.poly_t(), cp.poly_t(), cp.poly_t()
+    for x in (a, b, c):
+        cp.poly_init(ctx, x)
+        cp.Sampler.sample(ctx, x, cp.UNIFORM)
+    A = [cp.poly_get_coeff(ctx, a, i) for i in range(nphi)]
+    Bc = [cp.poly_get_coeff(ctx, b, i) for i in range(nphi)]
+    Cc = [cp.poly_get_coeff(ctx, c, i) for i in range(nphi)]
+    assert all(0 <= v < q for v in A)
+    cp.poly_add(ctx, d, a, b)
+    assert [cp.poly_get_coeff(ctx, d, i) for i in range(nphi)] == [(x + y) % q for x, y in zip(A, Bc)]
+    cp.poly_sub(ctx, d, a, b)
+    assert [cp.poly_get_coeff(ctx, d, i) for i in range(nphi)] == [(x - y) % q for x, y in zip(A, Bc)]
+    m = cp.poly_t()
+    cp.poly_mul(ctx, m, a, b)
+    got = [cp.poly_get_coeff(ctx, m, i) for i in range(nphi)]
+    ref = np.array([[v % p for v in A] for p in cp.CUDAEngine.RNSPrimes], dtype=np.uint64)
+    refb = np.array([[v % p for v in Bc] for p in cp.CUDAEngine.RNSPrimes], dtype=np.uint64)
+    prod_rows = CO.polymul(ref[None], refb[None], cp.CUDAEngine.RNSPrimes)[0]
+    exp = [O.crt(prod_rows[:, i].tolist(), cp.CUDAEngine.RNSPrimes) for i in range(nphi)]
+    assert got == exp
+    ma = cp.poly_t()
+    cp.poly_mul_add(ctx, ma, a, b, c)
+    assert [cp.poly_get_coeff(ctx, ma, i) for i in range(nphi)] == [(x + y) % q for x, y in zip(exp, Cc)]
+    mi = cp.poly_t()
+    cp.poly_mul_int(ctx, mi, a, 77)
+    assert [cp.poly_get_coeff(ctx, mi, i) for i in range(nphi)] == [x * 77 % q for x in A]
+    cp.poly_init(ctx, s)
+    cp.poly_set_coeff(ctx, s, 0, 42)
+    assert cp.poly_get_coeff(ctx, s, 0) == 42
+    ones = cp.poly_t()
+    cp.poly_init(ctx, ones)
+    for i in range(nphi):
+        cp.poly_set_coeff(ctx, ones, i, 1)
+    cp.poly_copy_to_device(ctx, ones)
+    ones.status = cp.RNSSTATE
+    cp.poly_copy_to_host(ctx, ones)
+    assert [cp.poly_get_coeff(ctx, ones, i) for i in range(nphi)] == [1] * nphi
+    assert cp.poly_get_coeff(ctx, ones, 2 * nphi - 1) == 0
+    cp.CUDAEngine.destroy()
+
+
+@pytest.mark.parametrize("logq2,nphi", [(120, 32), (170, 4096)])
+def test_reference_mul_base_b(gpu, logq2, nphi):
+    """cuPoly TestArithmetic.MulBaseB: extend both operands to B, multiply in B."""
+    cp, ctx = _ref_engine(logq2, nphi)
+    e = cp.CUDAEngine.engine
+    aq, bq, ab, bb, cb = (cp.poly_t() for _ in range(5))
+    for x in (aq, bq):
+        cp.poly_init(ctx, x)
+        cp.Sampler.sample(ctx, x, cp.UNIFORM)
+    A = [cp.poly_get_coeff(ctx, aq, i) for i in range(nphi)]
+    Bc = [cp.poly_get_coeff(ctx, bq, i) for i in range(nphi)]
+    cp.poly_basis_extension_Q_to_B(ctx, ab, aq)
+    cp.poly_basis_extension_Q_to_B(ctx, bb, bq)
+    cp.poly_mul(ctx, cb, ab, bb)
+    from cupoly_b200.engine import INVERSE, to_u64
+    for poly, vals in ((ab, A), (bb, Bc)):
+        t = poly.d_coefs.clone()
+        e.dgt(t, 1, INVERSE, stream=ctx.stream)
+        got = unfold(to_u64(t))[0]
+        assert np.array_equal(got, np.array([[v % p for v in vals] for p in e.B], dtype=np.uint64))
+    t = cb.d_coefs.clone()
+    e.dgt(t, 1, INVERSE, stream=ctx.stream)
+    rows_a = np.array([[v % p for v in A] for p in e.B], dtype=np.uint64)
+    rows_b = np.array([[v % p for v in Bc] for p in e.B], dtype=np.uint64)
+    assert np.array_equal(unfold(to_u64(t))[0], CO.polymul(rows_a[None], rows_b[None], e.B)[0])
+    cp.CUDAEngine.destroy()
+
+
+def test_engines_coexist(gpu):
+    """Several parameter sets at once (cuPoly holds one per process)."""
+    from cupoly_b200.engine import FORWARD, Engine, from_u64, to_u64
+    engines = [Engine(k, 0, nphi, 256) for k, nphi in [(1, 2048), (4, 8192), (2, 32768)]]
+    for e in engines:
+        x = fold(random_poly_residues(e.nphi, e.Q, e.nphi))[None]
+        t = from_u64(x)
+        e.dgt(t, 0, FORWARD)
+        assert np.array_equal(to_u64(t), CO.dgt(x, e.Q))

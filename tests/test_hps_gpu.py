@@ -1,0 +1,212 @@
+"""HPS basis extension, scaling and the BFV multiplication chain on the GPU,
+bit-exact against the exact oracle (cuPoly TestRNS ports included)."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import coracle as CO
+from oracle import pyoracle as O
+from tests.common import fold, random_poly_int, random_poly_residues, sha, unfold
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _dev(x):
+    from cupoly_b200.engine import from_u64
+    return from_u64(x)
+
+
+def _host(t):
+    from cupoly_b200.engine import to_u64
+    return to_u64(t)
+
+
+@pytest.mark.parametrize("k,nphi", [(1, 32), (2, 2048), (5, 8192), (8, 4096), (16, 32768), (24, 64)])
+def test_basis_extension_exact(gpu, k, nphi):
+    from cupoly_b200.engine import Engine
+    e = Engine(k, 0, nphi, 256)
+    xq = random_poly_residues(k, e.Q, nphi)
+    yb = random_poly_residues(k + 1, e.B, nphi)
+    out = e.empty(1)
+    e.basis_ext_q_to_b(out, _dev(fold(xq)[None]))
+    assert np.array_equal(unfold(_host(out))[0], CO.basis_ext(xq, e.Q, e.B))
+    outq = e.empty(0)
+    e.basis_ext_b_to_q(outq, _dev(fold(yb)[None]))
+    assert np.array_equal(unfold(_host(outq))[0], CO.basis_ext(yb, e.B, e.Q))
+
+
+def test_basis_extension_edges(gpu):
+    """X = 0, 1, Q-1, (Q-1)/2: exact lift (cuPoly's float v maps X near Q to X - Q)."""
+    from cupoly_b200.engine import Engine
+    e = Engine(3, 0, 32, 256)
+    Qp = O.prod(e.Q)
+    vals = [0, 1, Qp - 1, (Qp - 1) // 2, (Qp + 1) // 2, 12345] + [Qp - 1 - i for i in range(26)]
+    xq = np.array([[v % q for v in vals] for q in e.Q], dtype=np.uint64)
+    out = e.empty(1)
+    e.basis_ext_q_to_b(out, _dev(fold(xq)[None]))
+    assert unfold(_host(out))[0].tolist() == [[v % b for v in vals] for b in e.B]
+
+
+@pytest.mark.parametrize("k,nphi,t", [(1, 32, 256), (2, 2048, 256), (5, 8192, 256), (3, 4096, 65537),
+                                      (16, 32768, 65537), (4, 64, 3)])
+def test_complex_and_simple_scaling(gpu, k, nphi, t):
+    from cupoly_b200.engine import Engine
+    e = Engine(k, 0, nphi, t)
+    xq = random_poly_residues(3 * k, e.Q, nphi)
+    yb = random_poly_residues(3 * k + 1, e.B, nphi)
+    out = e.empty(1)
+    e.complex_scaling(out, _dev(fold(xq)[None]), _dev(fold(yb)[None]))
+    assert np.array_equal(unfold(_host(out))[0], CO.complex_scaling(xq, yb, e.Q, e.B, t))
+    ot = e.empty(3)
+    e.simple_scaling(ot, _dev(fold(xq)[None]))
+    assert np.array_equal(unfold(_host(ot))[0, 0], CO.simple_scaling(xq, e.Q, t))
+
+
+def test_golden_hps(gpu):
+    from cupoly_b200.engine import Engine
+    for case in json.load(open(os.path.join(GOLD, "hps_golden.json"))):
+        e = Engine(case["k"], case["kl"], case["nphi"], case["t"])
+        xq = random_poly_residues(case["seed"], e.Q, case["nphi"])
+        yb = random_poly_residues(case["seed"] + 1000, e.B, case["nphi"])
+        out = e.empty(1)
+        e.basis_ext_q_to_b(out, _dev(fold(xq)[None]))
+        assert sha(unfold(_host(out))[0]) == case["ext_q_to_b"]
+        outq = e.empty(0)
+        e.basis_ext_b_to_q(outq, _dev(fold(yb)[None]))
+        assert sha(unfold(_host(outq))[0]) == case["ext_b_to_q"]
+        e.complex_scaling(out, _dev(fold(xq)[None]), _dev(fold(yb)[None]))
+        assert sha(unfold(_host(out))[0]) == case["complex_scaling"]
+        ot = e.empty(3)
+        e.simple_scaling(ot, _dev(fold(xq)[None]))
+        assert sha(unfold(_host(ot))[0, 0]) == case["simple_scaling"]
+
+
+def _bfv_case(k, nphi, t, seed):
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine
+    e = Engine(k, 0, nphi, t)
+    rows = [random_poly_residues(seed + i, e.Q, nphi) for i in range(4)]
+    dev = []
+    for r in rows:
+        d = _dev(fold(r)[None])
+        e.dgt(d, 0, FORWARD)
+        dev.append(d)
+    outs = [e.empty(0) for _ in range(3)]
+    e.bfv_mul(*outs, *dev)
+    got = []
+    for o in outs:
+        e.dgt(o, 0, INVERSE)
+        got.append(unfold(_host(o))[0])
+    ref = CO.bfv_mul(*[r[None] for r in rows], e.Q, e.B, t)
+    return got, [r[0] for r in ref], e, dev
+
+
+@pytest.mark.parametrize("k,nphi,t", [(1, 32, 256), (2, 4096, 256), (5, 8192, 256), (3, 2048, 65537)])
+def test_bfv_mul_plain_vs_oracle(gpu, k, nphi, t):
+    got, ref, e, dev = _bfv_case(k, nphi, t, 100 + k)
+    for g, r in zip(got, ref):
+        assert np.array_equal(g, r)
+
+
+def test_bfv_mul_keeps_inputs(gpu):
+    got, ref, e, dev = _bfv_case(2, 2048, 256, 7)
+    got2, _, _, _ = _bfv_case(2, 2048, 256, 7)
+    for a, b in zip(got, got2):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("logq2,nphi", [(30, 32), (120, 2048), (250, 8192)])
+def test_reference_rns_tests(gpu, logq2, nphi):
+    """cuPoly TestRNS.{SimpleBasisExtensionQuadQtoB, SimpleScalingtDivQ,
+    ComplexBasisScalingUniform, WorddecompPowersOf} (test_bfv_mode.cu:492-1104)."""
+    from cupoly_b200 import cupoly as cp
+    from cupoly_b200.engine import INVERSE
+    k = math.ceil(logq2 / 63)
+    t = 256
+    cp.CUDAEngine.init(k, k + 1, nphi, t)
+    ctx = cp.Context()
+    e = cp.CUDAEngine.engine
+    q = cp.CUDAEngine.RNSProduct
+    # quadratic input i^2 mod t extended to B
+    aq, ab = cp.poly_t(), cp.poly_t()
+    cp.poly_init(ctx, aq)
+    for i in range(nphi):
+        cp.poly_set_coeff(ctx, aq, i, i * i % t)
+    cp.poly_basis_extension_Q_to_B(ctx, ab, aq)
+    tb = ab.d_coefs.clone()
+    e.dgt(tb, 1, INVERSE, stream=ctx.stream)
+    assert unfold(_host(tb))[0].tolist() == [[i * i % t % b for i in range(nphi)] for b in e.B]
+    # simple scaling vs round(t x / q) mod t
+    a, b = cp.poly_t(), cp.poly_t()
+    cp.poly_init(ctx, a)
+    cp.Sampler.sample(ctx, a, cp.UNIFORM)
+    A = [cp.poly_get_coeff(ctx, a, i) for i in range(nphi)]
+    cp.poly_simple_scaling_tDivQ(ctx, b, a)
+    assert [cp.poly_get_coeff(ctx, b, i) for i in range(nphi)] == [(2 * t * x + q) // (2 * q) % t for x in A]
+    # complex scaling: |b - t c / q| < 2 in the reference; here exact round(t c / q)
+    aq2, ab2, out = cp.poly_t(), cp.poly_t(), cp.poly_t()
+    cp.poly_init(ctx, aq2)
+    cp.Sampler.sample(ctx, aq2, cp.UNIFORM)
+    C = [cp.poly_get_coeff(ctx, aq2, i) for i in range(nphi)]
+    cp.poly_basis_extension_Q_to_B(ctx, ab2, aq2)
+    cp.poly_complex_scaling_tDivQ(ctx, out, aq2, ab2)
+    got = [cp.poly_get_coeff(ctx, out, i) for i in range(nphi)]
+    assert got == [(2 * t * c + q) // (2 * q) for c in C]
+    assert all(abs(g - t * c / q) < 2 for g, c in zip(got, C))
+    # <rho(a), xi(b)> == a * b mod q
+    x, y, prod_ = cp.poly_t(), cp.poly_t(), cp.poly_t()
+    for p_ in (x, y):
+        cp.poly_init(ctx, p_)
+        cp.Sampler.sample(ctx, p_, cp.DISCRETE_GAUSSIAN)
+    R = [cp.poly_t() for _ in range(k)]
+    X = [cp.poly_t() for _ in range(k)]
+    cp.poly_rho_bfv(ctx, R, x)
+    cp.poly_xi_bfv(ctx, X, y)
+    acc = cp.poly_t()
+    cp.poly_init(ctx, acc)
+    for i in range(k):
+        cp.poly_mul_add(ctx, acc, R[i], X[i], acc)
+    cp.poly_mul(ctx, prod_, x, y)
+    assert [cp.poly_get_coeff(ctx, acc, i) for i in range(nphi)] == \
+        [cp.poly_get_coeff(ctx, prod_, i) for i in range(nphi)]
+    cp.CUDAEngine.destroy()
+
+
+def test_simple_scaling_exact_vs_bigint(gpu):
+    from cupoly_b200.engine import Engine
+    e = Engine(3, 0, 64, 65537)
+    Qp = O.prod(e.Q)
+    ints = random_poly_int(5, Qp, 64)
+    xq = np.array([[v % q for v in ints] for q in e.Q], dtype=np.uint64)
+    ot = e.empty(3)
+    e.simple_scaling(ot, _dev(fold(xq)[None]))
+    assert unfold(_host(ot))[0, 0].tolist() == [(2 * 65537 * v + Qp) // (2 * Qp) % 65537 for v in ints]
+
+
+@pytest.mark.parametrize("k,nphi,npairs", [(2, 2048, 3), (5, 8192, 4)])
+def test_bfv_mul_batch_vs_plain_and_oracle(gpu, k, nphi, npairs):
+    """Batched chain == per-call chain == oracle, pair by pair."""
+    import torch
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine
+    e = Engine(k, 0, nphi, 256)
+    rows = [np.stack([random_poly_residues(200 + 10 * i + j, e.Q, nphi) for i in range(npairs)]) for j in range(4)]
+    dev = []
+    for r in rows:
+        d = _dev(fold(r))
+        e.dgt(d, 0, FORWARD)
+        dev.append(d)
+    c = e.empty(0, 3 * npairs)
+    e.bfv_mul_batch(c, *dev, npairs, e.bfv_mul_batch_workspace(npairs))
+    for i in range(npairs):
+        outs = [e.empty(0) for _ in range(3)]
+        e.bfv_mul(*outs, *[d[i:i + 1] for d in dev])
+        for j in range(3):
+            assert torch.equal(outs[j][0], c[j * npairs + i])
+    e.dgt(c, 0, INVERSE)
+    got = unfold(_host(c))
+    ref = CO.bfv_mul(*rows, e.Q, e.B, 256)
+    for j in range(3):
+        assert np.array_equal(got[j * npairs:(j + 1) * npairs], ref[j])
