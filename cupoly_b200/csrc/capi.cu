@@ -58,7 +58,7 @@ int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int l
   CP_REQUIRE(nphi >= 2 && nphi <= 65536 && (nphi & (nphi - 1)) == 0,
              "cp_engine_create: nphi must be a power of two in [2, 65536]");
   CP_REQUIRE(t >= 2 && t < kPrimes[kNumPrimes - 1], "cp_engine_create: t must be in [2, min prime)");
-  CP_REQUIRE(log_radix == 0 || log_radix == 3 || log_radix == 4, "cp_engine_create: log_radix must be 0, 3 or 4");
+  CP_REQUIRE(log_radix == 0 || (log_radix >= 2 && log_radix <= 4), "cp_engine_create: log_radix must be 0, 2, 3 or 4");
   cp_engine* h = new (std::nothrow) cp_engine();
   if (!h) {
     set_error("cp_engine_create: host allocation failed");

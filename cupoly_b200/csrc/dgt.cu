@@ -43,6 +43,8 @@ RunFn pick(int logNc, int logR) {
   CP_CASE(5, 4) CP_CASE(5, 3) CP_CASE(6, 4) CP_CASE(6, 3) CP_CASE(7, 4) CP_CASE(7, 3)
   CP_CASE(8, 4) CP_CASE(8, 3) CP_CASE(9, 4) CP_CASE(9, 3) CP_CASE(10, 4) CP_CASE(10, 3)
   CP_CASE(11, 4) CP_CASE(11, 3) CP_CASE(12, 4) CP_CASE(12, 3) CP_CASE(13, 4) CP_CASE(13, 3)
+  CP_CASE(5, 2) CP_CASE(6, 2) CP_CASE(7, 2) CP_CASE(8, 2) CP_CASE(9, 2) CP_CASE(10, 2)
+  CP_CASE(11, 2) CP_CASE(12, 2)
 #undef CP_CASE
   return nullptr;
 }

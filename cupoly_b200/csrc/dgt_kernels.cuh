@@ -169,9 +169,14 @@ constexpr int dgt_smem_bytes() {
 // Forward transform of 2^LOGNC elements per CTA, in place.
 // blockIdx.x = (poly * nres + r) * 2^S + h; element block h of residue r.
 // Occupancy hint: at most 128 registers per thread for the CTA sizes used.
+// Register budget: 64 per thread for radix <= 8 (two 512-thread CTAs per SM),
+// 128 for radix 16.
 template <int LOGNC, int LOGR>
 constexpr int dgt_min_blocks() {
-  return (512 >> (LOGNC - LOGR)) > 0 ? ((512 >> (LOGNC - LOGR)) < 32 ? (512 >> (LOGNC - LOGR)) : 32) : 1;
+  constexpr int T = (1 << LOGNC) >> LOGR;
+  constexpr int regs = LOGR >= 4 ? 128 : 64;
+  constexpr int b = 65536 / (T * regs);
+  return b < 1 ? 1 : (b > 16 ? 16 : b);
 }
 
 template <int LOGNC, int LOGR>

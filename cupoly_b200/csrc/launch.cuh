@@ -33,12 +33,14 @@ inline int check_launch(const char* what) {
 // Raise a kernel's dynamic shared-memory limit once per device.
 template <typename K>
 inline int ensure_smem(K kernel, int bytes, std::atomic<unsigned long long>& done_mask) {
-  if (bytes <= 48 * 1024) return CP_OK_;
   int dev = 0;
   cudaGetDevice(&dev);
   const unsigned long long bit = 1ULL << (dev & 63);
   if (done_mask.load() & bit) return CP_OK_;
-  cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t err = cudaSuccess;
+  if (bytes > 48 * 1024) err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (err == cudaSuccess)  // favour shared memory: several CTAs per SM
+    err = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (err != cudaSuccess) return cuda_fail("cudaFuncSetAttribute", err);
   done_mask.fetch_or(bit);
   return CP_OK_;

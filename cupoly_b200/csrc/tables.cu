@@ -131,6 +131,7 @@ DgtPlan make_plan(int logN, int logR) {
   P.logNc = logN < kMaxLogNc ? logN : kMaxLogNc;
   P.S = logN - P.logNc;
   P.logR = logR < P.logNc ? logR : P.logNc;
+  while ((P.logNc - P.logR) > 10) ++P.logR;  // at most 1024 threads per CTA
   P.npass = (P.logNc + P.logR - 1) / P.logR;
   P.w[0] = P.logNc - (P.npass - 1) * P.logR;
   P.p[0] = P.logNc - P.w[0];

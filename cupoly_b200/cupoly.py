@@ -98,11 +98,17 @@ def _E() -> Engine:
 
 
 class Context:
-    """One stream plus scratch (cuPoly include/cuPoly/arithmetic/context.h:34-109)."""
+    """One stream plus scratch (cuPoly include/cuPoly/arithmetic/context.h:34-109).
 
-    def __init__(self):
+    By default the context runs on torch's current stream, so tensors handed
+    between poly_* calls and ordinary torch code stay ordered; pass
+    ``own_stream=True`` for a private stream (then synchronise before touching
+    ``d_coefs`` from another stream, as with cuPoly's per-context streams).
+    """
+
+    def __init__(self, own_stream: bool = False):
         e = _E()
-        self.stream = torch.cuda.Stream()
+        self.stream = torch.cuda.Stream() if own_stream else torch.cuda.current_stream()
         with torch.cuda.stream(self.stream):
             self.workspace = e.workspace()
             self.d_aux_coefs = e.empty(QBBase)

@@ -25,10 +25,11 @@ def _host(t):
     return to_u64(t)
 
 
-@pytest.mark.parametrize("k,nphi", [(1, 32), (2, 2048), (5, 8192), (8, 4096), (16, 32768), (24, 64)])
-def test_basis_extension_exact(gpu, k, nphi):
+@pytest.mark.parametrize("k,kl,nphi", [(1, 2, 32), (2, 3, 2048), (5, 6, 8192), (8, 9, 4096), (16, 17, 32768),
+                                        (24, 24, 64), (7, 3, 256)])
+def test_basis_extension_exact(gpu, k, kl, nphi):
     from cupoly_b200.engine import Engine
-    e = Engine(k, 0, nphi, 256)
+    e = Engine(k, kl, nphi, 256)
     xq = random_poly_residues(k, e.Q, nphi)
     yb = random_poly_residues(k + 1, e.B, nphi)
     out = e.empty(1)
