@@ -69,6 +69,7 @@ SIGNATURES = {
     "cp_poly_complex_scaling_tdivq": (_i, [_vp, _vp, _vp, _vp, C.c_uint, _vp, _vp]),
     "cp_poly_simple_scaling_tdivq": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cp_bfv_mul": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "cp_bfv_mul_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cp_bfv_mul_batch_workspace_bytes": (C.c_size_t, [_vp, _i]),
     "cp_bfv_mul_batch": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
     "cp_sample": (_i, [_vp, _vp, _i, _i, _u64, _u32, _i, _i, _vp]),

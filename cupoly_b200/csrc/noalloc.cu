@@ -1,0 +1,85 @@
+// BFV multiplication with library-owned static scratch: the one entry point
+// that never allocates device memory.
+//
+// Who needs it: callers that cannot call cudaMalloc on the path that
+// multiplies -- a serving runtime or host framework that reserves all device
+// memory up front and forbids allocation afterwards, code that must not take
+// the implicit device synchronisation cudaMalloc/cudaFree can cause, or a
+// plugin host that gives the library no allocator.  cp_bfv_mul needs a
+// caller-provided workspace; cp_bfv_mul_noalloc uses the fixed array below
+// instead.
+//
+// The scratch is a file-scope __device__ array of CP_NOALLOC_SCRATCH_BYTES
+// (8 MiB).  Every GPU that loads this library holds it until the process
+// exits.  In host code `g_noalloc_scratch` names a host-side stand-in, not a
+// device address: it must never be passed to a kernel.  The device address is
+// obtained with cudaGetSymbolAddress once per device, with that device
+// current, on the first call made on that device; that first call should
+// therefore come before any stream capture.
+//
+// All calls share the one array and it keeps whatever the last call left
+// there.  Nothing in it needs to start at zero: every region the chain uses
+// is written before it is read.  Calls whose executions overlap on the GPU
+// (different streams, or different threads without ordering) race on the
+// array and corrupt each other's results; serialise them.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <mutex>
+
+#include "../../include/cupoly_b200.h"
+#include "launch.cuh"
+
+namespace {
+
+constexpr size_t kScratchBytes = CP_NOALLOC_SCRATCH_BYTES;
+static_assert(kScratchBytes == (size_t)8 << 20, "header and library disagree on the scratch size");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+void* g_dev_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (set-up on first use).
+int scratch_address(void** out) {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return cpoly::cuda_fail("cp_bfv_mul_noalloc: cudaGetDevice", err);
+  if (dev < 0 || dev >= kMaxDevices) {
+    cpoly::set_error("cp_bfv_mul_noalloc: device index out of range");
+    return CP_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!g_dev_ptr[dev]) {
+    void* p = nullptr;
+    err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess || !p) return cpoly::cuda_fail("cp_bfv_mul_noalloc: cudaGetSymbolAddress", err);
+    g_dev_ptr[dev] = p;
+  }
+  *out = g_dev_ptr[dev];
+  return CP_OK;
+}
+
+}  // namespace
+
+extern "C" int cp_bfv_mul_noalloc(const cp_engine* e, void* c0, void* c1, void* c2, const void* a0, const void* a1,
+                                  const void* b0, const void* b1, void* stream) {
+  if (!e || !c0 || !c1 || !c2 || !a0 || !a1 || !b0 || !b1) {
+    cpoly::set_error("cp_bfv_mul_noalloc: NULL argument");
+    return CP_ERR_INVALID;
+  }
+  const size_t need = cp_workspace_bytes(e);
+  if (need > kScratchBytes) {
+    char msg[256];
+    std::snprintf(msg, sizeof msg,
+                  "cp_bfv_mul_noalloc: this parameter set needs %zu bytes of scratch; the static scratch holds %zu "
+                  "bytes (use cp_bfv_mul with a caller workspace)",
+                  need, kScratchBytes);
+    cpoly::set_error(msg);
+    return CP_ERR_UNSUPPORTED;
+  }
+  void* ws = nullptr;
+  if (int rc = scratch_address(&ws)) return rc;
+  return cp_bfv_mul(e, c0, c1, c2, a0, a1, b0, b1, ws, stream);
+}

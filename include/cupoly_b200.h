@@ -142,6 +142,20 @@ int cp_poly_simple_scaling_tdivq(const cp_engine* e, void* out_t, const void* in
  *      order (src/arithmetic/polynomial.cu:350-527, 951-999). ---- */
 int cp_bfv_mul(const cp_engine* e, void* c0, void* c1, void* c2, const void* a0, const void* a1, const void* b0,
                const void* b1, void* workspace, void* stream);
+/* cp_bfv_mul without a caller workspace, for callers that cannot allocate
+ * device memory on this path (a runtime that reserves all HBM up front and
+ * forbids later allocation, code that must not take cudaMalloc's implicit
+ * synchronisation, a plugin host with no allocator).  No counterpart in
+ * cuPoly.  Scratch is a static device array of CP_NOALLOC_SCRATCH_BYTES inside
+ * the library, held by every GPU that loads it until exit; parameter sets
+ * needing more (cp_workspace_bytes(e) > CP_NOALLOC_SCRATCH_BYTES, e.g. nphi
+ * 16384 with k = 10) return CP_ERR_UNSUPPORTED.  The first call on a device
+ * looks up the array's device address, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race; serialise
+ * them.  Allocates nothing (no cudaMalloc/cudaFree). */
+#define CP_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
+int cp_bfv_mul_noalloc(const cp_engine* e, void* c0, void* c1, void* c2, const void* a0, const void* a1,
+                       const void* b0, const void* b1, void* stream);
 /* Batched form of the same chain: npairs ciphertext pairs per call, each input
  * uint64_t[npairs][k][N][2] (DGT domain), output c = uint64_t[3][npairs][k][N][2]
  * (c0 of every pair, then c1, then c2).  No counterpart in cuPoly (one
