@@ -236,7 +236,9 @@ def run_ours(args, D: Dist):
         D.barrier()
     ms = D.max(ev0.elapsed_time(ev1))
     value = D.world * P * args.steps / (ms / 1e3)
-    launches_per_step = 10  # 5 DGT + 2 base conversions + 2 tensor + 1 scaling (nphi <= 16384)
+    # inverse DGT (gather) + Q->B + forward DGT(B) + 2 inverse DGTs with the tensor
+    # product fused in + fused scale->Q + forward DGT(Q) (nphi <= 16384: one kernel per DGT)
+    launches_per_step = 7
 
     # ---- e2e: C ABI with pinned host buffers, copies inside the timed region ----
     hin = [torch.empty_like(x, device="cpu").pin_memory() for x in ins]

@@ -392,16 +392,28 @@ int cp_bfv_mul_batch(const cp_engine* h, void* c, const void* a0, const void* a1
   ulonglong2* CQ = XB + 4 * P * be;                    // [3][P][k]
   ulonglong2* CB = CQ + 3 * P * qe;                    // [3][P][kl]
   ulonglong2* U = CB + 3 * P * be;                     // [3][P][kl]
-  const void* in[4] = {a0, a1, b0, b1};
-  for (int v = 0; v < 4; ++v) CP_TRY(d2d(X + v * P * qe, in[v], P * qe * 16, st));
-  CP_TRY(launch_dgt(e, X, CP_QBASE, 4 * npairs, 0, true, st));
+  // 1. inverse DGT of the four inputs over Q, gathered into X (no copies)
+  InvSrc gather{};
+  gather.p[0] = reinterpret_cast<const ulonglong2*>(a0);
+  gather.p[1] = reinterpret_cast<const ulonglong2*>(a1);
+  gather.p[2] = reinterpret_cast<const ulonglong2*>(b0);
+  gather.p[3] = reinterpret_cast<const ulonglong2*>(b1);
+  gather.mode = 2;
+  gather.npairs = npairs;
+  CP_TRY(launch_dgt_ex(e, X, nullptr, &gather, CP_QBASE, 4 * npairs, 0, true, st));
+  // 2. exact Q -> B extension, forward DGT over B
   CP_TRY(hps_basis_ext(e, XB, X, true, 4 * npairs, st));
   CP_TRY(launch_dgt(e, XB, CP_BBASE, 4 * npairs, 0, false, st));
-  CP_TRY(pw_dr2(e, CQ, CQ + P * qe, CQ + 2 * P * qe, a0, a1, b0, b1, CP_QBASE, st, npairs));
-  CP_TRY(pw_dr2(e, CB, CB + P * be, CB + 2 * P * be, XB, XB + P * be, XB + 2 * P * be, XB + 3 * P * be, CP_BBASE,
-                st, npairs));
-  CP_TRY(launch_dgt(e, CQ, CP_QBASE, 3 * npairs, 0, true, st));
-  CP_TRY(launch_dgt(e, CB, CP_BBASE, 3 * npairs, 0, true, st));
+  // 3. tensor product computed inside the inverse DGTs (Q side from the inputs, B side from XB)
+  InvSrc tq = gather;
+  tq.mode = 1;
+  CP_TRY(launch_dgt_ex(e, CQ, nullptr, &tq, CP_QBASE, 3 * npairs, 0, true, st));
+  InvSrc tb{};
+  for (int v = 0; v < 4; ++v) tb.p[v] = XB + v * P * be;
+  tb.mode = 1;
+  tb.npairs = npairs;
+  CP_TRY(launch_dgt_ex(e, CB, nullptr, &tb, CP_BBASE, 3 * npairs, 0, true, st));
+  // 4. round(t X / Q) and B -> Q, then forward DGT of the outputs
   CP_TRY(hps_scale_to_q(e, c, CQ, CB, U, 3 * npairs, st));
   return launch_dgt(e, c, CP_QBASE, 3 * npairs, 0, false, st);
 }

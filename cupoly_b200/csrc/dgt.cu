@@ -9,8 +9,8 @@ namespace cpoly {
 namespace {
 
 template <int LOGNC, int LOGR>
-int run_cta(const Engine& e, ulonglong2* data, int nres, int rid_off, int npolys, long long poly_stride,
-            bool inverse, bool twist, cudaStream_t st) {
+int run_cta(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres, int rid_off,
+            int npolys, long long poly_stride, bool inverse, bool twist, cudaStream_t st) {
   constexpr int T = (1 << LOGNC) >> LOGR;
   constexpr int smem = dgt_smem_bytes<LOGNC, LOGR>();
   DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc};
@@ -24,16 +24,19 @@ int run_cta(const Engine& e, ulonglong2* data, int nres, int rid_off, int npolys
   if (!inverse) {
     static std::atomic<unsigned long long> done{0};
     if (int rc = ensure_smem(k_dgt_fwd<LOGNC, LOGR>, smem, done)) return rc;
-    k_dgt_fwd<LOGNC, LOGR><<<(unsigned)blocks, T, smem, st>>>(data, A, nres, rid_off, poly_stride, S, twist ? 1 : 0);
+    k_dgt_fwd<LOGNC, LOGR><<<(unsigned)blocks, T, smem, st>>>(data, fsrc, A, nres, rid_off, poly_stride, S,
+                                                              twist ? 1 : 0);
   } else {
     static std::atomic<unsigned long long> done{0};
     if (int rc = ensure_smem(k_dgt_inv<LOGNC, LOGR>, smem, done)) return rc;
-    k_dgt_inv<LOGNC, LOGR><<<(unsigned)blocks, T, smem, st>>>(data, A, nres, rid_off, poly_stride, S, twist ? 1 : 0);
+    k_dgt_inv<LOGNC, LOGR><<<(unsigned)blocks, T, smem, st>>>(data, isrc, A, nres, rid_off, poly_stride, S,
+                                                              twist ? 1 : 0);
   }
   return check_launch("dgt");
 }
 
-using RunFn = int (*)(const Engine&, ulonglong2*, int, int, int, long long, bool, bool, cudaStream_t);
+using RunFn = int (*)(const Engine&, ulonglong2*, const ulonglong2*, const InvSrc&, int, int, int, long long, bool,
+                      bool, cudaStream_t);
 
 // (logNc, effective logR) -> instantiation.
 RunFn pick(int logNc, int logR) {
@@ -49,10 +52,34 @@ RunFn pick(int logNc, int logR) {
   return nullptr;
 }
 
+int launch_split(const Engine& e, ulonglong2* data, const ulonglong2* src, int nres, int rid_off, int npolys,
+                 long long poly_stride, bool inverse, cudaStream_t st) {
+  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc};
+  const int Nc = 1 << e.plan.logNc;
+  const long long blocks = (long long)npolys * nres * (Nc / 256);
+  if (blocks > 0x7fffffffLL) {
+    set_error("dgt: grid too large");
+    return 1;
+  }
+  const int S = e.plan.S, lc = e.plan.logNc, lr = e.plan.logR;
+  if (!inverse) {
+    if (S == 1)
+      k_dgt_split<1, false><<<(unsigned)blocks, 256, 0, st>>>(data, src, A, nres, rid_off, poly_stride, lc, lr);
+    else
+      k_dgt_split<2, false><<<(unsigned)blocks, 256, 0, st>>>(data, src, A, nres, rid_off, poly_stride, lc, lr);
+  } else {
+    if (S == 1)
+      k_dgt_split<1, true><<<(unsigned)blocks, 256, 0, st>>>(data, nullptr, A, nres, rid_off, poly_stride, lc, lr);
+    else
+      k_dgt_split<2, true><<<(unsigned)blocks, 256, 0, st>>>(data, nullptr, A, nres, rid_off, poly_stride, lc, lr);
+  }
+  return check_launch("dgt split");
+}
+
 }  // namespace
 
-int launch_dgt(const Engine& e, void* data_v, int base, int npolys, long long poly_stride, bool inverse,
-               cudaStream_t st) {
+int launch_dgt_ex(const Engine& e, void* dst_v, const void* fsrc_v, const InvSrc* isrc_p, int base, int npolys,
+                  long long poly_stride, bool inverse, cudaStream_t st) {
   if (base == 3) return 0;  // TBase: no transform (cuPoly dgt.cu:1087-1088)
   const int nres = e.n_residues(base);
   if (nres < 0) {
@@ -60,39 +87,39 @@ int launch_dgt(const Engine& e, void* data_v, int base, int npolys, long long po
     return 1;
   }
   const int rid_off = e.rid_offset(base);
-  ulonglong2* data = reinterpret_cast<ulonglong2*>(data_v);
+  ulonglong2* data = reinterpret_cast<ulonglong2*>(dst_v);
+  const ulonglong2* fsrc = reinterpret_cast<const ulonglong2*>(fsrc_v);
   if (poly_stride == 0) poly_stride = (long long)nres * e.N;
   RunFn fn = pick(e.plan.logNc, e.plan.logR);
   if (!fn) {
     set_error("dgt: no kernel for this size");
     return 3;
   }
+  InvSrc isrc{};
+  if (isrc_p) {
+    isrc = *isrc_p;
+  } else {
+    isrc.p[0] = data;
+    isrc.mode = 0;
+    isrc.npairs = 1;
+  }
   const int S = e.plan.S;
-  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc};
-  const int Nc = 1 << e.plan.logNc;
-  const long long split_blocks = (long long)npolys * nres * (Nc / 256);
   if (!inverse) {
     if (S > 0) {
-      if (S == 1)
-        k_dgt_split<1, false><<<(unsigned)split_blocks, 256, 0, st>>>(data, A, nres, rid_off, poly_stride,
-                                                                       e.plan.logNc, e.plan.logR);
-      else
-        k_dgt_split<2, false><<<(unsigned)split_blocks, 256, 0, st>>>(data, A, nres, rid_off, poly_stride,
-                                                                       e.plan.logNc, e.plan.logR);
-      int rc = check_launch("dgt split");
+      int rc = launch_split(e, data, fsrc, nres, rid_off, npolys, poly_stride, false, st);
       if (rc) return rc;
+      return fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, false, false, st);
     }
-    return fn(e, data, nres, rid_off, npolys, poly_stride, false, S == 0, st);
+    return fn(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, false, true, st);
   }
-  int rc = fn(e, data, nres, rid_off, npolys, poly_stride, true, S == 0, st);
+  int rc = fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, true, S == 0, st);
   if (rc || S == 0) return rc;
-  if (S == 1)
-    k_dgt_split<1, true><<<(unsigned)split_blocks, 256, 0, st>>>(data, A, nres, rid_off, poly_stride, e.plan.logNc,
-                                                                  e.plan.logR);
-  else
-    k_dgt_split<2, true><<<(unsigned)split_blocks, 256, 0, st>>>(data, A, nres, rid_off, poly_stride, e.plan.logNc,
-                                                                  e.plan.logR);
-  return check_launch("dgt split");
+  return launch_split(e, data, nullptr, nres, rid_off, npolys, poly_stride, true, st);
+}
+
+int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly_stride, bool inverse,
+               cudaStream_t st) {
+  return launch_dgt_ex(e, data, nullptr, nullptr, base, npolys, poly_stride, inverse, st);
 }
 
 }  // namespace cpoly

@@ -181,8 +181,8 @@ constexpr int dgt_min_blocks() {
 
 template <int LOGNC, int LOGR>
 __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
-    k_dgt_fwd(ulonglong2* __restrict__ data, DgtArgs A, int nres, int rid_off, long long poly_stride, int S,
-              int twist) {
+    k_dgt_fwd(ulonglong2* __restrict__ data, const ulonglong2* __restrict__ src_base, DgtArgs A, int nres,
+              int rid_off, long long poly_stride, int S, int twist) {
   constexpr int NC = 1 << LOGNC, R = 1 << LOGR, T = NC >> LOGR;
   using C = PassCfg<LOGNC, LOGR>;
   extern __shared__ ulonglong2 smem[];
@@ -196,7 +196,9 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   const int rid = rid_off + r;
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
-  ulonglong2* x = data + poly * poly_stride + ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
+  const size_t off = poly * poly_stride + ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
+  ulonglong2* x = data + off;
+  const ulonglong2* xs = (src_base ? src_base : data) + off;  // out of place when src_base is set
   for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
   __syncthreads();
   {
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
 #pragma unroll
       for (int v = 0; v < (1 << W); ++v) {
         const int idx = Lw + (v << PF);
-        const ulonglong2 a = x[idx];
+        const ulonglong2 a = xs[idx];
         uint64_t ar = a.x, ai = a.y;
         if (twist) {
           const ulonglong2 tr = __ldg(tab + A.L.off_twist + 2 * idx);
@@ -242,12 +244,29 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   }
 }
 
-// Inverse transform of 2^LOGNC elements per CTA, in place; untwist (with
-// N^-1) applied when `untwist` is set (S == 0).
+__device__ __forceinline__ ulonglong2 tensor_load(const InvSrc& s, int j, size_t off, const ModConst& m) {
+  const ulonglong2 a0 = s.p[0][off], a1 = s.p[1][off], b0 = s.p[2][off], b1 = s.p[3][off];
+  uint64_t r, i;
+  if (j == 0) {
+    gi_mul(r, i, a0.x, a0.y, b0.x, b0.y, m);
+  } else if (j == 2) {
+    gi_mul(r, i, a1.x, a1.y, b1.x, b1.y, m);
+  } else {
+    uint64_t r1, i1, r2, i2;
+    gi_mul_mont(r1, i1, a0.x, a0.y, b1.x, b1.y, m);
+    gi_mul_mont(r2, i2, a1.x, a1.y, b0.x, b0.y, m);
+    r = shoup_mul(add_mod(r1, r2, m.p), m.r1, m.r1s, m.p);
+    i = shoup_mul(add_mod(i1, i2, m.p), m.r1, m.r1s, m.p);
+  }
+  return make_ulonglong2(r, i);
+}
+
+// Inverse transform of 2^LOGNC elements per CTA; untwist (with N^-1) applied
+// when `untwist` is set (S == 0).  Input per InvSrc, output to `data`.
 template <int LOGNC, int LOGR>
 __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
-    k_dgt_inv(ulonglong2* __restrict__ data, DgtArgs A, int nres, int rid_off, long long poly_stride, int S,
-              int untwist) {
+    k_dgt_inv(ulonglong2* __restrict__ data, InvSrc src, DgtArgs A, int nres, int rid_off, long long poly_stride,
+              int S, int untwist) {
   constexpr int NC = 1 << LOGNC, R = 1 << LOGR, T = NC >> LOGR;
   using C = PassCfg<LOGNC, LOGR>;
   extern __shared__ ulonglong2 smem[];
@@ -261,12 +280,27 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   const int rid = rid_off + r;
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
-  ulonglong2* x = data + poly * poly_stride + ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
+  const size_t inner = ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
+  ulonglong2* x = data + poly * poly_stride + inner;
   for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
+  if (src.mode != 1) {
+    const ulonglong2* xs = src.mode == 0
+                               ? src.p[0] + poly * poly_stride + inner
+                               : src.p[poly / src.npairs] + (poly % src.npairs) * poly_stride + inner;
 #pragma unroll
-  for (int j = 0; j < R; ++j) {
-    const int idx = tid + j * T;
-    sdat[pad16(idx)] = x[idx];
+    for (int j = 0; j < R; ++j) {
+      const int idx = tid + j * T;
+      sdat[pad16(idx)] = xs[idx];
+    }
+  } else {
+    const int jt = poly / src.npairs;  // which tensor output
+    const size_t base = (size_t)(poly % src.npairs) * poly_stride + inner;
+    const ModConst m = A.mc[rid];
+#pragma unroll 4
+    for (int j = 0; j < R; ++j) {
+      const int idx = tid + j * T;
+      sdat[pad16(idx)] = tensor_load(src, jt, base + idx, m);
+    }
   }
   __syncthreads();
   inv_passes<LOGNC, LOGR, C::NP - 1>(sdat, srad, tab, A.L, p);
@@ -311,8 +345,8 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
 // over the top S bits + twiddle; inverse: twiddle + radix-2^S DIT + untwist).
 template <int S, bool INV>
 __global__ void __launch_bounds__(256)
-    k_dgt_split(ulonglong2* __restrict__ data, DgtArgs A, int nres, int rid_off, long long poly_stride, int logNc,
-                int logR) {
+    k_dgt_split(ulonglong2* __restrict__ data, const ulonglong2* __restrict__ src_base, DgtArgs A, int nres,
+                int rid_off, long long poly_stride, int logNc, int logR) {
   const int Nc = 1 << logNc;
   const int chunks = Nc / 256;
   const int pr = blockIdx.x / chunks;
@@ -323,6 +357,7 @@ __global__ void __launch_bounds__(256)
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
   ulonglong2* x = data + poly * poly_stride + ((size_t)r << (logNc + S));
+  const ulonglong2* xs = (src_base ? src_base : data) + poly * poly_stride + ((size_t)r << (logNc + S));
   constexpr int K = 1 << S;
   uint64_t xr[K], xi[K];
   const int R = 1 << logR;
@@ -330,7 +365,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int hh = 0; hh < K; ++hh) {
       const int n = Lw + hh * Nc;
-      const ulonglong2 a = x[n];
+      const ulonglong2 a = xs[n];
       uint64_t ar = a.x, ai = a.y;
       const ulonglong2 tr = __ldg(tab + A.L.off_twist + 2 * n);
       const ulonglong2 ti = __ldg(tab + A.L.off_twist + 2 * n + 1);

@@ -55,6 +55,18 @@ struct DgtArgs {
   const ModConst* mc;      // per engine residue
 };
 
+// Where the inverse DGT reads its input.
+//  mode 0: p[0] (same layout as the output; p[0] == output for in place);
+//  mode 1: the BFV tensor product of two ciphertexts (a0, a1) x (b0, b1) =
+//          p[0..3], computed while loading; output polynomial j * npairs + q
+//          is c_j of pair q: c0 = a0 b0, c1 = a0 b1 + a1 b0, c2 = a1 b1;
+//  mode 2: gather: output polynomial j * npairs + q reads polynomial q of p[j].
+struct InvSrc {
+  const ulonglong2* p[4];
+  int mode;
+  int npairs;
+};
+
 // Mixed-radix conversion constants of one (source base -> targets) pair.
 // Source base: n primes s_0..s_{n-1}; targets: K moduli m_0..m_{K-1}.
 struct MrcTables {

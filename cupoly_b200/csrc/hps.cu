@@ -22,7 +22,7 @@ namespace {
 
 constexpr int kMaxBase = 24;  // largest |Q| or |B| with a compiled kernel
 
-__device__ __forceinline__ uint64_t red1(uint64_t x, uint64_t m) { return x >= m ? x - m : x; }
+__device__ __forceinline__ uint64_t red1(uint64_t x, uint64_t m) { return red2p(x, m); }  // x < 2m
 
 // Mixed-radix digits of the value with residues z over primes s.
 template <int NS>
@@ -165,6 +165,48 @@ __global__ void __launch_bounds__(128) k_complex_scaling(ulonglong2* __restrict_
   }
 }
 
+// Complex scaling fused with the exact B -> Q conversion of its result:
+// out_q = (round(t X / Q) mod B) mod q_i; the kl B-residues stay in registers.
+// One thread per Gaussian element; the two coefficients are done in turn.
+template <int NQ, int NB>
+__global__ void __launch_bounds__(128) k_scale_to_q(ulonglong2* __restrict__ out_q, const ulonglong2* __restrict__ in_q,
+                                                    const ulonglong2* __restrict__ in_b, ScaleArgs a, ConvArgs c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.N) return;
+  in_q += blockIdx.y * a.q_stride;
+  in_b += blockIdx.y * a.b_stride;
+  uint64_t* o = reinterpret_cast<uint64_t*>(out_q + blockIdx.y * a.q_stride);
+  uint64_t s[NQ], sb[NB];
+#pragma unroll
+  for (int i = 0; i < NQ; ++i) s[i] = a.mc[i].p;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) sb[i] = a.mc[NQ + i].p;
+#pragma unroll 1
+  for (int comp = 0; comp < 2; ++comp) {
+    uint64_t d[NQ], u[NB];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+      const uint64_t* x = reinterpret_cast<const uint64_t*>(in_q + (size_t)i * a.N + j);
+      d[i] = shoup_mul(x[comp], __ldg(a.t_q + i), __ldg(a.t_q_s + i), s[i]);
+    }
+    mrc<NQ>(d, s, a.inv, a.inv_s);
+    const bool neg = above_half<NQ>(d, a.half);
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+      const uint64_t b = sb[t];
+      uint64_t r = horner<NQ>(d, b, a.hor + t * (NQ - 1), a.hor_s + t * (NQ - 1));
+      if (neg) r = sub_mod(r, __ldg(a.q_mod_b + t), b);
+      const uint64_t* y = reinterpret_cast<const uint64_t*>(in_b + (size_t)t * a.N + j);
+      const uint64_t ty = shoup_mul(y[comp], __ldg(a.t_b + t), __ldg(a.t_b_s + t), b);
+      u[t] = shoup_mul(ty + b - r, __ldg(a.qinv_b + t), __ldg(a.qinv_b_s + t), b);
+    }
+    mrc<NB>(u, sb, c.inv, c.inv_s);
+#pragma unroll
+    for (int i = 0; i < NQ; ++i)
+      o[2 * ((size_t)i * a.N + j) + comp] = horner<NB>(u, s[i], c.hor + i * (NB - 1), c.hor_s + i * (NB - 1));
+  }
+}
+
 struct SimpleArgs {
   const ModConst* mc;
   const uint64_t *inv, *inv_s, *hor, *hor_s, *half, *t_q, *t_q_s;
@@ -298,8 +340,41 @@ int hps_complex_scaling(const Engine& e, void* out_b, const void* in_q, const vo
 #undef CALL
 }
 
+namespace {
+template <int NQ>
+int launch_scale_to_q_n(ulonglong2* o, const ulonglong2* q, const ulonglong2* b, const ScaleArgs& a,
+                        const ConvArgs& c, int npolys, cudaStream_t st) {
+  dim3 grid((a.N + 127) / 128, npolys);
+  k_scale_to_q<NQ, NQ + 1><<<grid, 128, 0, st>>>(o, q, b, a, c);
+  return check_launch("scale_to_q");
+}
+}  // namespace
+
 int hps_scale_to_q(const Engine& e, void* out_q, const void* in_q, const void* in_b, void* scratch_b, int npolys,
                    cudaStream_t st) {
+  if (e.kl == e.k + 1 && e.k <= 16) {  // fused kernel: the B residues never leave registers
+    ScaleArgs a = scale_args(e);
+    ConvArgs c;
+    c.mc = e.d_mc;
+    c.N = e.N;
+    c.inv = e.d_hps + e.ho.bq_inv;
+    c.inv_s = e.d_hps + e.ho.bq_inv_s;
+    c.hor = e.d_hps + e.ho.bq_hor;
+    c.hor_s = e.d_hps + e.ho.bq_hor_s;
+    c.src_off = e.k;
+    c.dst_off = 0;
+    c.ndst = e.k;
+    auto* o = reinterpret_cast<ulonglong2*>(out_q);
+    auto* q = reinterpret_cast<const ulonglong2*>(in_q);
+    auto* b = reinterpret_cast<const ulonglong2*>(in_b);
+    switch (e.k) {
+#define CP_SQ(n) \
+  case n: return launch_scale_to_q_n<n>(o, q, b, a, c, npolys, st);
+      CP_SQ(1) CP_SQ(2) CP_SQ(3) CP_SQ(4) CP_SQ(5) CP_SQ(6) CP_SQ(7) CP_SQ(8)
+      CP_SQ(9) CP_SQ(10) CP_SQ(11) CP_SQ(12) CP_SQ(13) CP_SQ(14) CP_SQ(15) CP_SQ(16)
+#undef CP_SQ
+    }
+  }
   int rc = hps_complex_scaling(e, scratch_b, in_q, in_b, npolys, st);
   if (rc) return rc;
   return hps_basis_ext(e, out_q, scratch_b, false, npolys, st);

@@ -49,5 +49,9 @@ inline int ensure_smem(K kernel, int bytes, std::atomic<unsigned long long>& don
 // Kernel entry points implemented in the .cu files.
 int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly_stride, bool inverse,
                cudaStream_t st);
+// Out-of-place forms: forward reads `fsrc` (nullptr = in place); inverse reads
+// per `isrc` (nullptr = in place).  Output always to `dst`.
+int launch_dgt_ex(const Engine& e, void* dst, const void* fsrc, const InvSrc* isrc, int base, int npolys,
+                  long long poly_stride, bool inverse, cudaStream_t st);
 
 }  // namespace cpoly

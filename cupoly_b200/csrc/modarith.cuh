@@ -37,30 +37,32 @@ CP_HD uint64_t mulhi64(uint64_t a, uint64_t b) {
 #endif
 }
 
-CP_HD uint64_t add_mod(uint64_t a, uint64_t b, uint64_t p) {
-  uint64_t s = a + b;
-  return s >= p ? s - p : s;
+// The corrections below select on the sign of a 64-bit difference: every
+// intermediate lies in (-p, 2p) with p < 2^63, so its sign bit decides.
+CP_HD uint64_t red2p(uint64_t s, uint64_t p) {  // s in [0, 2p) -> [0, p)
+  const int64_t t = (int64_t)(s - p);
+  return t < 0 ? s : (uint64_t)t;
 }
 
+CP_HD uint64_t add_mod(uint64_t a, uint64_t b, uint64_t p) { return red2p(a + b, p); }
+
 CP_HD uint64_t sub_mod(uint64_t a, uint64_t b, uint64_t p) {
-  uint64_t d = a - b;
-  return a < b ? d + p : d;
+  const int64_t d = (int64_t)(a - b);
+  return d < 0 ? (uint64_t)d + p : (uint64_t)d;
 }
 
 CP_HD uint64_t neg_mod(uint64_t a, uint64_t p) { return a == 0 ? 0 : p - a; }
 
 // a * w mod p, w < p constant, ws = floor(w * 2^64 / p); any a < 2^64.
 CP_HD uint64_t shoup_mul(uint64_t a, uint64_t w, uint64_t ws, uint64_t p) {
-  uint64_t q = mulhi64(a, ws);
-  uint64_t r = a * w - q * p;  // in [0, 2p)
-  return r >= p ? r - p : r;
+  const uint64_t q = mulhi64(a, ws);
+  return red2p(a * w - q * p, p);  // a w - q p in [0, 2p)
 }
 
 // Montgomery reduction of hi:lo < p * 2^64 -> hi:lo * 2^-64 mod p.
 CP_HD uint64_t mont_redc(uint64_t hi, uint64_t lo, uint64_t p, uint64_t pneg) {
   uint64_t m = lo * pneg;
-  uint64_t t = hi + mulhi64(m, p) + (lo != 0);
-  return t >= p ? t - p : t;
+  return red2p(hi + mulhi64(m, p) + (lo != 0), p);
 }
 
 // a * b * 2^-64 mod p for a * b < p * 2^64.
