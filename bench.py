@@ -305,6 +305,19 @@ def run_ours(args, D: Dist):
     dgt_ms = ev0.elapsed_time(ev1) / reps
     dgt_bytes = 2 * 16 * e.N * 4 * P * K_B  # read + write every Gaussian element once
     achieved = dgt_bytes / (dgt_ms / 1e3) / 1e9
+    # integer roofline of the same launch: algorithmic Shoup multiplies and modular
+    # adds at the measured peak rates of those primitives on this GPU
+    from cupoly_b200.engine import dgt_op_counts, int_peaks
+    peaks_int = int_peaks()
+    ops = dgt_op_counts(e.N)
+    nres_launch = 4 * P * K_B
+    t_int = nres_launch * (ops["shoup"] / peaks_int["shoup"] + ops["addmod"] / peaks_int["addmod"])
+    int_roof = {"model_ms": round(t_int * 1e3, 4), "measured_ms": round(dgt_ms, 4),
+                "frac": round(t_int * 1e3 / dgt_ms, 4),
+                "shoup_per_launch": ops["shoup"] * nres_launch, "addmod_per_launch": ops["addmod"] * nres_launch,
+                "peak_shoup_per_s": round(peaks_int["shoup"], 1), "peak_addmod_per_s": round(peaks_int["addmod"], 1),
+                "peak_mont_per_s": round(peaks_int["mont"], 1), "peak_imad32_per_s": round(peaks_int["imad32"], 1),
+                "note": "frac = (Shoup / peak Shoup + adds / peak add) / measured; peaks measured live by cp_calibrate_int"}
 
     # ---- polymul/s of the nphi = 4096, k = 2 configuration (batched) ----
     e1 = Engine(2, 3, 4096, 256)
@@ -359,7 +372,8 @@ def run_ours(args, D: Dist):
                          "frac": round(achieved / hbm_peak, 4), "traffic": None,
                          "kernel": "k_dgt_fwd (forward DGT, %d residues of N=%d per launch, timed alone)" %
                                    (4 * P * K_B, e.N),
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback"},
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback",
+                         "int": int_roof},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": launches_per_step * args.steps,

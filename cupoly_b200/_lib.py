@@ -72,6 +72,7 @@ SIGNATURES = {
     "cp_bfv_mul_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cp_bfv_mul_batch_workspace_bytes": (C.c_size_t, [_vp, _i]),
     "cp_bfv_mul_batch": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
+    "cp_calibrate_int": (_i, [_i, _i, _vp, C.c_longlong, C.POINTER(C.c_float), _vp]),
     "cp_sample": (_i, [_vp, _vp, _i, _i, _u64, _u32, _i, _i, _vp]),
 }
 

@@ -164,6 +164,13 @@ size_t cp_bfv_mul_batch_workspace_bytes(const cp_engine* e, int npairs);
 int cp_bfv_mul_batch(const cp_engine* e, void* c, const void* a0, const void* a1, const void* b0, const void* b1,
                      int npairs, void* workspace, void* stream);
 
+/* ---- integer-throughput calibration (no counterpart in cuPoly): times `iters`
+ *      x 8 independent applications per thread of one primitive over nthreads
+ *      threads (a multiple of 256) and returns the kernel time in *ms.  kind:
+ *      0 Shoup constant multiply, 1 Montgomery multiply, 2 modular add,
+ *      3 32-bit multiply-add.  sink: nthreads uint64 of device memory. ---- */
+int cp_calibrate_int(int kind, int iters, void* sink, long long nthreads, float* ms, void* stream);
+
 /* ---- sampler: replaces Sampler::sample(ctx, p, kind) (src/cuda/sampler.cu:576-645).
  *      npolys consecutive polynomials over `base` with stream ids stream_id ..
  *      stream_id + npolys - 1; to_dgt != 0 applies the forward DGT (cuPoly does). */
