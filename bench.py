@@ -44,6 +44,10 @@ def parse():
     ap.add_argument("--pairs", type=int, default=128, help="ciphertext pairs per step (batched form)")
     ap.add_argument("--plain-pairs", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=10000)
+    ap.add_argument("--serving-rate", type=float, default=5000.0)
     return ap.parse_args()
 
 
@@ -346,6 +350,62 @@ def run_ours(args, D: Dist):
     torch.cuda.synchronize()
     polymul_value = NPm * 5 / (ev0.elapsed_time(ev1) / 1e3)
 
+    # ---- large configuration: nphi = 32768, k = 16, kl = 17, t = 65537, 64 pairs + sampling ----
+    large = None
+    if not args.no_large:
+        eL = Engine(16, 17, 32768, 65537)
+        PL = 64
+        insL = []
+        for j in range(4):
+            x = eL.empty(QBase, PL)
+            eL.sample(x, QBase, UNIFORM, seed, 4096 * j, npolys=PL, to_dgt=True)
+            insL.append(x)
+        cL = eL.empty(QBase, 3 * PL)
+        wsL = eL.bfv_mul_batch_workspace(PL)
+        eL.bfv_mul_batch(cL, *insL, PL, wsL)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(3):
+            eL.bfv_mul_batch(cL, *insL, PL, wsL)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        large_ms = ev0.elapsed_time(ev1) / 3
+        del insL, cL, wsL
+        # fresh noise: 2^24 samples of each distribution (512 polys of nphi 32768), coefficient domain
+        from cupoly_b200.engine import GAUSSIAN, TERNARY
+        buf = eL.empty(QBase, 512)
+        samp = {}
+        for name, kind in (("ternary", TERNARY), ("gaussian", GAUSSIAN), ("uniform", UNIFORM)):
+            eL.sample(buf, QBase, kind, seed, 0, npolys=512, to_dgt=False)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            eL.sample(buf, QBase, kind, seed, 7, npolys=512, to_dgt=False)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            sms = ev0.elapsed_time(ev1)
+            samp[name] = {"samples_per_s": round((1 << 24) / (sms / 1e3), 1),
+                          "GB_per_s_written": round(buf.numel() * 8 / (sms / 1e3) / 1e9, 1)}
+        eL.check()
+        large = {"config": "nphi=32768, k=16, kl=17, t=65537, 64 pairs per call", "hom_mul_per_s":
+                 round(PL / (large_ms / 1e3), 1), "ms_per_call": round(large_ms, 3),
+                 "sampling_2^24": samp}
+        del buf, eL
+        torch.cuda.empty_cache()
+
+    # ---- serving loop: open-loop Poisson arrivals, nphi in {4096..32768}, k = nphi/2048 ----
+    serving = None
+    if not args.no_serving and D.rank == 0:
+        from cupoly_b200 import serving as SV
+        classes = SV.default_classes()
+        ex = SV.GpuExecutor(classes)
+        sch = SV.Scheduler(classes, ex, 40 << 30)
+        reqs = sch.run(SV.poisson_requests(args.serving_requests, args.serving_rate, len(classes), 1))
+        serving = sch.stats(reqs)
+        serving["rate_req_s"] = args.serving_rate
+        serving["classes"] = "nphi 4096/8192/16384/32768, k = nphi/2048, kl = k+1, t = 256, uniform mix"
+        del ex, sch
+        torch.cuda.empty_cache()
+
     cpu = None
     if D.rank == 0 and not args.no_cpu_baseline:
         rate, done, el, cores = cpu_bfv_rate(10.0)
@@ -374,6 +434,8 @@ def run_ours(args, D: Dist):
                                    (4 * P * K_B, e.N),
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback",
                          "int": int_roof},
+            "large": large,
+            "serving": serving,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": launches_per_step * args.steps,

@@ -74,6 +74,7 @@ SIGNATURES = {
     "cp_bfv_mul_batch": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
     "cp_calibrate_int": (_i, [_i, _i, _vp, C.c_longlong, C.POINTER(C.c_float), _vp]),
     "cp_sample": (_i, [_vp, _vp, _i, _i, _u64, _u32, _i, _i, _vp]),
+    "cp_sample_ids": (_i, [_vp, _vp, _i, _i, _u64, _vp, _i, _i, _vp]),
 }
 
 _LIB = None

@@ -427,4 +427,13 @@ int cp_sample(const cp_engine* h, void* out, int base, int kind, uint64_t seed, 
   return CP_OK;
 }
 
+int cp_sample_ids(const cp_engine* h, void* out, int base, int kind, uint64_t seed, const uint32_t* stream_ids,
+                  int npolys, int to_dgt, void* stream) {
+  CP_REQUIRE(valid_base(h, base) && out && stream_ids && npolys >= 0, "cp_sample_ids: bad argument");
+  if (npolys == 0) return CP_OK;
+  CP_TRY(sample_poly(h->e, out, base, kind, seed, 0, npolys, S(stream), stream_ids));
+  if (to_dgt) return launch_dgt(h->e, out, base, npolys, 0, false, S(stream));
+  return CP_OK;
+}
+
 }  // extern "C"

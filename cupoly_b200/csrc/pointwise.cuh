@@ -31,6 +31,6 @@ int rns_xi_rho(const Engine& e, void* out, const void* in, bool rho, cudaStream_
 
 // Sampler
 int sample_poly(const Engine& e, void* out, int base, int kind, uint64_t seed, uint32_t stream_id, int npolys,
-                cudaStream_t st);
+                cudaStream_t st, const uint32_t* ids = nullptr);
 
 }  // namespace cpoly

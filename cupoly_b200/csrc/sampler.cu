@@ -106,10 +106,11 @@ __device__ __forceinline__ uint64_t lift(int64_t v, uint64_t p) { return v >= 0 
 // One thread per Gaussian element j (coefficients j and j + N) of one polynomial.
 __global__ void __launch_bounds__(256) k_sample(ulonglong2* __restrict__ out, const ModConst* __restrict__ mc, int N,
                                                 int nres, int rid_off, int kind, uint32_t k0, uint32_t k1,
-                                                uint32_t sid0, long long poly_stride, int* __restrict__ err) {
+                                                uint32_t sid0, long long poly_stride, int* __restrict__ err,
+                                                const uint32_t* __restrict__ ids) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= N) return;
-  const uint32_t sid = sid0 + blockIdx.y;
+  const uint32_t sid = ids ? ids[blockIdx.y] : sid0 + blockIdx.y;
   out += blockIdx.y * poly_stride;
   if (kind == UNIFORM) {
     for (int r = 0; r < nres; ++r) {
@@ -156,12 +157,12 @@ __global__ void __launch_bounds__(256) k_sample(ulonglong2* __restrict__ out, co
 __global__ void __launch_bounds__(256) k_sample_hw(ulonglong2* __restrict__ out, const ModConst* __restrict__ mc,
                                                    int N, int logNphi, int nres, int rid_off, uint32_t k0,
                                                    uint32_t k1, uint32_t sid0, long long poly_stride,
-                                                   int* __restrict__ err) {
+                                                   int* __restrict__ err, const uint32_t* __restrict__ ids) {
   extern __shared__ uint32_t bitmap[];  // nphi bits
   __shared__ int pos[64];
   __shared__ int sgn[64];
   const int nphi = 2 * N;
-  const uint32_t sid = sid0 + blockIdx.x;
+  const uint32_t sid = ids ? ids[blockIdx.x] : sid0 + blockIdx.x;
   out += blockIdx.x * poly_stride;
   for (int i = threadIdx.x; i < (nphi + 31) / 32; i += blockDim.x) bitmap[i] = 0;
   for (int r = 0; r < nres; ++r)
@@ -216,7 +217,7 @@ int upload_cdt() {
 }  // namespace
 
 int sample_poly(const Engine& e, void* out_v, int base, int kind, uint64_t seed, uint32_t stream_id, int npolys,
-                cudaStream_t st) {
+                cudaStream_t st, const uint32_t* ids) {
   if (kind < 0 || kind > GAUSSIAN) {
     set_error("sample: unknown distribution");
     return CP_ERR_INVALID_;
@@ -234,10 +235,11 @@ int sample_poly(const Engine& e, void* out_v, int base, int kind, uint64_t seed,
   if (kind == HAMMINGWEIGHT) {
     const int words = (e.nphi + 31) / 32;
     k_sample_hw<<<npolys, 256, words * 4, st>>>(out, e.d_mc, e.N, e.logN + 1, nres, e.rid_offset(base), k0, k1,
-                                                stream_id, ps, err);
+                                                stream_id, ps, err, ids);
   } else {
     dim3 grid((e.N + 255) / 256, npolys);
-    k_sample<<<grid, 256, 0, st>>>(out, e.d_mc, e.N, nres, e.rid_offset(base), kind, k0, k1, stream_id, ps, err);
+    k_sample<<<grid, 256, 0, st>>>(out, e.d_mc, e.N, nres, e.rid_offset(base), kind, k0, k1, stream_id, ps, err,
+                                   ids);
   }
   return check_launch("sample");
 }

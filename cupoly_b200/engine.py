@@ -248,6 +248,11 @@ class Engine:
         call("cp_sample", self._h, _ptr(out), base, kind, int(seed), int(stream_id), n, 1 if to_dgt else 0,
              _stream(stream))
 
+    def sample_ids(self, out, base, kind, seed, stream_ids: torch.Tensor, to_dgt=True, stream=None):
+        """Polynomial i of `out` drawn with stream id stream_ids[i] (int32 device tensor)."""
+        call("cp_sample_ids", self._h, _ptr(out), base, kind, int(seed), _ptr(stream_ids), int(stream_ids.numel()),
+             1 if to_dgt else 0, _stream(stream))
+
     # ---- host helpers (folded layout) ----
     def fold(self, coeffs_per_residue: np.ndarray) -> np.ndarray:
         """(nres, nphi) uint64 coefficient rows -> (nres, N, 2) folded layout."""

@@ -1,0 +1,303 @@
+"""Serving loop: continuous batching of homomorphic multiplications of mixed sizes.
+
+A request asks for one BFV multiplication (two ciphertexts -> three output
+polynomials) at one of several ring sizes.  The server keeps one engine per
+size class (its DGT/HPS tables resident in HBM) and a few preallocated batch
+*pools* per class.  The host loop
+
+  * admits arrived requests into the filling pool of their class while the
+    memory budget allows (each admitted request reserves its operand, result
+    and workspace bytes until it completes);
+  * launches a pool as one batched call (operands sampled on the device from
+    the request's identity, then the fused BFV chain) as soon as it is full or
+    its class has fewer than `max_inflight` batches on the GPU -- so requests
+    that arrive while others run join the next batch, and batches of different
+    classes (and up to `max_inflight` of one class) overlap on separate
+    streams;
+  * completes requests when their batch's event fires and frees their budget.
+
+The scheduler is host logic with a pluggable executor; `GpuExecutor` runs the
+batches through the C ABI, `FakeExecutor` (tests) completes them on a timer.
+"""
+from __future__ import annotations
+
+import argparse
+import collections
+import json
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+
+@dataclass
+class SizeClass:
+    nphi: int
+    k: int
+    kl: int
+    t: int
+    max_batch: int
+
+    def request_bytes(self) -> int:
+        """Device bytes one admitted request holds: 4 operands + 3 results over Q
+        and its share of the batch workspace ((7k + 10kl) N per pair)."""
+        N = self.nphi // 2
+        return (4 * self.k + 3 * self.k + 7 * self.k + 10 * self.kl) * N * 16
+
+
+def default_classes(max_batches=(256, 128, 64, 32), t=256) -> List[SizeClass]:
+    """nphi in {4096, 8192, 16384, 32768} with k = nphi / 2048, kl = k + 1."""
+    return [SizeClass(n, n // 2048, n // 2048 + 1, t, b) for n, b in zip((4096, 8192, 16384, 32768), max_batches)]
+
+
+@dataclass
+class Request:
+    rid: int
+    cls: int
+    arrival: float
+    admit: float = -1.0
+    done: float = -1.0
+    slot: int = -1
+    pool: int = -1
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+@dataclass
+class Pool:
+    cls: int
+    index: int
+    capacity: int
+    reqs: List[Request] = field(default_factory=list)
+    busy: bool = False
+    handle: object = None
+
+
+class Scheduler:
+    def __init__(self, classes: Sequence[SizeClass], executor, budget_bytes: int, pools_per_class: int = 3,
+                 max_inflight: int = 2):
+        self.classes = list(classes)
+        self.ex = executor
+        self.budget = int(budget_bytes)
+        self.used = 0
+        self.peak_used = 0
+        self.max_inflight = max_inflight
+        self.pools: List[List[Pool]] = [[Pool(c, i, cl.max_batch) for i in range(pools_per_class)]
+                                        for c, cl in enumerate(self.classes)]
+        self.batches = 0
+        self.batch_sizes: List[int] = []
+        for cl in self.classes:
+            if cl.request_bytes() > self.budget:
+                raise ValueError("budget smaller than one request of nphi=%d" % cl.nphi)
+
+    def _inflight(self, c: int) -> int:
+        return sum(1 for p in self.pools[c] if p.busy)
+
+    def _filling(self, c: int) -> Optional[Pool]:
+        """The pool new requests of class c go to: a partly filled idle pool first."""
+        idle = [p for p in self.pools[c] if not p.busy]
+        for p in idle:
+            if p.reqs:
+                return p
+        return idle[0] if idle else None
+
+    def run(self, requests: Sequence[Request], clock=time.perf_counter, time_limit_s: float = 600.0):
+        """Serve `requests` (arrival times relative to start); returns them completed."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        queues = [collections.deque() for _ in self.classes]
+        n, nxt, done = len(reqs), 0, 0
+        t0 = clock()
+        while done < n:
+            now = clock() - t0
+            if now > time_limit_s:
+                raise TimeoutError("serving loop exceeded %.0f s" % time_limit_s)
+            progressed = False
+            while nxt < n and reqs[nxt].arrival <= now:
+                queues[reqs[nxt].cls].append(reqs[nxt])
+                nxt += 1
+                progressed = True
+            # completions
+            for c in range(len(self.classes)):
+                for p in self.pools[c]:
+                    if p.busy and self.ex.poll(p.handle):
+                        t_done = clock() - t0
+                        self.ex.finish(p)
+                        for r in p.reqs:
+                            r.done = t_done
+                            self.used -= self.classes[c].request_bytes()
+                        done += len(p.reqs)
+                        p.reqs, p.busy, p.handle = [], False, None
+                        progressed = True
+            # admission and launch
+            for c, cl in enumerate(self.classes):
+                q = queues[c]
+                while q:
+                    pool = self._filling(c)
+                    if pool is None:
+                        break
+                    rb = cl.request_bytes()
+                    while q and len(pool.reqs) < pool.capacity and self.used + rb <= self.budget:
+                        r = q.popleft()
+                        r.admit, r.slot, r.pool = now, len(pool.reqs), pool.index
+                        pool.reqs.append(r)
+                        self.used += rb
+                        progressed = True
+                    self.peak_used = max(self.peak_used, self.used)
+                    if pool.reqs and (len(pool.reqs) == pool.capacity or self._inflight(c) < self.max_inflight):
+                        pool.handle = self.ex.launch(c, pool)
+                        pool.busy = True
+                        self.batches += 1
+                        self.batch_sizes.append(len(pool.reqs))
+                        progressed = True
+                    else:
+                        break
+                # a filling pool left partly full launches once an in-flight batch finishes
+                pool = self._filling(c)
+                if pool is not None and pool.reqs and self._inflight(c) < self.max_inflight:
+                    pool.handle = self.ex.launch(c, pool)
+                    pool.busy = True
+                    self.batches += 1
+                    self.batch_sizes.append(len(pool.reqs))
+                    progressed = True
+            if not progressed:
+                busy = any(p.busy for ps in self.pools for p in ps)
+                if not busy and nxt < n and all(not q for q in queues):
+                    wait = reqs[nxt].arrival - (clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.01))
+        return reqs
+
+    def stats(self, reqs: Sequence[Request]) -> Dict:
+        lat = np.array([r.latency for r in reqs]) * 1e3
+        span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
+        return {"requests": len(reqs), "throughput_req_s": round(len(reqs) / span, 1),
+                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "max_ms": round(float(lat.max()), 3), "batches": self.batches,
+                "mean_batch": round(float(np.mean(self.batch_sizes)), 2) if self.batch_sizes else 0,
+                "peak_budget_bytes": self.peak_used, "budget_bytes": self.budget}
+
+
+def poisson_requests(n: int, rate: float, nclasses: int, seed: int) -> List[Request]:
+    """Open-loop Poisson arrivals at `rate` req/s; size class uniform; seeded."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=n)
+    cls = rng.integers(0, nclasses, size=n)
+    t = np.cumsum(gaps)
+    return [Request(i, int(c), float(a)) for i, (c, a) in enumerate(zip(cls, t))]
+
+
+class FakeExecutor:
+    """Completes a batch `delay(c, size)` seconds after launch (scheduler tests)."""
+
+    def __init__(self, delay, clock=time.perf_counter):
+        self.delay = delay
+        self.clock = clock
+        self.launched = []
+
+    def launch(self, c, pool):
+        self.launched.append((c, pool.index, [r.rid for r in pool.reqs]))
+        return self.clock() + self.delay(c, len(pool.reqs))
+
+    def poll(self, handle):
+        return self.clock() >= handle
+
+    def finish(self, pool):
+        pass
+
+
+class GpuExecutor:
+    """Runs batches on the device: operands sampled from each request's identity
+    (stream ids 4 rid + v under one seed, uniform mod q_i, DGT domain), then the
+    fused BFV chain (`cp_bfv_mul_batch`).  One CUDA stream per pool."""
+
+    def __init__(self, classes: Sequence[SizeClass], pools_per_class: int = 3, seed: int = 0xC0FFEE,
+                 keep_results: bool = False):
+        import torch
+
+        from .engine import Engine
+
+        self.torch = torch
+        self.seed = seed
+        self.keep = keep_results
+        self.results: Dict[int, "torch.Tensor"] = {}
+        self.engines, self.pool_bufs = [], []
+        for cl in classes:
+            e = Engine(cl.k, cl.kl, cl.nphi, cl.t)
+            self.engines.append(e)
+            bufs = []
+            for _ in range(pools_per_class):
+                bufs.append({
+                    "ins": [e.empty(0, cl.max_batch) for _ in range(4)],
+                    "out": e.empty(0, 3 * cl.max_batch),
+                    "ws": e.bfv_mul_batch_workspace(cl.max_batch),
+                    "ids_d": torch.empty(4 * cl.max_batch, dtype=torch.int32, device="cuda"),
+                    "ids_h": torch.empty(4 * cl.max_batch, dtype=torch.int32).pin_memory(),
+                    "stream": torch.cuda.Stream(),
+                })
+            self.pool_bufs.append(bufs)
+        torch.cuda.synchronize()
+
+    def launch(self, c, pool):
+        from .engine import QBase, UNIFORM
+
+        torch = self.torch
+        e, b = self.engines[c], self.pool_bufs[c][pool.index]
+        B = len(pool.reqs)
+        ids = np.array([[4 * r.rid + v for r in pool.reqs] for v in range(4)], dtype=np.int64).astype(np.uint32)
+        b["ids_h"][: 4 * B].copy_(torch.from_numpy(ids.reshape(-1).view(np.int32)))
+        s = b["stream"]
+        with torch.cuda.stream(s):
+            b["ids_d"][: 4 * B].copy_(b["ids_h"][: 4 * B], non_blocking=True)
+            for v in range(4):
+                e.sample_ids(b["ins"][v], QBase, UNIFORM, self.seed, b["ids_d"][v * B:(v + 1) * B], stream=s)
+            e.bfv_mul_batch(b["out"], *b["ins"], B, b["ws"], stream=s)
+            ev = torch.cuda.Event()
+            ev.record(s)
+        return ev
+
+    def poll(self, ev):
+        return ev.query()
+
+    def finish(self, pool):
+        if not self.keep:
+            return
+        b = self.pool_bufs[pool.cls][pool.index]
+        B = len(pool.reqs)
+        for r in pool.reqs:
+            self.results[r.rid] = self.torch.stack([b["out"][j * B + r.slot] for j in range(3)]).clone()
+
+    def run_alone(self, c: int, rid: int):
+        """The result of request `rid` computed in a batch of its own."""
+        pool = Pool(c, 0, 1, [Request(rid, c, 0.0, slot=0, pool=0)])
+        ev = self.launch(c, pool)
+        ev.synchronize()
+        b = self.pool_bufs[c][0]
+        return self.torch.stack([b["out"][j] for j in range(3)]).clone()
+
+
+def main():
+    ap = argparse.ArgumentParser(description="BFV serving loop: open-loop Poisson arrivals of mixed sizes")
+    ap.add_argument("--requests", type=int, default=50000)
+    ap.add_argument("--rates", default="5000,10000,20000,40000")
+    ap.add_argument("--budget-gb", type=float, default=40.0)
+    ap.add_argument("--seed", type=int, default=1)
+    a = ap.parse_args()
+    classes = default_classes()
+    ex = GpuExecutor(classes)
+    out = []
+    for rate in [float(x) for x in a.rates.split(",")]:
+        sch = Scheduler(classes, ex, int(a.budget_gb * 2 ** 30))
+        reqs = sch.run(poisson_requests(a.requests, rate, len(classes), a.seed))
+        st = sch.stats(reqs)
+        st["rate_req_s"] = rate
+        out.append(st)
+        print(json.dumps(st), flush=True)
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -176,6 +176,10 @@ int cp_calibrate_int(int kind, int iters, void* sink, long long nthreads, float*
  *      stream_id + npolys - 1; to_dgt != 0 applies the forward DGT (cuPoly does). */
 int cp_sample(const cp_engine* e, void* out, int base, int kind, uint64_t seed, uint32_t stream_id, int npolys,
               int to_dgt, void* stream);
+/* Same, polynomial i drawn with stream id stream_ids[i] (a device array), so a
+ * batch can hold requests whose operands have unrelated identities. */
+int cp_sample_ids(const cp_engine* e, void* out, int base, int kind, uint64_t seed, const uint32_t* stream_ids,
+                  int npolys, int to_dgt, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,101 @@
+"""Serving loop: scheduler logic on the CPU (fake executor) and, on the GPU,
+results that are bit-identical alone and in the mix."""
+import time
+
+import numpy as np
+import pytest
+
+from cupoly_b200.serving import FakeExecutor, Request, Scheduler, SizeClass, default_classes, poisson_requests
+
+
+def _classes():
+    return [SizeClass(4096, 2, 3, 256, 4), SizeClass(8192, 4, 5, 256, 3)]
+
+
+def test_scheduler_completes_everything_in_order_of_constraints():
+    cls = _classes()
+    ex = FakeExecutor(lambda c, b: 0.002 + 0.0005 * b)
+    sch = Scheduler(cls, ex, budget_bytes=10 ** 12)
+    reqs = sch.run(poisson_requests(200, 20000.0, len(cls), seed=3))
+    assert all(r.done >= r.admit >= r.arrival for r in reqs)
+    assert len({r.rid for r in reqs}) == 200
+    for c, pool_idx, rids in ex.launched:
+        assert 1 <= len(rids) <= cls[c].max_batch
+        assert all(reqs[i].cls == c for i in rids)
+    launched = sorted(rid for _, _, rids in ex.launched for rid in rids)
+    assert launched == list(range(200))  # every request in exactly one batch
+    st = sch.stats(reqs)
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_requests_join_batches_while_others_run():
+    """Continuous batching: a class keeps up to max_inflight batches on the device
+    and new arrivals fill the next pool meanwhile."""
+    cls = [SizeClass(4096, 2, 3, 256, 8)]
+    ex = FakeExecutor(lambda c, b: 0.02)
+    sch = Scheduler(cls, ex, budget_bytes=10 ** 12, max_inflight=2)
+    reqs = [Request(i, 0, 0.001 * i) for i in range(40)]
+    sch.run(reqs)
+    sizes = sch.batch_sizes
+    assert sizes[0] == 1 and sizes[1] == 1  # idle GPU: launch at once
+    assert max(sizes) > 1  # later arrivals batched while two batches run
+    assert sum(sizes) == 40
+
+
+def test_admission_respects_memory_budget():
+    cls = _classes()
+    budget = 3 * cls[1].request_bytes()
+    ex = FakeExecutor(lambda c, b: 0.001)
+    sch = Scheduler(cls, ex, budget_bytes=budget)
+    reqs = sch.run(poisson_requests(60, 50000.0, len(cls), seed=5))
+    assert sch.peak_used <= budget
+    assert all(r.done > 0 for r in reqs)
+    with pytest.raises(ValueError):
+        Scheduler(cls, ex, budget_bytes=cls[0].request_bytes() - 1)
+
+
+def test_default_classes_follow_k_equals_nphi_over_2048():
+    for c in default_classes():
+        assert c.k == c.nphi // 2048 and c.kl == c.k + 1 and c.t == 256
+
+
+@pytest.mark.gpu
+def test_results_identical_alone_and_in_the_mix(gpu):
+    import torch
+
+    from cupoly_b200.serving import GpuExecutor
+
+    cls = _classes()
+    ex = GpuExecutor(cls, keep_results=True)
+    sch = Scheduler(cls, ex, budget_bytes=8 << 30)
+    reqs = sch.run(poisson_requests(48, 50000.0, len(cls), seed=9))
+    assert max(sch.batch_sizes) > 1  # some requests really shared batches
+    for r in reqs:
+        alone = ex.run_alone(r.cls, r.rid)
+        assert torch.equal(alone, ex.results[r.rid]), r
+
+
+@pytest.mark.gpu
+def test_served_result_matches_oracle(gpu):
+    """One request per class: operands re-derived by the oracle's sampler restatement."""
+    from cupoly_b200.engine import INVERSE, to_u64
+    from cupoly_b200.serving import GpuExecutor
+    from oracle import coracle
+    from oracle import pyoracle as O
+    from tests.common import unfold
+
+    cls = [SizeClass(64, 2, 3, 256, 2), SizeClass(128, 3, 4, 65537, 2)]
+    ex = GpuExecutor(cls, keep_results=True, seed=77)
+    sch = Scheduler(cls, ex, budget_bytes=1 << 30)
+    reqs = sch.run([Request(0, 0, 0.0), Request(1, 1, 0.0), Request(2, 0, 0.0)])
+    for r in reqs:
+        c = cls[r.cls]
+        e = ex.engines[r.cls]
+        ops = [np.array(O.sample_poly(O.UNIFORM, e.Q, c.nphi, 4 * r.rid + v, 77), dtype=np.uint64)[None]
+               for v in range(4)]
+        ref = coracle.bfv_mul(*ops, e.Q, e.B, c.t)
+        got = ex.results[r.rid].clone()
+        e.dgt(got, 0, INVERSE)
+        got = unfold(to_u64(got))
+        for j in range(3):
+            assert np.array_equal(got[j], ref[j][0])
