@@ -77,6 +77,11 @@ int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int l
     const uint64_t p = kPrimes[i];
     e.primes.push_back(p);
     e.mconst.push_back(h_modconst(p));
+    if (e.mconst.back().r1 >> 32) {  // the lazy base-conversion reduction relies on 2^64 mod p < 2^32
+      delete h;
+      set_error("cp_engine_create: prime with 2^64 mod p >= 2^32 is not supported");
+      return CP_ERR_UNSUPPORTED;
+    }
     e.xi.push_back(canonical_xi(p, kPrimitiveRoots[i], (uint64_t)e.N));
   }
   e.plan = make_plan(e.logN, log_radix ? log_radix : 3);

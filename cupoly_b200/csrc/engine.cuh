@@ -110,6 +110,9 @@ struct Engine {
     int qinv_t, qinv_t_s;          // Q^-1 mod t
     int xi_q, xi_q_s;              // (Q/q_i)^-1 mod q_i
     int rho_q, rho_q_s;            // (Q/q_i) mod q_i
+    int qb_pm, bq_pm;              // mixed-radix weights prod_{l<i} s_l mod m_j, [target][i]
+    int qq_w, bb_w;                // Garner weights of Q and of B, [i][l]
+    int q_pinv, q_pinv_s, b_pinv, b_pinv_s;  // (prod_{j<i} s_j)^-1 mod s_i
   } ho{};
   uint64_t t_shoup_one = 0;        // floor(2^64 / t)
   uint64_t h_q_mod_t = 0, h_qinv_t = 0, h_qinv_t_s = 0;  // Q mod t, Q^-1 mod t

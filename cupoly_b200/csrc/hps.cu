@@ -6,8 +6,9 @@
 // cuPoly estimates the CRT overflow v with doubles (FPERROR = 1e-9) and the
 // HPS rounding with a 64-bit fraction sum in double.  Here both are exact and
 // use only word-size modular arithmetic:
-//  * base conversion: mixed-radix digits d_i of X (MRC), then X mod m by a
-//    Horner evaluation with the constants s_i mod m;
+//  * base conversion: mixed-radix digits d_i of X (MRC), then X mod m as the
+//    dot product sum_i d_i (prod_{l<i} s_l mod m), accumulated in 192 bits
+//    and reduced once per target;
 //  * complex scaling: with r the centred lift of (t x_i mod q_i) over Q,
 //    round(t X / Q) = (t X - r) / Q, hence
 //    round(t X / Q) mod b_j = (t y_j - [r]_{b_j}) Q^-1 mod b_j;
@@ -23,6 +24,24 @@ namespace {
 constexpr int kMaxBase = 24;  // largest |Q| or |B| with a compiled kernel
 
 __device__ __forceinline__ uint64_t red1(uint64_t x, uint64_t m) { return red2p(x, m); }  // x < 2m
+
+// Garner form of the mixed-radix conversion for larger bases:
+// d_i = (x_i - sum_{l<i} d_l W[i][l]) Pinv_i mod s_i, W[i][l] = prod_{j<l} s_j
+// mod s_i, Pinv_i = (prod_{j<i} s_j)^-1 mod s_i; the sums are lazy (192-bit).
+template <int NS>
+__device__ __forceinline__ void mrc_garner(uint64_t (&d)[NS], const ModConst* __restrict__ mcs,
+                                           const uint64_t* __restrict__ W, const uint64_t* __restrict__ pinv,
+                                           const uint64_t* __restrict__ pinv_s) {
+#pragma unroll
+  for (int i = 1; i < NS; ++i) {
+    uint64_t l = 0, h = 0, t = 0;
+#pragma unroll
+    for (int j = 0; j < i; ++j) mac192(l, h, t, d[j], __ldg(W + i * NS + j));
+    const ModConst m = mcs[i];
+    const uint64_t sum = red192(l, h, t, m.p, m.r1, m.r2);
+    d[i] = shoup_mul(d[i] + m.p - sum, __ldg(pinv + i), __ldg(pinv_s + i), m.p);
+  }
+}
 
 // Mixed-radix digits of the value with residues z over primes s.
 template <int NS>
@@ -41,17 +60,16 @@ __device__ __forceinline__ void mrc(uint64_t (&d)[NS], const uint64_t (&s)[NS], 
   }
 }
 
-// X mod m from digits (m a 63-bit prime: digits need one conditional subtract).
+// Sequential MRC for small bases (k(k-1)/2 dependent Shoup steps), Garner with
+// lazy sums from 8 primes on (fewer instructions once the sums are long).
 template <int NS>
-__device__ __forceinline__ uint64_t horner(const uint64_t (&d)[NS], uint64_t m, const uint64_t* __restrict__ hor,
-                                           const uint64_t* __restrict__ hor_s) {
-  uint64_t acc = red1(d[NS - 1], m);
-#pragma unroll
-  for (int i = NS - 2; i >= 0; --i) {
-    acc = shoup_mul(acc, __ldg(hor + i), __ldg(hor_s + i), m);
-    acc = add_mod(acc, red1(d[i], m), m);
-  }
-  return acc;
+__device__ __forceinline__ void mrc_any(uint64_t (&d)[NS], const uint64_t (&s)[NS], const uint64_t* inv,
+                                        const uint64_t* inv_s, const ModConst* mcs, const uint64_t* W,
+                                        const uint64_t* pinv, const uint64_t* pinv_s) {
+  if constexpr (NS >= 8)
+    mrc_garner<NS>(d, mcs, W, pinv, pinv_s);
+  else
+    mrc<NS>(d, s, inv, inv_s);
 }
 
 // X mod t for an arbitrary modulus t < 2^63 (digits reduced by a Shoup step).
@@ -66,6 +84,17 @@ __device__ __forceinline__ uint64_t horner_small(const uint64_t (&d)[NS], uint64
     acc = add_mod(acc, shoup_mul(d[i], 1 % t, one_s, t), t);
   }
   return acc;
+}
+
+// X mod m = sum_i d_i w_i with w_i = prod_{l<i} s_l mod m, accumulated in three
+// words and reduced once (every target prime has 2^64 mod m < 2^32).
+template <int NS>
+__device__ __forceinline__ uint64_t dot_mod(const uint64_t (&d)[NS], const uint64_t* __restrict__ w,
+                                            const ModConst& mt) {
+  uint64_t l = 0, h = 0, t = 0;
+#pragma unroll
+  for (int i = 0; i < NS; ++i) mac192(l, h, t, d[i], __ldg(w + i));
+  return red192(l, h, t, mt.p, mt.r1, mt.r2);
 }
 
 // digits > (prod - 1) / 2 ?
@@ -86,6 +115,8 @@ struct ConvArgs {
   const uint64_t* inv_s;
   const uint64_t* hor;
   const uint64_t* hor_s;
+  const uint64_t* pm;  // mixed-radix weights [target][source]
+  const uint64_t *W, *pinv, *pinv_s;  // Garner constants of the source base
   int src_off, dst_off, ndst, N;
   long long in_stride, out_stride;  // per polynomial, in elements
 };
@@ -98,27 +129,41 @@ __global__ void __launch_bounds__(128) k_basis_ext(ulonglong2* __restrict__ out,
   if (j >= a.N) return;
   in += blockIdx.y * a.in_stride;
   out += blockIdx.y * a.out_stride;
-  uint64_t s[NS], dr[NS], di[NS];
+  if constexpr (NS < 8) {  // small bases: both coefficients at once (more ILP)
+    uint64_t s[NS], dr[NS], di[NS];
 #pragma unroll
-  for (int i = 0; i < NS; ++i) {
-    s[i] = a.mc[a.src_off + i].p;
-    const ulonglong2 x = in[(size_t)i * a.N + j];
-    dr[i] = x.x;
-    di[i] = x.y;
-  }
-  mrc<NS>(dr, s, a.inv, a.inv_s);
-  mrc<NS>(di, s, a.inv, a.inv_s);
-  for (int t = 0; t < a.ndst; ++t) {
-    const uint64_t m = a.mc[a.dst_off + t].p;
-    const uint64_t* h = a.hor + t * (NS - 1);
-    const uint64_t* hs = a.hor_s + t * (NS - 1);
-    out[(size_t)t * a.N + j] = make_ulonglong2(horner<NS>(dr, m, h, hs), horner<NS>(di, m, h, hs));
+    for (int i = 0; i < NS; ++i) {
+      s[i] = a.mc[a.src_off + i].p;
+      const ulonglong2 x = in[(size_t)i * a.N + j];
+      dr[i] = x.x;
+      di[i] = x.y;
+    }
+    mrc_any<NS>(dr, s, a.inv, a.inv_s, a.mc + a.src_off, a.W, a.pinv, a.pinv_s);
+    mrc_any<NS>(di, s, a.inv, a.inv_s, a.mc + a.src_off, a.W, a.pinv, a.pinv_s);
+    for (int t = 0; t < a.ndst; ++t) {
+      const ModConst mt = a.mc[a.dst_off + t];
+      const uint64_t* w = a.pm + t * NS;
+      out[(size_t)t * a.N + j] = make_ulonglong2(dot_mod<NS>(dr, w, mt), dot_mod<NS>(di, w, mt));
+    }
+  } else {  // large bases: one coefficient at a time keeps the digits in registers
+    const uint64_t* iw = reinterpret_cast<const uint64_t*>(in);
+    uint64_t* ow = reinterpret_cast<uint64_t*>(out);
+#pragma unroll 1
+    for (int comp = 0; comp < 2; ++comp) {
+      uint64_t s[NS], d[NS];
+#pragma unroll
+      for (int i = 0; i < NS; ++i) d[i] = iw[2 * ((size_t)i * a.N + j) + comp];
+      mrc_any<NS>(d, s, a.inv, a.inv_s, a.mc + a.src_off, a.W, a.pinv, a.pinv_s);
+      for (int t = 0; t < a.ndst; ++t)
+        ow[2 * ((size_t)t * a.N + j) + comp] = dot_mod<NS>(d, a.pm + t * NS, a.mc[a.dst_off + t]);
+    }
   }
 }
 
 struct ScaleArgs {
   const ModConst* mc;
-  const uint64_t *inv, *inv_s, *hor, *hor_s, *half;
+  const uint64_t *inv, *inv_s, *hor, *hor_s, *half, *pm;
+  const uint64_t *W, *pinv, *pinv_s;  // Garner constants of Q
   const uint64_t *t_q, *t_q_s, *t_b, *t_b_s, *q_mod_b, *qinv_b, *qinv_b_s;
   int k, kl, N;
   long long q_stride, b_stride, out_stride;
@@ -134,6 +179,31 @@ __global__ void __launch_bounds__(128) k_complex_scaling(ulonglong2* __restrict_
   in_q += blockIdx.y * a.q_stride;
   in_b += blockIdx.y * a.b_stride;
   out_b += blockIdx.y * a.out_stride;
+  if constexpr (NQ >= 8) {  // large bases: one coefficient at a time (register pressure)
+    const uint64_t* qw = reinterpret_cast<const uint64_t*>(in_q);
+    const uint64_t* bw = reinterpret_cast<const uint64_t*>(in_b);
+    uint64_t* ow = reinterpret_cast<uint64_t*>(out_b);
+#pragma unroll 1
+    for (int comp = 0; comp < 2; ++comp) {
+      uint64_t s[NQ], d[NQ];
+#pragma unroll
+      for (int i = 0; i < NQ; ++i) {
+        const uint64_t p = a.mc[i].p;
+        d[i] = shoup_mul(qw[2 * ((size_t)i * a.N + j) + comp], __ldg(a.t_q + i), __ldg(a.t_q_s + i), p);
+      }
+      mrc_any<NQ>(d, s, a.inv, a.inv_s, a.mc, a.W, a.pinv, a.pinv_s);
+      const bool neg = above_half<NQ>(d, a.half);
+      for (int t = 0; t < a.kl; ++t) {
+        const ModConst mt = a.mc[a.k + t];
+        const uint64_t b = mt.p;
+        uint64_t r = dot_mod<NQ>(d, a.pm + t * NQ, mt);
+        if (neg) r = sub_mod(r, __ldg(a.q_mod_b + t), b);
+        const uint64_t ty = shoup_mul(bw[2 * ((size_t)t * a.N + j) + comp], __ldg(a.t_b + t), __ldg(a.t_b_s + t), b);
+        ow[2 * ((size_t)t * a.N + j) + comp] = shoup_mul(ty + b - r, __ldg(a.qinv_b + t), __ldg(a.qinv_b_s + t), b);
+      }
+    }
+    return;
+  }
   uint64_t s[NQ], dr[NQ], di[NQ];
 #pragma unroll
   for (int i = 0; i < NQ; ++i) {
@@ -143,17 +213,16 @@ __global__ void __launch_bounds__(128) k_complex_scaling(ulonglong2* __restrict_
     dr[i] = shoup_mul(x.x, tq, tqs, s[i]);
     di[i] = shoup_mul(x.y, tq, tqs, s[i]);
   }
-  mrc<NQ>(dr, s, a.inv, a.inv_s);
-  mrc<NQ>(di, s, a.inv, a.inv_s);
+  mrc_any<NQ>(dr, s, a.inv, a.inv_s, a.mc, a.W, a.pinv, a.pinv_s);
+  mrc_any<NQ>(di, s, a.inv, a.inv_s, a.mc, a.W, a.pinv, a.pinv_s);
   const bool nr = above_half<NQ>(dr, a.half);
   const bool ni = above_half<NQ>(di, a.half);
   for (int t = 0; t < a.kl; ++t) {
-    const uint64_t b = a.mc[a.k + t].p;
-    const uint64_t* h = a.hor + t * (NQ - 1);
-    const uint64_t* hs = a.hor_s + t * (NQ - 1);
+    const ModConst mt = a.mc[a.k + t];
+    const uint64_t b = mt.p;
     const uint64_t qb = __ldg(a.q_mod_b + t);
-    uint64_t rr = horner<NQ>(dr, b, h, hs);
-    uint64_t ri = horner<NQ>(di, b, h, hs);
+    uint64_t rr = dot_mod<NQ>(dr, a.pm + t * NQ, mt);
+    uint64_t ri = dot_mod<NQ>(di, a.pm + t * NQ, mt);
     if (nr) rr = sub_mod(rr, qb, b);
     if (ni) ri = sub_mod(ri, qb, b);
     const ulonglong2 y = in_b[(size_t)t * a.N + j];
@@ -176,40 +245,47 @@ __global__ void __launch_bounds__(128) k_scale_to_q(ulonglong2* __restrict__ out
   in_q += blockIdx.y * a.q_stride;
   in_b += blockIdx.y * a.b_stride;
   uint64_t* o = reinterpret_cast<uint64_t*>(out_q + blockIdx.y * a.q_stride);
+  // primes are re-read from the (cached) constant table instead of living in
+  // registers: the digit arrays are what must stay resident
   uint64_t s[NQ], sb[NB];
+  if constexpr (NQ < 8) {
 #pragma unroll
-  for (int i = 0; i < NQ; ++i) s[i] = a.mc[i].p;
+    for (int i = 0; i < NQ; ++i) s[i] = a.mc[i].p;
+  }
+  if constexpr (NB < 8) {
 #pragma unroll
-  for (int i = 0; i < NB; ++i) sb[i] = a.mc[NQ + i].p;
+    for (int i = 0; i < NB; ++i) sb[i] = a.mc[NQ + i].p;
+  }
 #pragma unroll 1
   for (int comp = 0; comp < 2; ++comp) {
     uint64_t d[NQ], u[NB];
 #pragma unroll
     for (int i = 0; i < NQ; ++i) {
       const uint64_t* x = reinterpret_cast<const uint64_t*>(in_q + (size_t)i * a.N + j);
-      d[i] = shoup_mul(x[comp], __ldg(a.t_q + i), __ldg(a.t_q_s + i), s[i]);
+      d[i] = shoup_mul(x[comp], __ldg(a.t_q + i), __ldg(a.t_q_s + i), a.mc[i].p);
     }
-    mrc<NQ>(d, s, a.inv, a.inv_s);
+    mrc_any<NQ>(d, s, a.inv, a.inv_s, a.mc, a.W, a.pinv, a.pinv_s);
     const bool neg = above_half<NQ>(d, a.half);
 #pragma unroll
     for (int t = 0; t < NB; ++t) {
-      const uint64_t b = sb[t];
-      uint64_t r = horner<NQ>(d, b, a.hor + t * (NQ - 1), a.hor_s + t * (NQ - 1));
+      const uint64_t b = a.mc[NQ + t].p;
+      uint64_t r = dot_mod<NQ>(d, a.pm + t * NQ, a.mc[NQ + t]);
       if (neg) r = sub_mod(r, __ldg(a.q_mod_b + t), b);
       const uint64_t* y = reinterpret_cast<const uint64_t*>(in_b + (size_t)t * a.N + j);
       const uint64_t ty = shoup_mul(y[comp], __ldg(a.t_b + t), __ldg(a.t_b_s + t), b);
       u[t] = shoup_mul(ty + b - r, __ldg(a.qinv_b + t), __ldg(a.qinv_b_s + t), b);
     }
-    mrc<NB>(u, sb, c.inv, c.inv_s);
+    mrc_any<NB>(u, sb, c.inv, c.inv_s, c.mc + c.src_off, c.W, c.pinv, c.pinv_s);
 #pragma unroll
     for (int i = 0; i < NQ; ++i)
-      o[2 * ((size_t)i * a.N + j) + comp] = horner<NB>(u, s[i], c.hor + i * (NB - 1), c.hor_s + i * (NB - 1));
+      o[2 * ((size_t)i * a.N + j) + comp] = dot_mod<NB>(u, c.pm + i * NB, a.mc[i]);
   }
 }
 
 struct SimpleArgs {
   const ModConst* mc;
   const uint64_t *inv, *inv_s, *hor, *hor_s, *half, *t_q, *t_q_s;
+  const uint64_t *W, *pinv, *pinv_s;  // Garner constants of Q
   uint64_t t, one_s, q_mod_t, qinv_t, qinv_t_s;
   int N;
 };
@@ -220,6 +296,24 @@ __global__ void __launch_bounds__(128) k_simple_scaling(ulonglong2* __restrict__
                                                         const ulonglong2* __restrict__ in_q, SimpleArgs a) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.N) return;
+  if constexpr (NQ >= 8) {  // large bases: one coefficient at a time (register pressure)
+    const uint64_t* qw = reinterpret_cast<const uint64_t*>(in_q);
+    uint64_t res[2];
+#pragma unroll 1
+    for (int comp = 0; comp < 2; ++comp) {
+      uint64_t s[NQ], d[NQ];
+#pragma unroll
+      for (int i = 0; i < NQ; ++i)
+        d[i] = shoup_mul(qw[2 * ((size_t)i * a.N + j) + comp], __ldg(a.t_q + i), __ldg(a.t_q_s + i), a.mc[i].p);
+      mrc_any<NQ>(d, s, a.inv, a.inv_s, a.mc, a.W, a.pinv, a.pinv_s);
+      const bool neg = above_half<NQ>(d, a.half);
+      uint64_t r = horner_small<NQ>(d, a.t, a.one_s, a.hor, a.hor_s);
+      if (neg) r = sub_mod(r, a.q_mod_t, a.t);
+      res[comp] = shoup_mul(neg_mod(r, a.t), a.qinv_t, a.qinv_t_s, a.t);
+    }
+    out[j] = make_ulonglong2(res[0], res[1]);
+    return;
+  }
   uint64_t s[NQ], dr[NQ], di[NQ];
 #pragma unroll
   for (int i = 0; i < NQ; ++i) {
@@ -229,8 +323,8 @@ __global__ void __launch_bounds__(128) k_simple_scaling(ulonglong2* __restrict__
     dr[i] = shoup_mul(x.x, tq, tqs, s[i]);
     di[i] = shoup_mul(x.y, tq, tqs, s[i]);
   }
-  mrc<NQ>(dr, s, a.inv, a.inv_s);
-  mrc<NQ>(di, s, a.inv, a.inv_s);
+  mrc_any<NQ>(dr, s, a.inv, a.inv_s, a.mc, a.W, a.pinv, a.pinv_s);
+  mrc_any<NQ>(di, s, a.inv, a.inv_s, a.mc, a.W, a.pinv, a.pinv_s);
   const bool nr = above_half<NQ>(dr, a.half);
   const bool ni = above_half<NQ>(di, a.half);
   uint64_t rr = horner_small<NQ>(dr, a.t, a.one_s, a.hor, a.hor_s);
@@ -281,16 +375,24 @@ int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int n
   if (q_to_b) {
     a.inv = e.d_hps + e.ho.qb_inv;
     a.inv_s = e.d_hps + e.ho.qb_inv_s;
+    a.W = e.d_hps + e.ho.qq_w;
+    a.pinv = e.d_hps + e.ho.q_pinv;
+    a.pinv_s = e.d_hps + e.ho.q_pinv_s;
     a.hor = e.d_hps + e.ho.qb_hor;
     a.hor_s = e.d_hps + e.ho.qb_hor_s;
+    a.pm = e.d_hps + e.ho.qb_pm;
     a.src_off = 0;
     a.dst_off = e.k;
     a.ndst = e.kl;
   } else {
     a.inv = e.d_hps + e.ho.bq_inv;
     a.inv_s = e.d_hps + e.ho.bq_inv_s;
+    a.W = e.d_hps + e.ho.bb_w;
+    a.pinv = e.d_hps + e.ho.b_pinv;
+    a.pinv_s = e.d_hps + e.ho.b_pinv_s;
     a.hor = e.d_hps + e.ho.bq_hor;
     a.hor_s = e.d_hps + e.ho.bq_hor_s;
+    a.pm = e.d_hps + e.ho.bq_pm;
     a.src_off = e.k;
     a.dst_off = 0;
     a.ndst = e.k;
@@ -310,7 +412,11 @@ static ScaleArgs scale_args(const Engine& e) {
   a.mc = e.d_mc;
   a.inv = e.d_hps + e.ho.qb_inv;
   a.inv_s = e.d_hps + e.ho.qb_inv_s;
+  a.W = e.d_hps + e.ho.qq_w;
+  a.pinv = e.d_hps + e.ho.q_pinv;
+  a.pinv_s = e.d_hps + e.ho.q_pinv_s;
   a.hor = e.d_hps + e.ho.qb_hor;
+  a.pm = e.d_hps + e.ho.qb_pm;
   a.hor_s = e.d_hps + e.ho.qb_hor_s;
   a.half = e.d_hps + e.ho.qb_half;
   a.t_q = e.d_hps + e.ho.t_q;
@@ -352,15 +458,21 @@ int launch_scale_to_q_n(ulonglong2* o, const ulonglong2* q, const ulonglong2* b,
 
 int hps_scale_to_q(const Engine& e, void* out_q, const void* in_q, const void* in_b, void* scratch_b, int npolys,
                    cudaStream_t st) {
-  if (e.kl == e.k + 1 && e.k <= 16) {  // fused kernel: the B residues never leave registers
+  // fused kernel for small bases (the B residues never leave registers); from
+  // 8 primes on the two separate kernels keep more warps resident and win
+  if (e.kl == e.k + 1 && e.k < 8) {
     ScaleArgs a = scale_args(e);
     ConvArgs c;
     c.mc = e.d_mc;
     c.N = e.N;
     c.inv = e.d_hps + e.ho.bq_inv;
     c.inv_s = e.d_hps + e.ho.bq_inv_s;
+    c.W = e.d_hps + e.ho.bb_w;
+    c.pinv = e.d_hps + e.ho.b_pinv;
+    c.pinv_s = e.d_hps + e.ho.b_pinv_s;
     c.hor = e.d_hps + e.ho.bq_hor;
     c.hor_s = e.d_hps + e.ho.bq_hor_s;
+    c.pm = e.d_hps + e.ho.bq_pm;
     c.src_off = e.k;
     c.dst_off = 0;
     c.ndst = e.k;
@@ -385,6 +497,9 @@ int hps_simple_scaling(const Engine& e, void* out_t, const void* in_q, cudaStrea
   a.mc = e.d_mc;
   a.inv = e.d_hps + e.ho.qb_inv;
   a.inv_s = e.d_hps + e.ho.qb_inv_s;
+  a.W = e.d_hps + e.ho.qq_w;
+  a.pinv = e.d_hps + e.ho.q_pinv;
+  a.pinv_s = e.d_hps + e.ho.q_pinv_s;
   a.hor = e.d_hps + e.ho.qt_hor;
   a.hor_s = e.d_hps + e.ho.qt_hor_s;
   a.half = e.d_hps + e.ho.qb_half;

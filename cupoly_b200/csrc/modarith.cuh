@@ -25,9 +25,45 @@ namespace cpoly {
 struct ModConst {
   uint64_t p;       // the prime
   uint64_t pneg;    // -p^-1 mod 2^64
-  uint64_t r1;      // 2^64 mod p
+  uint64_t r1;      // 2^64 mod p (below 2^32 for every prime of the table)
   uint64_t r1s;     // shoup companion of r1
+  uint64_t r2;      // 2^128 mod p
 };
+
+// Three-word accumulation (t:h:l) += a * b, for lazily reduced dot products.
+CP_HD void mac192(uint64_t& l, uint64_t& h, uint64_t& t, uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+  const uint64_t pl = a * b, ph = __umul64hi(a, b);
+  asm("add.cc.u64 %0, %0, %3;\n\taddc.cc.u64 %1, %1, %4;\n\taddc.u64 %2, %2, 0;"
+      : "+l"(l), "+l"(h), "+l"(t)
+      : "l"(pl), "l"(ph));
+#else
+  unsigned __int128 pr = (unsigned __int128)a * b;
+  unsigned __int128 lo = (unsigned __int128)l + (uint64_t)pr;
+  unsigned __int128 hi = (unsigned __int128)h + (uint64_t)(pr >> 64) + (uint64_t)(lo >> 64);
+  l = (uint64_t)lo;
+  h = (uint64_t)hi;
+  t += (uint64_t)(hi >> 64);
+#endif
+}
+
+// (t 2^128 + h 2^64 + l) mod p for t < 2^8, using r1 = 2^64 mod p < 2^32 and
+// r2 = 2^128 mod p: fold the high words down three times, then at most two
+// subtractions (the value is below 2^64 < 3p).
+CP_HD uint64_t red192(uint64_t l, uint64_t h, uint64_t t, uint64_t p, uint64_t r1, uint64_t r2) {
+  const uint32_t r = (uint32_t)r1;  // r1 < 2^32: 64 x 32-bit products below
+  // y = l + h r1 + t r2 < 2^97
+  unsigned __int128 y = (unsigned __int128)l + (unsigned __int128)h * r + (unsigned __int128)t * r2;
+  // z = lo(y) + hi(y) r1 < 2^66
+  unsigned __int128 z = (unsigned __int128)(uint64_t)y + (unsigned __int128)(uint64_t)(y >> 64) * r;
+  // w = lo(z) + hi(z) r1 < 2^64 + 2^34; one carry at most
+  const uint64_t zl = (uint64_t)z, zh = (uint64_t)(z >> 64);
+  uint64_t w = zl + zh * r1;
+  if (w < zl) w += r1;
+  w = w >= p ? w - p : w;
+  w = w >= p ? w - p : w;
+  return w;
+}
 
 CP_HD uint64_t mulhi64(uint64_t a, uint64_t b) {
 #ifdef __CUDA_ARCH__
@@ -150,6 +186,7 @@ inline ModConst h_modconst(uint64_t p) {
   m.pneg = (uint64_t)0 - inv;
   m.r1 = (uint64_t)(((unsigned __int128)1 << 64) % p);
   m.r1s = h_shoup(m.r1, p);
+  m.r2 = h_mulmod(m.r1, m.r1, p);
   return m;
 }
 

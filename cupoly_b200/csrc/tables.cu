@@ -287,6 +287,37 @@ int build_tables(Engine& e) {
     e.ho.bq_hor_s = append(c);
   }
   {
+    // mixed-radix weights: X mod m = sum_i d_i (prod_{l<i} s_l mod m)
+    auto weights = [&](const std::vector<uint64_t>& s, const std::vector<uint64_t>& m) {
+      std::vector<uint64_t> w;
+      for (size_t j = 0; j < m.size(); ++j) {
+        uint64_t acc = 1 % m[j];
+        for (size_t i = 0; i < s.size(); ++i) {
+          w.push_back(acc);
+          acc = h_mulmod(acc, s[i] % m[j], m[j]);
+        }
+      }
+      return w;
+    };
+    e.ho.qb_pm = append(weights(Q, B));
+    e.ho.bq_pm = append(weights(B, Q));
+    // Garner constants of each base: W[i][l] = prod_{j<l} s_j mod s_i, Pinv_i
+    e.ho.qq_w = append(weights(Q, Q));
+    e.ho.bb_w = append(weights(B, B));
+    auto pinv = [&](const std::vector<uint64_t>& s, int& off_v, int& off_s) {
+      std::vector<uint64_t> v, c;
+      for (size_t i = 0; i < s.size(); ++i) {
+        uint64_t pr = 1 % s[i];
+        for (size_t j = 0; j < i; ++j) pr = h_mulmod(pr, s[j] % s[i], s[i]);
+        push_pair(h_invmod(pr, s[i]), s[i], v, c);
+      }
+      off_v = append(v);
+      off_s = append(c);
+    };
+    pinv(Q, e.ho.q_pinv, e.ho.q_pinv_s);
+    pinv(B, e.ho.b_pinv, e.ho.b_pinv_s);
+  }
+  {
     std::vector<uint64_t> v, c;
     horner(Q, std::vector<uint64_t>{e.t}, v, c);
     e.ho.qt_hor = append(v);
