@@ -46,6 +46,8 @@ SIGNATURES = {
     "cp_workspace_bytes": (C.c_size_t, [_vp]),
     "cp_engine_check": (_i, [_vp, _vp]),
     "cp_dgt": (_i, [_vp, _vp, _i, _i, _i, _i64, _vp]),
+    "cp_dgt_list": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
+    "cp_mul_list": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "cp_add": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
     "cp_sub": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
     "cp_double_add": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),

@@ -1,0 +1,152 @@
+"""Batched forms under CUDA graphs.
+
+`MixedPolymul`: many independent negacyclic products c_i = a_i b_i in
+Z_q[x]/(x^nphi_i + 1) with per-instance ring size nphi_i and RNS width k_i.
+Instances are grouped by ring size; inside a group every residue of every
+instance is one entry of a work list (data pointer implied by its position,
+prime index = its residue number), so one forward DGT launch per operand, one
+pointwise launch and one inverse launch serve the whole group whatever the mix
+of widths.  All groups' launches are captured once in a CUDA graph and
+replayed.
+
+`BFVBatch`: the fused BFV multiplication chain over a fixed batch of pairs,
+captured in a CUDA graph.
+"""
+from __future__ import annotations
+
+from collections import OrderedDict
+from typing import List, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from .engine import FORWARD, INVERSE, QBase, Engine, _ptr, _stream, from_u64, to_u64
+from ._lib import call
+
+
+class MixedPolymul:
+    def __init__(self, specs: Sequence[Tuple[int, int]], kmax: int = 8, autotune: bool = False):
+        """specs[i] = (nphi_i, k_i) with 1 <= k_i <= kmax."""
+        self.specs = list(specs)
+        self.groups = OrderedDict()  # nphi -> dict
+        for i, (nphi, k) in enumerate(self.specs):
+            if not 1 <= k <= kmax:
+                raise ValueError("k must be in [1, kmax]")
+            self.groups.setdefault(nphi, {"inst": []})["inst"].append(i)
+        self.where = {}  # instance -> (nphi, first residue row)
+        for nphi, g in self.groups.items():
+            lr = 0
+            if autotune:
+                from .autotune import best_log_radix
+
+                lr = best_log_radix(nphi)
+            g["engine"] = Engine(kmax, 1, nphi, 256, lr)
+            rids, row = [], 0
+            for i in g["inst"]:
+                k = self.specs[i][1]
+                self.where[i] = (nphi, row)
+                rids.extend(range(k))
+                row += k
+            g["rows"] = row
+            g["rid"] = torch.tensor(rids, dtype=torch.int32, device="cuda")
+            N = nphi // 2
+            g["a"] = torch.zeros((row, N, 2), dtype=torch.int64, device="cuda")
+            g["b"] = torch.zeros_like(g["a"])
+            g["wa"] = torch.empty_like(g["a"])
+            g["wb"] = torch.empty_like(g["a"])
+            g["c"] = torch.empty_like(g["a"])
+        self.graph = None
+
+    # ---- data ----
+    def set_inputs(self, i: int, a_rows: np.ndarray, b_rows: np.ndarray):
+        """Coefficient rows (k_i, nphi_i), residues mod the first k_i primes."""
+        nphi, row = self.where[i]
+        k = self.specs[i][1]
+        g = self.groups[nphi]
+        N = nphi // 2
+        for dst, src in ((g["a"], a_rows), (g["b"], b_rows)):
+            src = np.asarray(src, dtype=np.uint64)
+            dst[row:row + k] = from_u64(np.stack([src[:, :N], src[:, N:]], axis=-1))
+
+    def result(self, i: int) -> np.ndarray:
+        nphi, row = self.where[i]
+        k = self.specs[i][1]
+        x = to_u64(self.groups[nphi]["c"][row:row + k])
+        return np.concatenate([x[..., 0], x[..., 1]], axis=-1)
+
+    # ---- execution ----
+    def _launch(self, stream=None):
+        s = _stream(stream)
+        for g in self.groups.values():
+            e, n, rid = g["engine"], g["rows"], g["rid"]
+            g["wa"].copy_(g["a"])
+            g["wb"].copy_(g["b"])
+            call("cp_dgt_list", e.handle, _ptr(g["wa"]), _ptr(rid), n, FORWARD, s)
+            call("cp_dgt_list", e.handle, _ptr(g["wb"]), _ptr(rid), n, FORWARD, s)
+            call("cp_mul_list", e.handle, _ptr(g["c"]), _ptr(g["wa"]), _ptr(g["wb"]), _ptr(rid), n, s)
+            call("cp_dgt_list", e.handle, _ptr(g["c"]), _ptr(rid), n, INVERSE, s)
+
+    def run(self):
+        """Eager execution (also warms up every kernel before capture)."""
+        self._launch()
+
+    def capture(self):
+        self._launch()  # first launches set kernel attributes outside the capture
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(self.graph, stream=s):
+                self._launch(stream=s)
+        torch.cuda.current_stream().wait_stream(s)
+        return self.graph
+
+    def replay(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    def launches_per_run(self) -> int:
+        return 4 * len(self.groups)
+
+    def algorithmic_bytes(self) -> int:
+        """24 nphi k bytes per product: read a, b and write c (16 B per Gaussian element)."""
+        return sum(24 * nphi * k for nphi, k in self.specs)
+
+
+class BFVBatch:
+    """Fused BFV multiplication of a fixed batch of pairs, captured in a CUDA graph."""
+
+    def __init__(self, engine: Engine, npairs: int):
+        self.e = engine
+        self.P = npairs
+        self.ins = [engine.empty(QBase, npairs) for _ in range(4)]
+        self.out = engine.empty(QBase, 3 * npairs)
+        self.ws = engine.bfv_mul_batch_workspace(npairs)
+        self.graph = None
+
+    def _launch(self, stream=None):
+        self.e.bfv_mul_batch(self.out, *self.ins, self.P, self.ws, stream=stream)
+
+    def capture(self):
+        self._launch()
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(self.graph, stream=s):
+                self._launch(stream=s)
+        torch.cuda.current_stream().wait_stream(s)
+
+    def replay(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+
+def random_specs(n: int, seed: int, sizes=(2048, 4096, 8192, 16384), kmax: int = 8) -> List[Tuple[int, int]]:
+    """n (nphi, k) draws: nphi uniform over `sizes`, k uniform in 1..kmax (seeded)."""
+    rng = np.random.default_rng(seed)
+    return [(int(sizes[rng.integers(len(sizes))]), int(rng.integers(1, kmax + 1))) for _ in range(n)]

@@ -186,6 +186,19 @@ int cp_dgt(const cp_engine* h, void* data, int base, int direction, int npolys, 
   return launch_dgt(h->e, data, base, npolys, poly_stride, direction == CP_INVERSE, S(stream));
 }
 
+int cp_dgt_list(const cp_engine* h, void* data, const int* rid_list, int nlist, int direction, void* stream) {
+  CP_REQUIRE(h && data && rid_list && nlist >= 0, "cp_dgt_list: bad argument");
+  CP_REQUIRE(direction == CP_FORWARD || direction == CP_INVERSE, "cp_dgt_list: bad direction");
+  return launch_dgt_list(h->e, data, rid_list, nlist, direction == CP_INVERSE, S(stream));
+}
+
+int cp_mul_list(const cp_engine* h, void* c, const void* a, const void* b, const int* rid_list, int nlist,
+                void* stream) {
+  CP_REQUIRE(h && c && a && b && rid_list && nlist >= 0, "cp_mul_list: bad argument");
+  if (nlist == 0) return CP_OK;
+  return pw_mul_list(h->e, c, a, b, rid_list, nlist, S(stream));
+}
+
 #define PW_CHECK(name) CP_REQUIRE(valid_base(h, base) && base != CP_TBASE, name ": bad engine or base")
 
 int cp_add(const cp_engine* h, void* c, const void* a, const void* b, int base, void* stream) {

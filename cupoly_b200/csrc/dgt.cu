@@ -10,10 +10,10 @@ namespace {
 
 template <int LOGNC, int LOGR>
 int run_cta(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres, int rid_off,
-            int npolys, long long poly_stride, bool inverse, bool twist, cudaStream_t st) {
+            int npolys, long long poly_stride, bool inverse, bool twist, cudaStream_t st, const int* rid_list) {
   constexpr int T = (1 << LOGNC) >> LOGR;
   constexpr int smem = dgt_smem_bytes<LOGNC, LOGR>();
-  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc};
+  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc, rid_list};
   const int S = e.plan.S;
   const long long blocks = (long long)npolys * nres << S;
   if (blocks <= 0) return 0;
@@ -36,7 +36,7 @@ int run_cta(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const Inv
 }
 
 using RunFn = int (*)(const Engine&, ulonglong2*, const ulonglong2*, const InvSrc&, int, int, int, long long, bool,
-                      bool, cudaStream_t);
+                      bool, cudaStream_t, const int*);
 
 // (logNc, effective logR) -> instantiation.
 RunFn pick(int logNc, int logR) {
@@ -53,8 +53,8 @@ RunFn pick(int logNc, int logR) {
 }
 
 int launch_split(const Engine& e, ulonglong2* data, const ulonglong2* src, int nres, int rid_off, int npolys,
-                 long long poly_stride, bool inverse, cudaStream_t st) {
-  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc};
+                 long long poly_stride, bool inverse, cudaStream_t st, const int* rid_list = nullptr) {
+  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc, rid_list};
   const int Nc = 1 << e.plan.logNc;
   const long long blocks = (long long)npolys * nres * (Nc / 256);
   if (blocks > 0x7fffffffLL) {
@@ -108,11 +108,11 @@ int launch_dgt_ex(const Engine& e, void* dst_v, const void* fsrc_v, const InvSrc
     if (S > 0) {
       int rc = launch_split(e, data, fsrc, nres, rid_off, npolys, poly_stride, false, st);
       if (rc) return rc;
-      return fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, false, false, st);
+      return fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, false, false, st, nullptr);
     }
-    return fn(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, false, true, st);
+    return fn(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, false, true, st, nullptr);
   }
-  int rc = fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, true, S == 0, st);
+  int rc = fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, true, S == 0, st, nullptr);
   if (rc || S == 0) return rc;
   return launch_split(e, data, nullptr, nres, rid_off, npolys, poly_stride, true, st);
 }
@@ -120,6 +120,36 @@ int launch_dgt_ex(const Engine& e, void* dst_v, const void* fsrc_v, const InvSrc
 int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly_stride, bool inverse,
                cudaStream_t st) {
   return launch_dgt_ex(e, data, nullptr, nullptr, base, npolys, poly_stride, inverse, st);
+}
+
+// Work-list form: `nlist` residues of N elements back to back, residue i
+// transformed with engine prime rid_list[i] (a device array).  Residues of
+// different polynomials and widths share one launch.
+int launch_dgt_list(const Engine& e, void* data_v, const int* rid_list, int nlist, bool inverse, cudaStream_t st) {
+  if (nlist <= 0) return 0;
+  RunFn fn = pick(e.plan.logNc, e.plan.logR);
+  if (!fn) {
+    set_error("dgt: no kernel for this size");
+    return 3;
+  }
+  ulonglong2* data = reinterpret_cast<ulonglong2*>(data_v);
+  InvSrc isrc{};
+  isrc.p[0] = data;
+  isrc.mode = 0;
+  isrc.npairs = 1;
+  const long long stride = e.N;
+  const int S = e.plan.S;
+  if (!inverse) {
+    if (S > 0) {
+      int rc = launch_split(e, data, nullptr, 1, 0, nlist, stride, false, st, rid_list);
+      if (rc) return rc;
+      return fn(e, data, nullptr, isrc, 1, 0, nlist, stride, false, false, st, rid_list);
+    }
+    return fn(e, data, nullptr, isrc, 1, 0, nlist, stride, false, true, st, rid_list);
+  }
+  int rc = fn(e, data, nullptr, isrc, 1, 0, nlist, stride, true, S == 0, st, rid_list);
+  if (rc || S == 0) return rc;
+  return launch_split(e, data, nullptr, 1, 0, nlist, stride, true, st, rid_list);
 }
 
 }  // namespace cpoly

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   const int pr = blockIdx.x >> S;
   const int r = pr % nres;
   const int poly = pr / nres;
-  const int rid = rid_off + r;
+  const int rid = A.rid_list ? A.rid_list[pr] : rid_off + r;
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
   const size_t off = poly * poly_stride + ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   const int pr = blockIdx.x >> S;
   const int r = pr % nres;
   const int poly = pr / nres;
-  const int rid = rid_off + r;
+  const int rid = A.rid_list ? A.rid_list[pr] : rid_off + r;
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
   const size_t inner = ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(256)
   const int Lw = (blockIdx.x % chunks) * 256 + threadIdx.x;
   const int r = pr % nres;
   const int poly = pr / nres;
-  const int rid = rid_off + r;
+  const int rid = A.rid_list ? A.rid_list[pr] : rid_off + r;
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
   ulonglong2* x = data + poly * poly_stride + ((size_t)r << (logNc + S));

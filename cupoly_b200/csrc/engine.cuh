@@ -53,6 +53,7 @@ struct DgtArgs {
   int stride;              // entries per residue block
   DgtTableLayout L;
   const ModConst* mc;      // per engine residue
+  const int* rid_list;     // work list: residue i of the data uses engine prime rid_list[i] (nullptr: base order)
 };
 
 // Where the inverse DGT reads its input.

@@ -53,5 +53,6 @@ int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly
 // per `isrc` (nullptr = in place).  Output always to `dst`.
 int launch_dgt_ex(const Engine& e, void* dst, const void* fsrc, const InvSrc* isrc, int base, int npolys,
                   long long poly_stride, bool inverse, cudaStream_t st);
+int launch_dgt_list(const Engine& e, void* data, const int* rid_list, int nlist, bool inverse, cudaStream_t st);
 
 }  // namespace cpoly

@@ -18,16 +18,16 @@ using u2 = ulonglong2;
 // blockIdx.y enumerates (polynomial, residue) pairs of a densely packed batch.
 template <class F>
 __global__ void __launch_bounds__(256)
-    k_elementwise(F f, int N, int nres, int rid_off, const ModConst* __restrict__ mc) {
+    k_elementwise(F f, int N, int nres, int rid_off, const ModConst* __restrict__ mc, const int* __restrict__ rid_list) {
   const int y = blockIdx.y + blockIdx.z * gridDim.y;
-  const ModConst m = mc[rid_off + y % nres];
+  const ModConst m = mc[rid_list ? rid_list[y] : rid_off + y % nres];
   const size_t base = (size_t)y * N;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) f(base + j, m);
 }
 
 template <class F>
-int launch_ew(const Engine& e, F f, int base, cudaStream_t st, int npolys = 1) {
-  const int nres = e.n_residues(base);
+int launch_ew(const Engine& e, F f, int base, cudaStream_t st, int npolys = 1, const int* rid_list = nullptr) {
+  const int nres = rid_list ? 1 : e.n_residues(base);
   if (nres <= 0) {
     set_error("pointwise: unknown base");
     return CP_ERR_INVALID_;
@@ -47,7 +47,7 @@ int launch_ew(const Engine& e, F f, int base, cudaStream_t st, int npolys = 1) {
     gy = (int)(rows / gz);
   }
   dim3 grid(bx, gy, gz);
-  k_elementwise<<<grid, threads, 0, st>>>(f, e.N, nres, e.rid_offset(base), e.d_mc);
+  k_elementwise<<<grid, threads, 0, st>>>(f, e.N, nres, rid_list ? 0 : e.rid_offset(base), e.d_mc, rid_list);
   return check_launch("pointwise");
 }
 
@@ -175,6 +175,10 @@ int pw_double_add(const Engine& e, void* c1, const void* a1, const void* b1, voi
 }
 int pw_mul(const Engine& e, void* c, const void* a, const void* b, int base, cudaStream_t st, int npolys) {
   return launch_ew(e, MulF{U2(c), CU2(a), CU2(b)}, base, st, npolys);
+}
+int pw_mul_list(const Engine& e, void* c, const void* a, const void* b, const int* rid_list, int nlist,
+                cudaStream_t st) {
+  return launch_ew(e, MulF{U2(c), CU2(a), CU2(b)}, 0, st, nlist, rid_list);
 }
 int pw_mul_u64(const Engine& e, void* c, const void* a, const uint64_t* b, int base, cudaStream_t st) {
   return launch_ew(e, MulU64F{U2(c), CU2(a), b}, base, st);

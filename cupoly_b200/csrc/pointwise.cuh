@@ -12,6 +12,8 @@ int pw_double_add(const Engine& e, void* c1, const void* a1, const void* b1, voi
                   const void* b2, int base, cudaStream_t st);
 int pw_mul(const Engine& e, void* c, const void* a, const void* b, int base, cudaStream_t st, int npolys = 1);
 int pw_mul_u64(const Engine& e, void* c, const void* a, const uint64_t* b, int base, cudaStream_t st);
+int pw_mul_list(const Engine& e, void* c, const void* a, const void* b, const int* rid_list, int nlist,
+                cudaStream_t st);
 int pw_muladd(const Engine& e, void* d, const void* a, const void* b, const void* c, int base, cudaStream_t st);
 int pw_dr2(const Engine& e, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, cudaStream_t st, int npolys = 1);

@@ -81,8 +81,13 @@ class Engine:
         if not torch.cuda.is_available():
             raise RuntimeError("cupoly_b200 needs a CUDA device")
         _lib.lib()
+        if log_radix == 0:  # use the autotuner's choice for this GPU and size when one is cached
+            from .autotune import cached_log_radix
+
+            log_radix = cached_log_radix(nphi)
         h = C.c_void_p()
         call("cp_engine_create", C.byref(h), k, kl, nphi, t, log_radix)
+        self.log_radix = log_radix
         self._h = h
         self.k = k
         self.kl = kl if kl > 0 else k + 1

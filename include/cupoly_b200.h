@@ -89,6 +89,14 @@ int cp_engine_check(const cp_engine* e, void* stream);
  *      of the base (poly_stride = 0 means densely packed). */
 int cp_dgt(const cp_engine* e, void* data, int base, int direction, int npolys, int64_t poly_stride, void* stream);
 
+/* ---- work-list forms (no counterpart in cuPoly): `nlist` residues of N Gaussian
+ *      elements back to back; residue i uses the engine's prime rid_list[i]
+ *      (device int array, values < cp_engine_n_residues(e, CP_QBBASE)).  Lets
+ *      polynomials of different RNS widths share one launch. ---- */
+int cp_dgt_list(const cp_engine* e, void* data, const int* rid_list, int nlist, int direction, void* stream);
+int cp_mul_list(const cp_engine* e, void* c, const void* a, const void* b, const int* rid_list, int nlist,
+                void* stream);
+
 /* ---- pointwise, DGT domain: replace DGTEngine::execute_{add,sub,double_add,
  *      mul_dgt_gi,mul_dgt_u64,muladd,dr2}_dgt (src/cuda/dgt.cu:1096-1499) ---- */
 int cp_add(const cp_engine* e, void* c, const void* a, const void* b, int base, void* stream);

@@ -1,0 +1,85 @@
+"""Batched forms: mixed-size polymul work lists and graph-captured BFV batches,
+bit-exact per instance against the plain per-call path and the oracle."""
+import numpy as np
+import pytest
+
+from oracle import coracle as CO
+from oracle import pyoracle as O
+from tests.common import fold, random_poly_residues, unfold
+
+pytestmark = pytest.mark.gpu
+
+
+def _plain_polymul(nphi, k, a, b):
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine, from_u64, to_u64
+    e = Engine(k, 0, nphi, 256)
+    ta, tb = from_u64(fold(a)[None]), from_u64(fold(b)[None])
+    e.dgt(ta, 0, FORWARD)
+    e.dgt(tb, 0, FORWARD)
+    tc = e.empty(0)
+    e.mul(tc, ta, tb, 0)
+    e.dgt(tc, 0, INVERSE)
+    return unfold(to_u64(tc))[0]
+
+
+def test_mixed_polymul_matches_plain_and_oracle(gpu):
+    from cupoly_b200.batch import MixedPolymul, random_specs
+    specs = random_specs(40, seed=3)
+    mp = MixedPolymul(specs)
+    data = []
+    for i, (nphi, k) in enumerate(specs):
+        a = random_poly_residues(1000 + i, O.PRIMES[:k], nphi)
+        b = random_poly_residues(2000 + i, O.PRIMES[:k], nphi)
+        mp.set_inputs(i, a, b)
+        data.append((a, b))
+    mp.run()
+    for i, (nphi, k) in enumerate(specs):
+        got = mp.result(i)
+        a, b = data[i]
+        assert np.array_equal(got, CO.polymul(a[None], b[None], O.PRIMES[:k])[0]), (i, nphi, k)
+        if i < 8:
+            assert np.array_equal(got, _plain_polymul(nphi, k, a, b))
+
+
+def test_mixed_polymul_graph_replay_follows_inputs(gpu):
+    import torch
+    from cupoly_b200.batch import MixedPolymul
+    specs = [(2048, 3), (4096, 1), (2048, 8), (16384, 2)]
+    mp = MixedPolymul(specs)
+    for rnd in range(2):
+        for i, (nphi, k) in enumerate(specs):
+            mp.set_inputs(i, random_poly_residues(7 * rnd + i, O.PRIMES[:k], nphi),
+                          random_poly_residues(50 + 7 * rnd + i, O.PRIMES[:k], nphi))
+        mp.replay()
+        torch.cuda.synchronize()
+        for i, (nphi, k) in enumerate(specs):
+            a = random_poly_residues(7 * rnd + i, O.PRIMES[:k], nphi)
+            b = random_poly_residues(50 + 7 * rnd + i, O.PRIMES[:k], nphi)
+            assert np.array_equal(mp.result(i), CO.polymul(a[None], b[None], O.PRIMES[:k])[0])
+    assert mp.launches_per_run() == 12
+
+
+def test_bfv_batch_graph_equals_eager(gpu):
+    import torch
+    from cupoly_b200.batch import BFVBatch
+    from cupoly_b200.engine import UNIFORM, Engine
+    e = Engine(3, 4, 4096, 256)
+    bb = BFVBatch(e, 5)
+    for j, x in enumerate(bb.ins):
+        e.sample(x, 0, UNIFORM, 9, 100 * j, npolys=5, to_dgt=True)
+    eager = e.empty(0, 15)
+    e.bfv_mul_batch(eager, *bb.ins, 5, e.bfv_mul_batch_workspace(5))
+    bb.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(bb.out, eager)
+
+
+def test_autotuner_picks_a_candidate_and_caches(gpu, tmp_path, monkeypatch):
+    import json
+    monkeypatch.setenv("CUPOLY_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    from cupoly_b200 import autotune
+    r = autotune.best_log_radix(4096, residues=256, reps=2)
+    assert r in autotune.candidates(4096)
+    assert autotune.cached_log_radix(4096) == r
+    data = json.load(open(tmp_path / "tune.json"))
+    assert len(next(iter(data.values()))["ms_fwd_inv"]) == len(autotune.candidates(4096))
