@@ -320,7 +320,7 @@ def run_ours(args, D: Dist):
                 "frac": round(t_int * 1e3 / dgt_ms, 4),
                 "shoup_per_launch": ops["shoup"] * nres_launch, "addmod_per_launch": ops["addmod"] * nres_launch,
                 "peak_shoup_per_s": round(peaks_int["shoup"], 1), "peak_addmod_per_s": round(peaks_int["addmod"], 1),
-                "peak_mont_per_s": round(peaks_int["mont"], 1), "peak_imad32_per_s": round(peaks_int["imad32"], 1),
+                "peak_mulmod_per_s": round(peaks_int["mulmod"], 1), "peak_imad32_per_s": round(peaks_int["imad32"], 1),
                 "note": "frac = (Shoup / peak Shoup + adds / peak add) / measured; peaks measured live by cp_calibrate_int"}
 
     # ---- polymul/s of the nphi = 4096, k = 2 configuration (batched) ----

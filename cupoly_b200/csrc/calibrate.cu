@@ -14,7 +14,7 @@ using namespace cpoly;
 
 template <int KIND>
 __global__ void __launch_bounds__(256) k_calibrate(uint64_t* __restrict__ sink, int iters, uint64_t p, uint64_t w,
-                                                   uint64_t ws, uint64_t pneg) {
+                                                   uint64_t ws, ModConst mc) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   uint64_t x[8];
 #pragma unroll
@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(256) k_calibrate(uint64_t* __restrict__ sink, 
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       if (KIND == 0) x[i] = shoup_mul(x[i], w, ws, p);               // constant multiply
-      if (KIND == 1) x[i] = mont_mul(x[i], x[(i + 1) & 7], p, pneg);  // data x data (Montgomery)
+      if (KIND == 1) x[i] = mul_mod(x[i], x[(i + 1) & 7], mc);       // data x data (pseudo-Mersenne)
       if (KIND == 2) x[i] = add_mod(x[i], x[(i + 3) & 7], p);        // modular add
       if (KIND == 3) x[i] = (uint64_t)((uint32_t)x[i] * (uint32_t)w + (uint32_t)(x[i] >> 32));  // 32-bit IMAD
     }
@@ -44,7 +44,7 @@ extern "C" int cp_calibrate_int(int kind, int iters, void* sink, long long nthre
   const uint64_t p = 9223372036801560577ULL;  // the first prime of the table
   const uint64_t w = 1234567890123456789ULL % p;
   const uint64_t ws = h_shoup(w, p);
-  const uint64_t pneg = h_modconst(p).pneg;
+  const ModConst mc = h_modconst(p);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cudaEvent_t a, b;
   cudaEventCreate(&a);
@@ -53,10 +53,10 @@ extern "C" int cp_calibrate_int(int kind, int iters, void* sink, long long nthre
   const unsigned blocks = (unsigned)(nthreads / 256);
   uint64_t* s = reinterpret_cast<uint64_t*>(sink);
   switch (kind) {
-    case 0: k_calibrate<0><<<blocks, 256, 0, st>>>(s, iters, p, w, ws, pneg); break;
-    case 1: k_calibrate<1><<<blocks, 256, 0, st>>>(s, iters, p, w, ws, pneg); break;
-    case 2: k_calibrate<2><<<blocks, 256, 0, st>>>(s, iters, p, w, ws, pneg); break;
-    default: k_calibrate<3><<<blocks, 256, 0, st>>>(s, iters, p, w, ws, pneg); break;
+    case 0: k_calibrate<0><<<blocks, 256, 0, st>>>(s, iters, p, w, ws, mc); break;
+    case 1: k_calibrate<1><<<blocks, 256, 0, st>>>(s, iters, p, w, ws, mc); break;
+    case 2: k_calibrate<2><<<blocks, 256, 0, st>>>(s, iters, p, w, ws, mc); break;
+    default: k_calibrate<3><<<blocks, 256, 0, st>>>(s, iters, p, w, ws, mc); break;
   }
   cudaEventRecord(b, st);
   cudaError_t err = cudaEventSynchronize(b);

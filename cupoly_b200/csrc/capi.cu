@@ -82,6 +82,11 @@ int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int l
       set_error("cp_engine_create: prime with 2^64 mod p >= 2^32 is not supported");
       return CP_ERR_UNSUPPORTED;
     }
+    if ((p >> 63) || (1ull << 63) - p >= (1ull << 31) - 1) {  // pm_red needs p = 2^63 - c, c < 2^31 - 1
+      delete h;
+      set_error("cp_engine_create: prime not of the form 2^63 - c with c < 2^31 - 1");
+      return CP_ERR_UNSUPPORTED;
+    }
     e.xi.push_back(canonical_xi(p, kPrimitiveRoots[i], (uint64_t)e.N));
   }
   e.plan = make_plan(e.logN, log_radix ? log_radix : 3);

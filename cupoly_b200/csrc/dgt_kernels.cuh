@@ -91,6 +91,19 @@ __device__ __forceinline__ void dit_regs(uint64_t* xr, uint64_t* xi, const ulong
   }
 }
 
+// x <- x * (w_re + i w_im) for canonical x, from the Karatsuba triple
+// k[0..2] = (w_re, w_im - w_re, w_re + w_im) with Shoup companions:
+// re = k1 - k3, im = k1 + k2 for k1 = w_re (x_re + x_im), k2 = x_re (w_im - w_re),
+// k3 = x_im (w_re + w_im).  Three constant products instead of four.
+__device__ __forceinline__ void gi_mul_const3(uint64_t& xr, uint64_t& xi, const ulonglong2* k, uint64_t p) {
+  const ulonglong2 k0 = __ldg(k), k1c = __ldg(k + 1), k2c = __ldg(k + 2);
+  const uint64_t k1 = shoup_mul(xr + xi, k0.x, k0.y, p);  // xr + xi < 2p < 2^64
+  const uint64_t k2 = shoup_mul(xr, k1c.x, k1c.y, p);
+  const uint64_t k3 = shoup_mul(xi, k2c.x, k2c.y, p);
+  xr = sub_mod(k1, k3, p);
+  xi = add_mod(k1, k2, p);
+}
+
 // One middle/late forward pass (I >= 1), full radix 2^LOGR, data in smem.
 template <int LOGNC, int LOGR, int I>
 __device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* tab,
@@ -212,11 +225,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
         const int idx = Lw + (v << PF);
         const ulonglong2 a = xs[idx];
         uint64_t ar = a.x, ai = a.y;
-        if (twist) {
-          const ulonglong2 tr = __ldg(tab + A.L.off_twist + 2 * idx);
-          const ulonglong2 ti = __ldg(tab + A.L.off_twist + 2 * idx + 1);
-          gi_mul_const(ar, ai, tr.x, tr.y, ti.x, ti.y, p);
-        }
+        if (twist) gi_mul_const3(ar, ai, tab + A.L.off_twist + 3 * idx, p);
         xr[g * (1 << W) + v] = ar;
         xi[g * (1 << W) + v] = ai;
       }
@@ -253,16 +262,19 @@ __device__ __forceinline__ ulonglong2 tensor_load(const InvSrc& s, int j, size_t
     gi_mul(r, i, a1.x, a1.y, b1.x, b1.y, m);
   } else {
     uint64_t r1, i1, r2, i2;
-    gi_mul_mont(r1, i1, a0.x, a0.y, b1.x, b1.y, m);
-    gi_mul_mont(r2, i2, a1.x, a1.y, b0.x, b0.y, m);
-    r = shoup_mul(add_mod(r1, r2, m.p), m.r1, m.r1s, m.p);
-    i = shoup_mul(add_mod(i1, i2, m.p), m.r1, m.r1s, m.p);
+    gi_mul(r1, i1, a0.x, a0.y, b1.x, b1.y, m);
+    gi_mul(r2, i2, a1.x, a1.y, b0.x, b0.y, m);
+    r = add_mod(r1, r2, m.p);
+    i = add_mod(i1, i2, m.p);
   }
   return make_ulonglong2(r, i);
 }
 
 // Inverse transform of 2^LOGNC elements per CTA; untwist (with N^-1) applied
 // when `untwist` is set (S == 0).  Input per InvSrc, output to `data`.
+// In tensor mode (src.mode 1) the CTAs of c0, c1, c2 of one (pair, residue)
+// are adjacent, so each operand residue is fetched from HBM once and served
+// from L2 to the other outputs.
 template <int LOGNC, int LOGR>
 __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
     k_dgt_inv(ulonglong2* __restrict__ data, InvSrc src, DgtArgs A, int nres, int rid_off, long long poly_stride,
@@ -275,8 +287,15 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   const int tid = threadIdx.x;
   const int h = blockIdx.x & ((1 << S) - 1);
   const int pr = blockIdx.x >> S;
-  const int r = pr % nres;
-  const int poly = pr / nres;
+  int r, poly;
+  if (src.mode == 1) {  // c0, c1, c2 of one (pair, residue) in adjacent CTAs
+    const int rest = pr / 3;
+    r = rest % nres;
+    poly = (pr % 3) * src.npairs + rest / nres;
+  } else {
+    r = pr % nres;
+    poly = pr / nres;
+  }
   const int rid = A.rid_list ? A.rid_list[pr] : rid_off + r;
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
@@ -330,11 +349,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
       for (int v = 0; v < (1 << W); ++v) {
         const int idx = Lw + (v << PF);
         uint64_t ar = xr[v], ai = xi[v];
-        if (untwist) {
-          const ulonglong2 tr = __ldg(tab + A.L.off_untwist + 2 * idx);
-          const ulonglong2 ti = __ldg(tab + A.L.off_untwist + 2 * idx + 1);
-          gi_mul_const(ar, ai, tr.x, tr.y, ti.x, ti.y, p);
-        }
+        if (untwist) gi_mul_const3(ar, ai, tab + A.L.off_untwist + 3 * idx, p);
         x[idx] = make_ulonglong2(ar, ai);
       }
     }
@@ -367,9 +382,7 @@ __global__ void __launch_bounds__(256)
       const int n = Lw + hh * Nc;
       const ulonglong2 a = xs[n];
       uint64_t ar = a.x, ai = a.y;
-      const ulonglong2 tr = __ldg(tab + A.L.off_twist + 2 * n);
-      const ulonglong2 ti = __ldg(tab + A.L.off_twist + 2 * n + 1);
-      gi_mul_const(ar, ai, tr.x, tr.y, ti.x, ti.y, p);
+      gi_mul_const3(ar, ai, tab + A.L.off_twist + 3 * n, p);
       xr[hh] = ar;
       xi[hh] = ai;
     }
@@ -440,9 +453,7 @@ __global__ void __launch_bounds__(256)
     for (int hh = 0; hh < K; ++hh) {
       const int n = Lw + hh * Nc;
       uint64_t ar = xr[hh], ai = xi[hh];
-      const ulonglong2 tr = __ldg(tab + A.L.off_untwist + 2 * n);
-      const ulonglong2 ti = __ldg(tab + A.L.off_untwist + 2 * n + 1);
-      gi_mul_const(ar, ai, tr.x, tr.y, ti.x, ti.y, p);
+      gi_mul_const3(ar, ai, tab + A.L.off_untwist + 3 * n, p);
       x[n] = make_ulonglong2(ar, ai);
     }
   }

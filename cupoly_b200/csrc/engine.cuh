@@ -42,8 +42,8 @@ struct DgtTableLayout {
   int off_inv[kMaxPasses] = {0};
   int off_split_fwd = 0;                // N entries (only if S > 0)
   int off_split_inv = 0;
-  int off_twist = 0;                    // 2N entries: (xr, xr'), (xi, xi')
-  int off_untwist = 0;                  // 2N entries, includes N^-1
+  int off_twist = 0;                    // 3N entries: xi^n as (re, im - re, re + im), Shoup pairs
+  int off_untwist = 0;                  // 3N entries: xi^-n N^-1, same form
   int stride = 0;                       // entries per residue block
 };
 

@@ -112,15 +112,14 @@ struct Dr2F {
   __device__ void operator()(size_t i, const ModConst& m) const {
     const u2 a0 = c01[i], a1 = c02[i], b0 = c11[i], b1 = c12[i];
     uint64_t r1, i1, r2, i2, r3, i3, r4, i4;
-    gi_mul_mont(r1, i1, a0.x, a0.y, b0.x, b0.y, m);
-    gi_mul_mont(r2, i2, a0.x, a0.y, b1.x, b1.y, m);
-    gi_mul_mont(r3, i3, a1.x, a1.y, b0.x, b0.y, m);
-    gi_mul_mont(r4, i4, a1.x, a1.y, b1.x, b1.y, m);
+    gi_mul(r1, i1, a0.x, a0.y, b0.x, b0.y, m);
+    gi_mul(r2, i2, a0.x, a0.y, b1.x, b1.y, m);
+    gi_mul(r3, i3, a1.x, a1.y, b0.x, b0.y, m);
+    gi_mul(r4, i4, a1.x, a1.y, b1.x, b1.y, m);
     const uint64_t p = m.p;
-    c21[i] = make_ulonglong2(shoup_mul(r1, m.r1, m.r1s, p), shoup_mul(i1, m.r1, m.r1s, p));
-    c22[i] = make_ulonglong2(shoup_mul(add_mod(r2, r3, p), m.r1, m.r1s, p),
-                             shoup_mul(add_mod(i2, i3, p), m.r1, m.r1s, p));
-    c23[i] = make_ulonglong2(shoup_mul(r4, m.r1, m.r1s, p), shoup_mul(i4, m.r1, m.r1s, p));
+    c21[i] = make_ulonglong2(r1, i1);
+    c22[i] = make_ulonglong2(add_mod(r2, r3, p), add_mod(i2, i3, p));
+    c23[i] = make_ulonglong2(r4, i4);
   }
 };
 struct NegF {

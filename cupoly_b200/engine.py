@@ -48,14 +48,14 @@ def from_u64(a: np.ndarray, device="cuda") -> torch.Tensor:
 def int_peaks(iters: int = 256, waves: int = 8, stream=None) -> dict:
     """Measured peak rates (operations/s) of the modular primitives on the current GPU.
 
-    Keys: shoup (constant multiply), mont (data x data Montgomery), addmod,
+    Keys: shoup (constant multiply), mulmod (data x data product), addmod,
     imad32.  Each is timed on one kernel that fills every SM `waves` times.
     """
     props = torch.cuda.get_device_properties(torch.cuda.current_device())
     nthreads = props.multi_processor_count * waves * 256
     sink = torch.empty(nthreads, dtype=torch.int64, device="cuda")
     out = {}
-    for kind, name in enumerate(("shoup", "mont", "addmod", "imad32")):
+    for kind, name in enumerate(("shoup", "mulmod", "addmod", "imad32")):
         ms = C.c_float()
         call("cp_calibrate_int", kind, iters, _ptr(sink), nthreads, C.byref(ms), _stream(stream))  # warm-up
         call("cp_calibrate_int", kind, iters, _ptr(sink), nthreads, C.byref(ms), _stream(stream))
@@ -67,11 +67,12 @@ def dgt_op_counts(N: int) -> dict:
     """Algorithmic integer work of one residue-transform of N Gaussian elements.
 
     Shoup constant multiplies: 2 per non-trivial radix-2 twiddle
-    (N/2 log2 N - N + 1 of them) plus 4 per element for the Gaussian twist;
-    modular adds/subs: 4 per radix-2 butterfly plus 2 per element for the twist.
+    (N/2 log2 N - N + 1 of them) plus 3 per element for the Gaussian twist
+    (Karatsuba form); modular adds/subs: 4 per radix-2 butterfly plus 2 per
+    element for the twist.
     """
     lg = N.bit_length() - 1
-    return {"shoup": 2 * (N // 2 * lg - N + 1) + 4 * N, "addmod": 2 * N * lg + 2 * N}
+    return {"shoup": 2 * (N // 2 * lg - N + 1) + 3 * N, "addmod": 2 * N * lg + 2 * N}
 
 
 class Engine:

@@ -175,7 +175,7 @@ int cp_bfv_mul_batch(const cp_engine* e, void* c, const void* a0, const void* a1
 /* ---- integer-throughput calibration (no counterpart in cuPoly): times `iters`
  *      x 8 independent applications per thread of one primitive over nthreads
  *      threads (a multiple of 256) and returns the kernel time in *ms.  kind:
- *      0 Shoup constant multiply, 1 Montgomery multiply, 2 modular add,
+ *      0 Shoup constant multiply, 1 data x data modular multiply, 2 modular add,
  *      3 32-bit multiply-add.  sink: nthreads uint64 of device memory. ---- */
 int cp_calibrate_int(int kind, int iters, void* sink, long long nthreads, float* ms, void* stream);
 
