@@ -350,6 +350,86 @@ def run_ours(args, D: Dist):
     torch.cuda.synchronize()
     polymul_value = NPm * 5 / (ev0.elapsed_time(ev1) / 1e3)
 
+    # ---- per-call polymul of the same configuration (one product per call sequence) ----
+    NPp = 64
+    qa, qb, qc = e1.empty(QBase), e1.empty(QBase), e1.empty(QBase)
+
+    def polymul_plain_step():
+        for i in range(NPp):
+            qa.copy_(pa[i:i + 1])
+            qb.copy_(pb[i:i + 1])
+            e1.dgt(qa, QBase, FORWARD)
+            e1.dgt(qb, QBase, FORWARD)
+            e1.mul(qc, qa, qb, QBase)
+            e1.dgt(qc, QBase, INVERSE)
+
+    polymul_plain_step()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    polymul_plain_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    polymul_plain_value = NPp / (ev0.elapsed_time(ev1) / 1e3)
+    del pa, pb, pc, ta, tb, qa, qb, qc
+
+    # ---- mixed-size batch: 1024 products, nphi in {2048..16384}, k in 1..8, one CUDA graph ----
+    from cupoly_b200.batch import MixedPolymul, random_specs
+    mixed_specs = random_specs(1024, seed)
+    mp = MixedPolymul(mixed_specs)
+    for g in mp.groups.values():  # residues below 2^62 are valid for every prime of the table
+        g["a"].random_(0, 1 << 62)
+        g["b"].random_(0, 1 << 62)
+    mp.capture()
+    mp.replay()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(5):
+        mp.replay()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    mixed_ms = ev0.elapsed_time(ev1) / 5
+    mixed = {"config": "1024 products, nphi uniform in {2048, 4096, 8192, 16384}, k uniform in 1..8 (seeded), "
+                       "one CUDA graph of %d launches" % mp.launches_per_run(),
+             "polymul_per_s": round(1024 / (mixed_ms / 1e3), 1), "ms_per_batch": round(mixed_ms, 3),
+             "algorithmic_GB_per_s": round(mp.algorithmic_bytes() / (mixed_ms / 1e3) / 1e9, 1)}
+    del mp
+    torch.cuda.empty_cache()
+
+    # ---- north-star configuration: nphi = 16384 (N = 2^14 coefficients), |Q| = 10, batched vs plain ----
+    eT = Engine(10, 11, 16384, T_PLAIN)
+    PT, PTp = 32, 4
+    insT = []
+    for j in range(4):
+        x = eT.empty(QBase, PT)
+        eT.sample(x, QBase, UNIFORM, seed, 4096 * j, npolys=PT, to_dgt=True)
+        insT.append(x)
+    cT = eT.empty(QBase, 3 * PT)
+    wsT = eT.bfv_mul_batch_workspace(PT)
+    eT.bfv_mul_batch(cT, *insT, PT, wsT)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(5):
+        eT.bfv_mul_batch(cT, *insT, PT, wsT)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    tgt_batched = 5 * PT / (ev0.elapsed_time(ev1) / 1e3)
+    outsT = [eT.empty(QBase) for _ in range(3)]
+    for i in range(PTp):
+        eT.bfv_mul(*outsT, *[x[i:i + 1] for x in insT])
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(2):
+        for i in range(PTp):
+            eT.bfv_mul(*outsT, *[x[i:i + 1] for x in insT])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    tgt_plain = 2 * PTp / (ev0.elapsed_time(ev1) / 1e3)
+    target = {"config": "nphi=16384, k=10, kl=11, t=256", "batched_hom_mul_per_s": round(tgt_batched, 1),
+              "pairs_per_call": PT, "plain_hom_mul_per_s": round(tgt_plain, 1),
+              "batched_over_plain": round(tgt_batched / tgt_plain, 2)}
+    del insT, cT, wsT, outsT, eT
+    torch.cuda.empty_cache()
+
     # ---- large configuration: nphi = 32768, k = 16, kl = 17, t = 65537, 64 pairs + sampling ----
     large = None
     if not args.no_large:
@@ -427,9 +507,19 @@ def run_ours(args, D: Dist):
                       "form": "one cp_bfv_mul call per pair (cuPoly's per-call composition)", "pairs": PP},
             "batched_over_plain": round(value / D.world / plain_value, 2),
             "polymul": ({"value": round(polymul_value, 1), "unit": "polymul/s",
-                         "config": "nphi=4096, k=2, batch 1024"} if polymul_value else None),
+                         "config": "nphi=4096, k=2, batch 1024 (3 transforms + pointwise per product)",
+                         "plain_value": round(polymul_plain_value, 1),
+                         "plain_form": "one product per call sequence (2 forward DGTs, multiply, inverse DGT)"}
+                        if polymul_value else None),
+            "mixed_polymul": mixed,
+            "target": target,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                         "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                         "frac": round(achieved / hbm_peak, 4),
+                         # dram__bytes_read.sum + dram__bytes_write.sum of this launch (same
+                         # kernel, 3072 residues of N = 4096) from one ncu capture; writes read low
+                         # because dirty lines are still in L2 when the kernel ends
+                         "traffic": 344781824 if (e.N == 4096 and 4 * P * K_B == 3072) else None,
+                         "traffic_source": "ncu capture summarised in profiles/k_dgt_fwd_nphi8192_k5_ncu.md",
                          "kernel": "k_dgt_fwd (forward DGT, %d residues of N=%d per launch, timed alone)" %
                                    (4 * P * K_B, e.N),
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback",

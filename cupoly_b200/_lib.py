@@ -75,6 +75,11 @@ SIGNATURES = {
     "cp_bfv_mul_batch_workspace_bytes": (C.c_size_t, [_vp, _i]),
     "cp_bfv_mul_batch": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
     "cp_calibrate_int": (_i, [_i, _i, _vp, C.c_longlong, C.POINTER(C.c_float), _vp]),
+    "cp_crt": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp]),
+    "cp_icrt": (_i, [_vp, _vp, _i, _vp, _i, _i, _vp]),
+    "cp_wire_bytes": (C.c_size_t, [_vp, _i, _i]),
+    "cp_export_residues": (_i, [_vp, _vp, C.c_size_t, _vp, _i, _i, _i, _vp]),
+    "cp_import_residues": (_i, [_vp, _vp, _vp, C.c_size_t, _i, _i, C.POINTER(_i), _vp]),
     "cp_sample": (_i, [_vp, _vp, _i, _i, _u64, _u32, _i, _i, _vp]),
     "cp_sample_ids": (_i, [_vp, _vp, _i, _i, _u64, _vp, _i, _i, _vp]),
 }

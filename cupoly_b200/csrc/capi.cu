@@ -8,9 +8,6 @@
 #include "pointwise.cuh"
 #include "prime_table.h"
 
-struct cp_engine {
-  cpoly::Engine e;
-};
 
 using namespace cpoly;
 

@@ -20,6 +20,7 @@ namespace cpoly {
 constexpr int kMaxLogNc = 13;   // largest transform kept whole in one CTA (8192 GIs, 136 KB smem)
 constexpr int kMaxPasses = 8;
 constexpr int kMaxResidues = 96; // |Q| + |B| limit of one engine
+constexpr int kMaxLimbs = 64;    // 64-bit limbs of a big-integer coefficient in cp_crt (4096 bits)
 
 // Radix plan of the in-CTA transform of size 2^logNc.  Passes run from the
 // top index bits down; pass i covers bits [p[i], p[i] + w[i]).
@@ -114,6 +115,7 @@ struct Engine {
     int qb_pm, bq_pm;              // mixed-radix weights prod_{l<i} s_l mod m_j, [target][i]
     int qq_w, bb_w;                // Garner weights of Q and of B, [i][l]
     int q_pinv, q_pinv_s, b_pinv, b_pinv_s;  // (prod_{j<i} s_j)^-1 mod s_i
+    int pow64;                     // 2^(64 l) mod p_r, [residue][kMaxLimbs]
   } ho{};
   uint64_t t_shoup_one = 0;        // floor(2^64 / t)
   uint64_t h_q_mod_t = 0, h_qinv_t = 0, h_qinv_t_s = 0;  // Q mod t, Q^-1 mod t
@@ -132,3 +134,8 @@ int build_tables(Engine& e);
 void free_tables(Engine& e);
 
 }  // namespace cpoly
+
+// The C ABI's opaque handle (include/cupoly_b200.h): one engine.
+struct cp_engine {
+  cpoly::Engine e;
+};

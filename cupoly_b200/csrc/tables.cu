@@ -373,6 +373,18 @@ int build_tables(Engine& e) {
     e.ho.rho_q = append(v2);
     e.ho.rho_q_s = append(c2);
   }
+  {
+    std::vector<uint64_t> v;  // 2^(64 l) mod p_r for the limb-to-residue conversion
+    for (auto p : e.primes) {
+      const uint64_t r1 = (uint64_t)(((unsigned __int128)1 << 64) % p);
+      uint64_t acc = 1;
+      for (int l = 0; l < kMaxLimbs; ++l) {
+        v.push_back(acc);
+        acc = h_mulmod(acc, r1, p);
+      }
+    }
+    e.ho.pow64 = append(v);
+  }
   e.hps_words = H.size();
 
   // ---------------- upload ----------------

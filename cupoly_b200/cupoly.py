@@ -26,7 +26,7 @@ import torch
 
 from .engine import (ADD, ADDADD, BBase, BINARY, DESTROY_INPUTS, DISCRETE_GAUSSIAN, FORWARD, GAUSSIAN,
                      HAMMINGWEIGHT, INVERSE, MUL, MULMUL, NARROW, QBBase, QBase, SUB, TBase, TERNARY, UNIFORM, ZO,
-                     Engine, from_u64, to_u64)
+                     Engine, from_u64, ints_to_limbs, limbs_to_ints, to_u64)
 
 HOSTSTATE, RNSSTATE, BOTHSTATE = 0, 1, 2
 HAMMINGWEIGHT_H = 64
@@ -200,48 +200,49 @@ def poly_clear(ctx: Context, a: poly_t):
     a.status = BOTHSTATE
 
 
-def _residues_of(coefs: List[int], primes: List[int], N: int) -> np.ndarray:
-    nphi = 2 * N
-    c = list(coefs[:nphi]) + [0] * max(0, nphi - len(coefs))
-    out = np.empty((len(primes), N, 2), dtype=np.uint64)
-    for r, p in enumerate(primes):
-        row = np.array([x % p for x in c], dtype=np.uint64)
-        out[r, :, 0] = row[:N]
-        out[r, :, 1] = row[N:]
+def _limbs_of(coefs: List[int], modulus: int, nphi: int):
+    """Coefficients (padded to nphi, negatives taken mod `modulus`) as uint64 limbs."""
+    c = [x % modulus if x < 0 else x for x in coefs[:nphi]] + [0] * max(0, nphi - len(coefs))
+    top = max(c) if c else 0
+    nlimbs = max(1, (top.bit_length() + 63) // 64)
+    if nlimbs > 64:  # beyond the device limb limit: reduce first (same residues)
+        c = [x % modulus for x in c]
+        nlimbs = max(1, (max(c).bit_length() + 63) // 64)
+    return ints_to_limbs(c, nlimbs)
+
+
+def poly_crt(ctx: Context, a: poly_t) -> torch.Tensor:
+    """Coefficient-domain residues of the host coefficients, computed on the device
+    (cuPoly reduces every ZZ coefficient on the host, polynomial.cu:190-221)."""
+    assert a.base in (QBase, QBBase)
+    e = _E()
+    limbs = _limbs_of(a.coefs, _prod(e.base_primes(a.base)), 2 * CUDAEngine.N)
+    with torch.cuda.stream(ctx.stream):
+        d = from_u64(limbs[None])
+        out = e.empty(a.base)
+    e.crt(out, d, a.base, stream=ctx.stream)
     return out
 
 
-def poly_crt(ctx: Context, a: poly_t) -> np.ndarray:
-    """Host residues of the coefficients (cuPoly polynomial.cu:190-221)."""
-    assert a.base in (QBase, QBBase)
-    return _residues_of(a.coefs, _E().base_primes(a.base), CUDAEngine.N)
-
-
-def poly_icrt(ctx: Context, a: poly_t, h: np.ndarray):
-    """CRT recombination into coefficients in [0, Q) (polynomial.cu:223-296)."""
-    N = CUDAEngine.N
-    if a.base == TBase:
-        a.coefs = [int(v) for v in np.concatenate([h[0, :, 0], h[0, :, 1]])]
-        return
-    if a.base != QBase:
+def poly_icrt(ctx: Context, a: poly_t, x: torch.Tensor):
+    """Coefficients in [0, Q) from coefficient-domain residues, recombined on the
+    device (cuPoly: host NTL CRT, polynomial.cu:223-296); base Q or T."""
+    if a.base not in (QBase, TBase):
         raise RuntimeError("Unknown base")
-    Q = CUDAEngine.RNSProduct
-    acc = [0] * (2 * N)
-    for r, p in enumerate(CUDAEngine.RNSPrimes):
-        Mi, inv = CUDAEngine.RNSMpi[r], CUDAEngine.RNSInvMpi[r]
-        row = np.concatenate([h[r, :, 0], h[r, :, 1]]).tolist()
-        for i, x in enumerate(row):
-            if x:
-                acc[i] += (x * inv % p) * Mi
-    a.coefs = [x % Q for x in acc]
+    e = _E()
+    nl = e.n_residues(a.base)
+    with torch.cuda.stream(ctx.stream):
+        limbs = torch.empty((1, 2 * CUDAEngine.N, nl), dtype=torch.int64, device="cuda")
+    e.icrt(limbs, x, a.base, stream=ctx.stream)
+    ctx.stream.synchronize()
+    a.coefs = limbs_to_ints(to_u64(limbs[0]))
 
 
 def poly_copy_to_device(ctx: Context, a: poly_t):
     if a.status in (RNSSTATE, BOTHSTATE):
         return
     e = _E()
-    with torch.cuda.stream(ctx.stream):
-        a.d_coefs = from_u64(poly_crt(ctx, a)[None])
+    a.d_coefs = poly_crt(ctx, a)
     e.dgt(a.d_coefs, a.base, FORWARD, stream=ctx.stream)
     ctx.stream.synchronize()
     a.status = BOTHSTATE
@@ -254,8 +255,7 @@ def poly_copy_to_host(ctx: Context, a: poly_t):
     with torch.cuda.stream(ctx.stream):
         aux = a.d_coefs.clone()
     e.dgt(aux, a.base, INVERSE, stream=ctx.stream)
-    ctx.stream.synchronize()
-    poly_icrt(ctx, a, to_u64(aux[0]))
+    poly_icrt(ctx, a, aux)
     a.status = BOTHSTATE
 
 
@@ -309,6 +309,71 @@ def poly_are_equal(ctx: Context, a: poly_t, b: poly_t) -> bool:
 
 def poly_to_string(ctx: Context, a: poly_t) -> str:
     return "".join("%d, " % poly_get_coeff(ctx, a, i) for i in range(poly_get_deg(ctx, a) + 1))
+
+
+def poly_export_residues(ctx: Context, a: poly_t) -> str:
+    """Coefficient-domain residues as text: for each residue, its nphi values in
+    coefficient order, space separated (cuPoly polynomial.cu:1291-1339)."""
+    e = _E()
+    poly_copy_to_device(ctx, a)
+    with torch.cuda.stream(ctx.stream):
+        aux = a.d_coefs.clone()
+    e.dgt(aux, a.base, INVERSE, stream=ctx.stream)
+    ctx.stream.synchronize()
+    h = e.unfold(to_u64(aux[0]))
+    return " ".join(str(int(v)) for v in h.reshape(-1).astype(np.int64))
+
+
+def poly_import_residues(ctx: Context, s: str, base: int = QBase) -> poly_t:
+    """Inverse of poly_export_residues; returns a new poly_t in RNSSTATE
+    (cuPoly polynomial.cu:1341-1383)."""
+    e = _E()
+    vals = np.array([int(v) for v in s.split()], dtype=np.int64).view(np.uint64)
+    nres, nphi = e.n_residues(base), 2 * CUDAEngine.N
+    h = np.zeros((nres, nphi), dtype=np.uint64)
+    h.reshape(-1)[: vals.size] = vals[: nres * nphi]
+    a = poly_t()
+    poly_init(ctx, a, base)
+    with torch.cuda.stream(ctx.stream):
+        a.d_coefs = from_u64(e.fold(h)[None])
+    e.dgt(a.d_coefs, base, FORWARD, stream=ctx.stream)
+    ctx.stream.synchronize()
+    a.status = RNSSTATE
+    return a
+
+
+def poly_export(ctx: Context, p: poly_t) -> str:
+    """Coefficients 0..deg as comma-separated integers (cuPoly polynomial.cu:1386-1404)."""
+    return ",".join(str(poly_get_coeff(ctx, p, i)) for i in range(poly_get_deg(ctx, p) + 1))
+
+
+def poly_import(ctx: Context, s: str) -> poly_t:
+    """Inverse of poly_export (cuPoly polynomial.cu:1406-1425)."""
+    p = poly_t()
+    poly_init(ctx, p)
+    if s.strip():
+        for i, v in enumerate(s.split(",")):
+            poly_set_coeff(ctx, p, i, int(v.replace(" ", "")))
+    return p
+
+
+def poly_export_binary(ctx: Context, a: poly_t) -> bytes:
+    """Binary wire form (cp_export_residues) of the device data, DGT domain."""
+    poly_copy_to_device(ctx, a)
+    return _E().export_residues(a.d_coefs, a.base, 1, stream=ctx.stream)
+
+
+def poly_import_binary(ctx: Context, data: bytes, base: int = QBase) -> poly_t:
+    """Inverse of poly_export_binary; coefficient-domain payloads are transformed."""
+    e = _E()
+    a = poly_t()
+    poly_init(ctx, a, base)
+    dom = e.import_residues(a.d_coefs, data, base, stream=ctx.stream)
+    if dom == 0:
+        e.dgt(a.d_coefs, base, FORWARD, stream=ctx.stream)
+    ctx.stream.synchronize()
+    a.status = RNSSTATE
+    return a
 
 
 # ---------------------------------------------------------------------------

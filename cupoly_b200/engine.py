@@ -45,6 +45,21 @@ def from_u64(a: np.ndarray, device="cuda") -> torch.Tensor:
     return torch.from_numpy(a.view(np.int64)).to(device)
 
 
+def ints_to_limbs(values, nlimbs: int) -> np.ndarray:
+    """Non-negative Python ints -> (len, nlimbs) uint64 limbs, least significant first."""
+    nbytes = 8 * nlimbs
+    buf = b"".join(int(v).to_bytes(nbytes, "little") for v in values)
+    return np.frombuffer(buf, dtype=np.uint64).reshape(len(values), nlimbs).copy()
+
+
+def limbs_to_ints(limbs: np.ndarray) -> List[int]:
+    """(n, nlimbs) uint64 limbs -> Python ints."""
+    a = np.ascontiguousarray(limbs, dtype=np.uint64)
+    raw = a.tobytes()
+    w = 8 * a.shape[-1]
+    return [int.from_bytes(raw[i * w:(i + 1) * w], "little") for i in range(a.shape[0])]
+
+
 def int_peaks(iters: int = 256, waves: int = 8, stream=None) -> dict:
     """Measured peak rates (operations/s) of the modular primitives on the current GPU.
 
@@ -194,6 +209,37 @@ class Engine:
     def double_op_by_int(self, b1, a1, b2, a2, base, x1, x2, op, stream=None):
         call("cp_double_op_by_int", self._h, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), base, int(x1), int(x2), op,
              _stream(stream))
+
+    # ---- coefficient I/O (big integers <-> residues, on the device) ----
+    def crt(self, out, coefs_limbs: torch.Tensor, base: int = QBase, stream=None):
+        """Residues of big-integer coefficients: coefs_limbs is (npolys, nphi, nlimbs) int64 (uint64 limbs)."""
+        npolys, nphi, nlimbs = coefs_limbs.shape
+        assert nphi == self.nphi
+        call("cp_crt", self._h, _ptr(out), _ptr(coefs_limbs), nlimbs, base, npolys, _stream(stream))
+        return out
+
+    def icrt(self, coefs_limbs: torch.Tensor, x, base: int = QBase, stream=None):
+        """Big-integer coefficients in [0, prod of the base) from coefficient-domain residues."""
+        npolys, nphi, nlimbs = coefs_limbs.shape
+        call("cp_icrt", self._h, _ptr(coefs_limbs), nlimbs, _ptr(x), base, npolys, _stream(stream))
+        return coefs_limbs
+
+    def wire_bytes(self, base: int, npolys: int = 1) -> int:
+        return int(_lib.lib().cp_wire_bytes(self._h, base, npolys))
+
+    def export_residues(self, x, base: int, domain: int, stream=None) -> bytes:
+        """Binary wire form of x (npolys, nres, N, 2); domain 0 coefficient, 1 DGT."""
+        n = self.wire_bytes(base, x.shape[0])
+        buf = C.create_string_buffer(n)
+        call("cp_export_residues", self._h, buf, n, _ptr(x), base, x.shape[0], domain, _stream(stream))
+        return buf.raw
+
+    def import_residues(self, x, data: bytes, base: int, stream=None) -> int:
+        """Fill x (npolys, nres, N, 2) from the wire form; returns the recorded domain."""
+        dom = C.c_int(-1)
+        call("cp_import_residues", self._h, _ptr(x), data, len(data), base, x.shape[0], C.byref(dom),
+             _stream(stream))
+        return dom.value
 
     # ---- HPS (coefficient domain) ----
     def basis_ext_q_to_b(self, out_b, in_q, npolys=1, stream=None):

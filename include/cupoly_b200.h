@@ -179,6 +179,32 @@ int cp_bfv_mul_batch(const cp_engine* e, void* c, const void* a0, const void* a1
  *      3 32-bit multiply-add.  sink: nthreads uint64 of device memory. ---- */
 int cp_calibrate_int(int kind, int iters, void* sink, long long nthreads, float* ms, void* stream);
 
+/* ---- coefficient I/O on the device: replaces the host NTL conversions poly_crt /
+ *      poly_icrt (src/arithmetic/polynomial.cu:190-296).  Coefficients are unsigned
+ *      integers of nlimbs 64-bit limbs, least significant first, coefficient-major:
+ *      uint64_t[npolys][nphi][nlimbs] in device memory.  Residues are in the
+ *      coefficient domain, uint64_t[npolys][nres][N][2].
+ *      cp_crt: base Q, B or QB, 1 <= nlimbs <= 64, residue = coefficient mod q_r.
+ *      cp_icrt: base Q or B (the unique X in [0, prod) with those residues, nlimbs >=
+ *      residues of the base) or T (the residue itself). ---- */
+int cp_crt(const cp_engine* e, void* out, const uint64_t* coefs, int nlimbs, int base, int npolys, void* stream);
+int cp_icrt(const cp_engine* e, uint64_t* coefs, int nlimbs, const void* in, int base, int npolys, void* stream);
+
+/* ---- binary residue wire format: replaces the string forms poly_export_residues /
+ *      poly_import_residues (src/arithmetic/polynomial.cu:1291-1383) for the serving
+ *      front-end.  Layout: a 64-byte header of sixteen little-endian uint32 words
+ *      {magic, version, nphi, nres, base, npolys, domain (0 coefficient, 1 DGT), flags
+ *      (0), 8 reserved zero words}, then the nres primes (uint64), then the residues in
+ *      the device layout uint64_t[npolys][nres][N][2].  Import checks the header, the
+ *      primes, the size and that every residue is reduced, before any copy. ---- */
+#define CP_WIRE_MAGIC 0x53525043u /* "CPRS" */
+#define CP_WIRE_VERSION 1u
+size_t cp_wire_bytes(const cp_engine* e, int base, int npolys);
+int cp_export_residues(const cp_engine* e, void* host_out, size_t cap, const void* poly, int base, int npolys,
+                       int domain, void* stream);
+int cp_import_residues(const cp_engine* e, void* poly, const void* host_in, size_t size, int base, int npolys,
+                       int* domain_out, void* stream);
+
 /* ---- sampler: replaces Sampler::sample(ctx, p, kind) (src/cuda/sampler.cu:576-645).
  *      npolys consecutive polynomials over `base` with stream ids stream_id ..
  *      stream_id + npolys - 1; to_dgt != 0 applies the forward DGT (cuPoly does). */
