@@ -37,6 +37,13 @@ SIGNATURES = {
     "cp_version": (C.c_char_p, []),
     "cp_last_error": (C.c_char_p, []),
     "cp_engine_create": (_i, [C.POINTER(_vp), _i, _i, _i, _u64, _i]),
+    "cp_ckks_engine_create": (_i, [C.POINTER(_vp), _i, _i, _i, _i, _i]),
+    "cp_engine_ckks_prec": (_i, [_vp]),
+    "cp_ckks_modulus_raising": (_i, [_vp, _vp, _vp, _i, _vp, _vp]),
+    "cp_ckks_modulus_reduction": (_i, [_vp, _vp, _vp, _i, _vp, _vp]),
+    "cp_ckks_rescale": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "cp_ckks_xi": (_i, [_vp, _vp, _vp, _vp]),
+    "cp_ckks_rho": (_i, [_vp, _vp, _vp, _vp]),
     "cp_engine_destroy": (_i, [_vp]),
     "cp_engine_n_residues": (_i, [_vp, _i]),
     "cp_engine_nphi": (_i, [_vp]),

@@ -7,6 +7,7 @@
 #include "launch.cuh"
 #include "pointwise.cuh"
 #include "prime_table.h"
+#include "prime_table_ckks.h"
 
 
 using namespace cpoly;
@@ -23,6 +24,15 @@ bool valid_base(const cp_engine* e, int base) { return e && base >= 0 && base <=
       set_error(msg);              \
       return CP_ERR_INVALID;       \
     }                              \
+  } while (0)
+
+// The exact BFV base conversions and scalings need the 63-bit prime form.
+#define CP_BFV_ONLY(h, name)                                                     \
+  do {                                                                           \
+    if ((h) && (h)->e.ckks_prec) {                                               \
+      set_error(name ": not available on a CKKS engine (BFV base conversions)"); \
+      return CP_ERR_UNSUPPORTED;                                                 \
+    }                                                                            \
   } while (0)
 
 // canonical xi with xi^N = i (see cp_engine_set_nthroot)
@@ -45,6 +55,55 @@ extern "C" {
 const char* cp_version(void) { return "cupoly_b200 0.1.0 (sm_100a)"; }
 const char* cp_last_error(void) { return last_error(); }
 
+}  // extern "C"
+
+namespace {
+
+// Shared tail of the two creation calls: tables for the given primes.
+int finish_engine(cp_engine** out, cp_engine* h, int log_radix) {
+  Engine& e = h->e;
+  for (size_t i = 0; i < e.primes.size(); ++i) {
+    const uint64_t p = e.primes[i];
+    e.mconst.push_back(h_modconst(p));
+    if ((p - 1) % (2 * (uint64_t)e.nphi) != 0) {  // xi is a root of unity of order 2 nphi
+      delete h;
+      set_error("engine create: a prime of the bases has no root of unity of order 2 nphi");
+      return CP_ERR_UNSUPPORTED;
+    }
+    e.xi.push_back(canonical_xi(p, e.roots[i], (uint64_t)e.N));
+  }
+  e.plan = make_plan(e.logN, log_radix ? log_radix : 3);
+  int rc = build_tables(e);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return CP_OK;
+}
+
+cp_engine* new_engine(int k, int kl, int nphi, uint64_t t) {
+  cp_engine* h = new (std::nothrow) cp_engine();
+  if (!h) {
+    set_error("engine create: host allocation failed");
+    return nullptr;
+  }
+  Engine& e = h->e;
+  cudaGetDevice(&e.device);
+  e.k = k;
+  e.kl = kl;
+  e.nphi = nphi;
+  e.N = nphi / 2;
+  e.logN = 0;
+  while ((1 << e.logN) < e.N) ++e.logN;
+  e.t = t;
+  return h;
+}
+
+}  // namespace
+
+extern "C" {
+
 int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int log_radix) {
   CP_REQUIRE(out, "cp_engine_create: out is NULL");
   *out = nullptr;
@@ -56,45 +115,62 @@ int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int l
              "cp_engine_create: nphi must be a power of two in [2, 65536]");
   CP_REQUIRE(t >= 2 && t < kPrimes[kNumPrimes - 1], "cp_engine_create: t must be in [2, min prime)");
   CP_REQUIRE(log_radix == 0 || (log_radix >= 2 && log_radix <= 4), "cp_engine_create: log_radix must be 0, 2, 3 or 4");
-  cp_engine* h = new (std::nothrow) cp_engine();
-  if (!h) {
-    set_error("cp_engine_create: host allocation failed");
-    return CP_ERR_OOM;
-  }
+  cp_engine* h = new_engine(k, kl, nphi, t);
+  if (!h) return CP_ERR_OOM;
   Engine& e = h->e;
-  cudaGetDevice(&e.device);
-  e.k = k;
-  e.kl = kl;
-  e.nphi = nphi;
-  e.N = nphi / 2;
-  e.logN = 0;
-  while ((1 << e.logN) < e.N) ++e.logN;
-  e.t = t;
   for (int i = 0; i < k + kl; ++i) {
     const uint64_t p = kPrimes[i];
+    // the BFV base conversions rely on 2^64 mod p < 2^32 and p = 2^63 - c, c < 2^31 - 1
+    if ((uint64_t)(((unsigned __int128)1 << 64) % p) >> 32 || (p >> 63) || (1ull << 63) - p >= (1ull << 31) - 1) {
+      delete h;
+      set_error("cp_engine_create: prime outside the supported 63-bit form");
+      return CP_ERR_UNSUPPORTED;
+    }
     e.primes.push_back(p);
-    e.mconst.push_back(h_modconst(p));
-    if (e.mconst.back().r1 >> 32) {  // the lazy base-conversion reduction relies on 2^64 mod p < 2^32
-      delete h;
-      set_error("cp_engine_create: prime with 2^64 mod p >= 2^32 is not supported");
-      return CP_ERR_UNSUPPORTED;
-    }
-    if ((p >> 63) || (1ull << 63) - p >= (1ull << 31) - 1) {  // pm_red needs p = 2^63 - c, c < 2^31 - 1
-      delete h;
-      set_error("cp_engine_create: prime not of the form 2^63 - c with c < 2^31 - 1");
-      return CP_ERR_UNSUPPORTED;
-    }
-    e.xi.push_back(canonical_xi(p, kPrimitiveRoots[i], (uint64_t)e.N));
+    e.roots.push_back(kPrimitiveRoots[i]);
   }
-  e.plan = make_plan(e.logN, log_radix ? log_radix : 3);
-  int rc = build_tables(e);
-  if (rc) {
-    delete h;
-    return rc;
-  }
-  *out = h;
-  return CP_OK;
+  return finish_engine(out, h, log_radix);
 }
+
+int cp_ckks_engine_create(cp_engine** out, int k, int kl, int nphi, int prec, int log_radix) {
+  CP_REQUIRE(out, "cp_ckks_engine_create: out is NULL");
+  *out = nullptr;
+  if (kl <= 0) kl = k + 1;
+  CP_REQUIRE(prec == 45 || prec == 48 || prec == 52 || prec == 55,
+             "cp_ckks_engine_create: prec must be 45, 48, 52 or 55");
+  CP_REQUIRE(k >= 1 && k <= 24, "cp_ckks_engine_create: k must be in [1, 24]");
+  CP_REQUIRE(kl >= 1 && kl <= 24, "cp_ckks_engine_create: kl must be in [1, 24]");
+  CP_REQUIRE(nphi >= 2 && nphi <= 65536 && (nphi & (nphi - 1)) == 0,
+             "cp_ckks_engine_create: nphi must be a power of two in [2, 65536]");
+  CP_REQUIRE(log_radix == 0 || (log_radix >= 2 && log_radix <= 4),
+             "cp_ckks_engine_create: log_radix must be 0, 2, 3 or 4");
+  // Q = the first 63-bit prime, then k - 1 primes of the precision bucket; B = kl primes of
+  // the 45-bit (prec 45) or 55-bit bucket from index k - 1 (cuPoly cudaengine.cu:1192-1232)
+  const uint64_t* qb = prec == 45 ? kPrimes45 : prec == 48 ? kPrimes48 : prec == 52 ? kPrimes52 : kPrimes55;
+  const uint32_t* qr = prec == 45 ? kRoots45 : prec == 48 ? kRoots48 : prec == 52 ? kRoots52 : kRoots55;
+  const int qn = prec == 45 ? kNumPrimes45 : prec == 48 ? kNumPrimes48 : prec == 52 ? kNumPrimes52 : kNumPrimes55;
+  const uint64_t* bb = prec == 45 ? kPrimes45 : kPrimes55;
+  const uint32_t* br = prec == 45 ? kRoots45 : kRoots55;
+  const int bn = prec == 45 ? kNumPrimes45 : kNumPrimes55;
+  CP_REQUIRE(k - 1 <= qn && k - 1 + kl <= bn, "cp_ckks_engine_create: k, kl exceed the precision bucket");
+  cp_engine* h = new_engine(k, kl, nphi, 2);
+  if (!h) return CP_ERR_OOM;
+  Engine& e = h->e;
+  e.ckks_prec = prec;
+  e.primes.push_back(kPrimes[0]);
+  e.roots.push_back(kPrimitiveRoots[0]);
+  for (int i = 0; i < k - 1; ++i) {
+    e.primes.push_back(qb[i]);
+    e.roots.push_back(qr[i]);
+  }
+  for (int j = 0; j < kl; ++j) {
+    e.primes.push_back(bb[k - 1 + j]);
+    e.roots.push_back(br[k - 1 + j]);
+  }
+  return finish_engine(out, h, log_radix);
+}
+
+int cp_engine_ckks_prec(const cp_engine* h) { return h ? h->e.ckks_prec : -1; }
 
 int cp_engine_destroy(cp_engine* h) {
   if (!h) return CP_OK;
@@ -263,30 +339,36 @@ int cp_double_op_by_int(const cp_engine* h, void* b1, const void* a1, void* b2, 
 }
 
 int cp_basis_ext_q_to_b(const cp_engine* h, void* out_b, const void* in_q, int npolys, void* stream) {
+  CP_BFV_ONLY(h, "cp_basis_ext_q_to_b");
   CP_REQUIRE(h && out_b && in_q && npolys >= 0, "cp_basis_ext_q_to_b: bad argument");
   if (npolys == 0) return CP_OK;
   return hps_basis_ext(h->e, out_b, in_q, true, npolys, S(stream));
 }
 int cp_basis_ext_b_to_q(const cp_engine* h, void* out_q, const void* in_b, int npolys, void* stream) {
+  CP_BFV_ONLY(h, "cp_basis_ext_b_to_q");
   CP_REQUIRE(h && out_q && in_b && npolys >= 0, "cp_basis_ext_b_to_q: bad argument");
   if (npolys == 0) return CP_OK;
   return hps_basis_ext(h->e, out_q, in_b, false, npolys, S(stream));
 }
 int cp_complex_scaling(const cp_engine* h, void* out_b, const void* in_q, const void* in_b, int npolys,
                        void* stream) {
+  CP_BFV_ONLY(h, "cp_complex_scaling");
   CP_REQUIRE(h && out_b && in_q && in_b && npolys >= 0, "cp_complex_scaling: bad argument");
   if (npolys == 0) return CP_OK;
   return hps_complex_scaling(h->e, out_b, in_q, in_b, npolys, S(stream));
 }
 int cp_simple_scaling(const cp_engine* h, void* out_t, const void* in_q, void* stream) {
+  CP_BFV_ONLY(h, "cp_simple_scaling");
   CP_REQUIRE(h && out_t && in_q, "cp_simple_scaling: bad argument");
   return hps_simple_scaling(h->e, out_t, in_q, S(stream));
 }
 int cp_xi(const cp_engine* h, void* out, const void* in, void* stream) {
+  CP_BFV_ONLY(h, "cp_xi");
   CP_REQUIRE(h && out && in, "cp_xi: bad argument");
   return rns_xi_rho(h->e, out, in, false, S(stream));
 }
 int cp_rho(const cp_engine* h, void* out, const void* in, void* stream) {
+  CP_BFV_ONLY(h, "cp_rho");
   CP_REQUIRE(h && out && in, "cp_rho: bad argument");
   return rns_xi_rho(h->e, out, in, true, S(stream));
 }
@@ -306,6 +388,7 @@ static int d2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   } while (0)
 
 int cp_poly_basis_extension_q_to_b(const cp_engine* h, void* out_b, const void* in_q, void* ws, void* stream) {
+  CP_BFV_ONLY(h, "cp_poly_basis_extension_q_to_b");
   CP_REQUIRE(h && out_b && in_q && ws, "cp_poly_basis_extension_q_to_b: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
@@ -317,6 +400,7 @@ int cp_poly_basis_extension_q_to_b(const cp_engine* h, void* out_b, const void* 
 }
 
 int cp_poly_basis_extension_q_to_qb(const cp_engine* h, void* out_qb, const void* in_q, void* ws, void* stream) {
+  CP_BFV_ONLY(h, "cp_poly_basis_extension_q_to_qb");
   CP_REQUIRE(h && out_qb && in_q && ws, "cp_poly_basis_extension_q_to_qb: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
@@ -330,6 +414,7 @@ int cp_poly_basis_extension_q_to_qb(const cp_engine* h, void* out_qb, const void
 }
 
 int cp_poly_basis_extension_b_to_q(const cp_engine* h, void* out_q, const void* in_b, void* ws, void* stream) {
+  CP_BFV_ONLY(h, "cp_poly_basis_extension_b_to_q");
   CP_REQUIRE(h && out_q && in_b && ws, "cp_poly_basis_extension_b_to_q: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
@@ -341,6 +426,7 @@ int cp_poly_basis_extension_b_to_q(const cp_engine* h, void* out_q, const void* 
 
 int cp_poly_complex_scaling_tdivq(const cp_engine* h, void* out_q, void* in_q, void* in_b, unsigned flags, void* ws,
                                   void* stream) {
+  CP_BFV_ONLY(h, "cp_poly_complex_scaling_tdivq");
   CP_REQUIRE(h && out_q && in_q && in_b && ws, "cp_poly_complex_scaling_tdivq: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
@@ -362,6 +448,7 @@ int cp_poly_complex_scaling_tdivq(const cp_engine* h, void* out_q, void* in_q, v
 }
 
 int cp_poly_simple_scaling_tdivq(const cp_engine* h, void* out_t, const void* in_q, void* ws, void* stream) {
+  CP_BFV_ONLY(h, "cp_poly_simple_scaling_tdivq");
   CP_REQUIRE(h && out_t && in_q && ws, "cp_poly_simple_scaling_tdivq: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
@@ -372,6 +459,7 @@ int cp_poly_simple_scaling_tdivq(const cp_engine* h, void* out_t, const void* in
 
 int cp_bfv_mul(const cp_engine* h, void* c0, void* c1, void* c2, const void* a0, const void* a1, const void* b0,
                const void* b1, void* ws, void* stream) {
+  CP_BFV_ONLY(h, "cp_bfv_mul");
   CP_REQUIRE(h && c0 && c1 && c2 && a0 && a1 && b0 && b1 && ws, "cp_bfv_mul: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
@@ -401,6 +489,7 @@ size_t cp_bfv_mul_batch_workspace_bytes(const cp_engine* h, int npairs) {
 
 int cp_bfv_mul_batch(const cp_engine* h, void* c, const void* a0, const void* a1, const void* b0, const void* b1,
                      int npairs, void* ws, void* stream) {
+  CP_BFV_ONLY(h, "cp_bfv_mul_batch");
   CP_REQUIRE(h && c && a0 && a1 && b0 && b1 && ws && npairs >= 0, "cp_bfv_mul_batch: bad argument");
   if (npairs == 0) return CP_OK;
   const Engine& e = h->e;

@@ -27,7 +27,8 @@ constexpr int kMaxIcrt = 24;  // largest base recombined by cp_icrt (|Q|, |B| <=
 // One thread per Gaussian element (coefficients j and j + N) of one residue.
 __global__ void __launch_bounds__(256) k_crt(ulonglong2* __restrict__ out, const uint64_t* __restrict__ coefs,
                                              int nlimbs, int N, int nres, int rid_off,
-                                             const ModConst* __restrict__ mc, const uint64_t* __restrict__ pow64) {
+                                             const ModConst* __restrict__ mc, const uint64_t* __restrict__ pow64,
+                                             const uint64_t* __restrict__ pow64m) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= N) return;
   const int y = blockIdx.y;  // poly * nres + r
@@ -37,13 +38,25 @@ __global__ void __launch_bounds__(256) k_crt(ulonglong2* __restrict__ out, const
   const uint64_t* w = pow64 + (size_t)rid * kMaxLimbs;
   const uint64_t* c0 = coefs + ((size_t)poly * 2 * N + j) * nlimbs;
   const uint64_t* c1 = c0 + (size_t)N * nlimbs;
-  uint64_t l0 = 0, h0 = 0, t0 = 0, l1 = 0, h1 = 0, t1 = 0;
-  for (int l = 0; l < nlimbs; ++l) {  // each product < 2^127; 64 terms < 2^133
-    const uint64_t wl = __ldg(w + l);
-    mac192(l0, h0, t0, c0[l], wl);
-    mac192(l1, h1, t1, c1[l], wl);
+  if (m.pm) {  // 63-bit primes (2^64 mod p < 2^32): lazy 192-bit sums, one reduction
+    uint64_t l0 = 0, h0 = 0, t0 = 0, l1 = 0, h1 = 0, t1 = 0;
+    for (int l = 0; l < nlimbs; ++l) {  // each product < 2^127; 64 terms < 2^133
+      const uint64_t wl = __ldg(w + l);
+      mac192(l0, h0, t0, c0[l], wl);
+      mac192(l1, h1, t1, c1[l], wl);
+    }
+    out[(size_t)y * N + j] =
+        make_ulonglong2(red192(l0, h0, t0, m.p, m.r1, m.r2), red192(l1, h1, t1, m.p, m.r1, m.r2));
+  } else {  // other primes: one Montgomery product per limb with 2^(64 l) in Montgomery form
+    const uint64_t* wm = pow64m + (size_t)rid * kMaxLimbs;
+    uint64_t a0 = 0, a1 = 0;
+    for (int l = 0; l < nlimbs; ++l) {
+      const uint64_t wl = __ldg(wm + l);
+      a0 = add_mod(a0, mont_mul(c0[l], wl, m.p, m.pneg), m.p);
+      a1 = add_mod(a1, mont_mul(c1[l], wl, m.p, m.pneg), m.p);
+    }
+    out[(size_t)y * N + j] = make_ulonglong2(a0, a1);
   }
-  out[(size_t)y * N + j] = make_ulonglong2(red192(l0, h0, t0, m.p, m.r1, m.r2), red192(l1, h1, t1, m.p, m.r1, m.r2));
 }
 
 // One thread per coefficient (index jj in [0, nphi)) of polynomial blockIdx.y.
@@ -66,7 +79,8 @@ __global__ void __launch_bounds__(128) k_icrt(uint64_t* __restrict__ coefs, int 
     const uint64_t si = mc[src_off + i].p;
     uint64_t y = d[i];
     for (int l = 0; l < i; ++l) {
-      const uint64_t dl = red2p(d[l], si);  // d_l < s_l < 2 s_i (all primes within 2^31 of 2^63)
+      uint64_t dl = d[l];  // d_l < s_l: one subtraction for primes of one size, a division otherwise
+      if (dl >= si) dl = dl - si < si ? dl - si : dl % si;
       const int c = i * (i - 1) / 2 + l;
       y = shoup_mul(y + si - dl, __ldg(inv + c), __ldg(inv_s + c), si);
     }
@@ -146,7 +160,7 @@ int cp_crt(const cp_engine* h, void* out, const uint64_t* coefs, int nlimbs, int
   dim3 grid((e.N + 255) / 256, npolys * nres);
   k_crt<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       reinterpret_cast<ulonglong2*>(out), coefs, nlimbs, e.N, nres, e.rid_offset(base), e.d_mc,
-      e.d_hps + e.ho.pow64);
+      e.d_hps + e.ho.pow64, e.d_hps + e.ho.pow64m);
   return check_launch("cp_crt");
 }
 

@@ -117,6 +117,36 @@ int launch_dgt_ex(const Engine& e, void* dst_v, const void* fsrc_v, const InvSrc
   return launch_split(e, data, nullptr, nres, rid_off, npolys, poly_stride, true, st);
 }
 
+// Residues rid_off .. rid_off + nres - 1 of npolys polynomials (stride poly_stride
+// elements), from src (nullptr: in place) into dst.
+int launch_dgt_part(const Engine& e, void* dst_v, const void* src_v, int rid_off, int nres, int npolys,
+                    long long poly_stride, bool inverse, cudaStream_t st) {
+  if (nres <= 0 || npolys <= 0) return 0;
+  RunFn fn = pick(e.plan.logNc, e.plan.logR);
+  if (!fn) {
+    set_error("dgt: no kernel for this size");
+    return 3;
+  }
+  ulonglong2* data = reinterpret_cast<ulonglong2*>(dst_v);
+  const ulonglong2* src = reinterpret_cast<const ulonglong2*>(src_v);
+  InvSrc isrc{};
+  isrc.p[0] = src ? src : data;
+  isrc.mode = 0;
+  isrc.npairs = 1;
+  const int S = e.plan.S;
+  if (!inverse) {
+    if (S > 0) {
+      int rc = launch_split(e, data, src, nres, rid_off, npolys, poly_stride, false, st);
+      if (rc) return rc;
+      return fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, false, false, st, nullptr);
+    }
+    return fn(e, data, src, isrc, nres, rid_off, npolys, poly_stride, false, true, st, nullptr);
+  }
+  int rc = fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, true, S == 0, st, nullptr);
+  if (rc || S == 0) return rc;
+  return launch_split(e, data, nullptr, nres, rid_off, npolys, poly_stride, true, st);
+}
+
 int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly_stride, bool inverse,
                cudaStream_t st) {
   return launch_dgt_ex(e, data, nullptr, nullptr, base, npolys, poly_stride, inverse, st);

@@ -89,6 +89,8 @@ struct Engine {
   int k = 0, kl = 0;
   uint64_t t = 0;
   std::vector<uint64_t> primes;   // Q then B
+  std::vector<uint64_t> roots;    // a primitive root of each prime
+  int ckks_prec = 0;              // 0: BFV engine (63-bit primes); 45/48/52/55: CKKS precision bucket
   std::vector<ModConst> mconst;
   std::vector<std::pair<uint64_t, uint64_t>> xi;  // Gaussian root of i used for the twist, per residue
   DgtPlan plan;
@@ -116,6 +118,15 @@ struct Engine {
     int qq_w, bb_w;                // Garner weights of Q and of B, [i][l]
     int q_pinv, q_pinv_s, b_pinv, b_pinv_s;  // (prod_{j<i} s_j)^-1 mod s_i
     int pow64;                     // 2^(64 l) mod p_r, [residue][kMaxLimbs]
+    int pow64m;                    // 2^(64 (l + 1)) mod p_r (Montgomery form of pow64), same shape
+    // CKKS (only when ckks_prec != 0); every constant with its Shoup companion
+    int ck_inv_ql, ck_inv_ql_s;    // q_l^-1 mod q_i, [l][i]
+    int ck_qlqi_inv, ck_qlqi_inv_s;  // (Q_l / q_i)^-1 mod q_i, [l][i]; Q_l = q_0 ... q_l
+    int ck_qlqi_b, ck_qlqi_b_s;    // (Q_l / q_i) mod b_j, [l][i][j]
+    int ck_bbj_inv, ck_bbj_inv_s;  // (B / b_j)^-1 mod b_j, [j]
+    int ck_bbj_q, ck_bbj_q_s;      // (B / b_j) mod q_i, [j][i]
+    int ck_binv_q, ck_binv_q_s;    // B^-1 mod q_i, [i]
+    int ck_b_q, ck_b_q_s;          // B mod q_i, [i]
   } ho{};
   uint64_t t_shoup_one = 0;        // floor(2^64 / t)
   uint64_t h_q_mod_t = 0, h_qinv_t = 0, h_qinv_t_s = 0;  // Q mod t, Q^-1 mod t

@@ -28,9 +28,10 @@ namespace cpoly {
 struct ModConst {
   uint64_t p;       // the prime
   uint64_t pneg;    // -p^-1 mod 2^64
-  uint64_t r1;      // 2^64 mod p (below 2^32 for every prime of the table)
+  uint64_t r1;      // 2^64 mod p (below 2^32 for every 63-bit prime of the table)
   uint64_t r1s;     // shoup companion of r1
   uint64_t r2;      // 2^128 mod p
+  uint64_t pm;      // 1: p = 2^63 - c with c < 2^31 - 1 (pm_red applies); 0: generic path
 };
 
 // Three-word accumulation (t:h:l) += a * b, for lazily reduced dot products.
@@ -127,9 +128,22 @@ CP_HD uint64_t pm_red(uint64_t hi, uint64_t lo, uint64_t p) {
   return red2p((zl & 0x7FFFFFFFFFFFFFFFull) + Zh * c, p);
 }
 
+// hi:lo mod p for hi:lo < p 2^64, any p < 2^63: Montgomery step, then the
+// factor 2^64 restored by a Shoup product with r1 = 2^64 mod p.
+CP_HD uint64_t gen_red(uint64_t hi, uint64_t lo, const ModConst& m) {
+  return shoup_mul(mont_redc(hi, lo, m.p, m.pneg), m.r1, m.r1s, m.p);
+}
+
+// hi:lo mod p: pseudo-Mersenne folding for the 63-bit primes, the generic
+// Montgomery path for the others (the CKKS precision buckets).  Callers keep
+// hi:lo < min(2^127, p 2^64).  The branch is uniform across a residue.
+CP_HD uint64_t red128(uint64_t hi, uint64_t lo, const ModConst& m) {
+  return m.pm ? pm_red(hi, lo, m.p) : gen_red(hi, lo, m);
+}
+
 // Exact a * b mod p for a < p, b < 2^64.
 CP_HD uint64_t mul_mod(uint64_t a, uint64_t b, const ModConst& m) {
-  return pm_red(mulhi64(a, b), a * b, m.p);
+  return red128(mulhi64(a, b), a * b, m);
 }
 
 // 128-bit accumulate helpers (hi:lo += a * b).
@@ -140,8 +154,8 @@ CP_HD void mac128(uint64_t& hi, uint64_t& lo, uint64_t a, uint64_t b) {
 }
 
 // Gaussian integer (re + im i) mod p: exact product, result canonical.
-// re = a0 b0 + a1 (p - b1), im = a0 b1 + a1 b0, each < 2 p^2 < 2^127,
-// reduced by pm_red.
+// re = a0 b0 + a1 (p - b1), im = a0 b1 + a1 b0, each < 2 p^2 < min(2^127, p 2^64),
+// reduced by red128.
 CP_HD void gi_mul(uint64_t& cr, uint64_t& ci, uint64_t a0, uint64_t a1, uint64_t b0,
                   uint64_t b1, const ModConst& m) {
   uint64_t rh = 0, rl = 0, ih = 0, il = 0;
@@ -149,8 +163,8 @@ CP_HD void gi_mul(uint64_t& cr, uint64_t& ci, uint64_t a0, uint64_t a1, uint64_t
   mac128(rh, rl, a1, b1 == 0 ? 0 : m.p - b1);
   mac128(ih, il, a0, b1);
   mac128(ih, il, a1, b0);
-  cr = pm_red(rh, rl, m.p);
-  ci = pm_red(ih, il, m.p);
+  cr = red128(rh, rl, m);
+  ci = red128(ih, il, m);
 }
 
 // Gaussian times a Gaussian constant with Shoup companions (4 shoup products).
@@ -193,6 +207,7 @@ inline ModConst h_modconst(uint64_t p) {
   m.r1 = (uint64_t)(((unsigned __int128)1 << 64) % p);
   m.r1s = h_shoup(m.r1, p);
   m.r2 = h_mulmod(m.r1, m.r1, p);
+  m.pm = (p >> 63) == 0 && (1ull << 63) - p < (1ull << 31) - 1;
   return m;
 }
 

@@ -176,7 +176,7 @@ int build_tables(Engine& e) {
   parallel_for(nres, [&](int r) {
     const uint64_t p = e.primes[r];
     ulonglong2* T = tab.data() + (size_t)r * L.stride;
-    const uint64_t gen = primitive_root_of(p);
+    const uint64_t gen = e.roots[r];
     const uint64_t wN = omega(p, gen, (uint64_t)N);
     const uint64_t wNi = h_invmod(wN, p);
     // powers of w_N and w_N^-1
@@ -384,6 +384,67 @@ int build_tables(Engine& e) {
       }
     }
     e.ho.pow64 = append(v);
+    std::vector<uint64_t> vm;  // the same powers times 2^64 (for the Montgomery path)
+    for (auto p : e.primes) {
+      const uint64_t r1 = (uint64_t)(((unsigned __int128)1 << 64) % p);
+      uint64_t acc = r1;
+      for (int l = 0; l < kMaxLimbs; ++l) {
+        vm.push_back(acc);
+        acc = h_mulmod(acc, r1, p);
+      }
+    }
+    e.ho.pow64m = append(vm);
+  }
+  if (e.ckks_prec) {
+    const int k = e.k, kl = e.kl;
+    std::vector<uint64_t> a, as, b, bs, c, cs, d, ds, f, fs, g, gs, h, hs;
+    for (int l = 0; l < k; ++l)
+      for (int i = 0; i < k; ++i) {
+        const uint64_t qi = Q[i];
+        const uint64_t inv_ql = i < l ? h_invmod(Q[l] % qi, qi) : 0;
+        push_pair(inv_ql, qi, a, as);
+        uint64_t m = 1 % qi;  // Q_l / q_i mod q_i
+        for (int u = 0; u <= l; ++u)
+          if (u != i) m = h_mulmod(m, Q[u] % qi, qi);
+        push_pair(i <= l ? h_invmod(m, qi) : 0, qi, b, bs);
+        for (int j = 0; j < kl; ++j) {
+          uint64_t mb = 1 % B[j];  // Q_l / q_i mod b_j
+          for (int u = 0; u <= l; ++u)
+            if (u != i) mb = h_mulmod(mb, Q[u] % B[j], B[j]);
+          push_pair(i <= l ? mb : 0, B[j], c, cs);
+        }
+      }
+    for (int j = 0; j < kl; ++j) {
+      uint64_t m = 1 % B[j];
+      for (int u = 0; u < kl; ++u)
+        if (u != j) m = h_mulmod(m, B[u] % B[j], B[j]);
+      push_pair(h_invmod(m, B[j]), B[j], d, ds);
+      for (int i = 0; i < k; ++i) {
+        uint64_t mq = 1 % Q[i];
+        for (int u = 0; u < kl; ++u)
+          if (u != j) mq = h_mulmod(mq, B[u] % Q[i], Q[i]);
+        push_pair(mq, Q[i], f, fs);
+      }
+    }
+    for (int i = 0; i < k; ++i) {
+      const uint64_t bq = prod_mod(B, Q[i]);
+      push_pair(h_invmod(bq, Q[i]), Q[i], g, gs);
+      push_pair(bq, Q[i], h, hs);
+    }
+    e.ho.ck_inv_ql = append(a);
+    e.ho.ck_inv_ql_s = append(as);
+    e.ho.ck_qlqi_inv = append(b);
+    e.ho.ck_qlqi_inv_s = append(bs);
+    e.ho.ck_qlqi_b = append(c);
+    e.ho.ck_qlqi_b_s = append(cs);
+    e.ho.ck_bbj_inv = append(d);
+    e.ho.ck_bbj_inv_s = append(ds);
+    e.ho.ck_bbj_q = append(f);
+    e.ho.ck_bbj_q_s = append(fs);
+    e.ho.ck_binv_q = append(g);
+    e.ho.ck_binv_q_s = append(gs);
+    e.ho.ck_b_q = append(h);
+    e.ho.ck_b_q_s = append(hs);
   }
   e.hps_words = H.size();
 

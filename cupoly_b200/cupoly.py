@@ -78,6 +78,23 @@ class CUDAEngine:
         cls.is_init = True
 
     @classmethod
+    def init_ckks(cls, k: int, kl: int, M: int, prec: int, log_radix: int = 0):
+        """CKKS build's init(k, kl, M, prec): Q = the first 63-bit prime and k - 1
+        primes of the prec-bit bucket, B = kl primes (cudaengine.cu:1192-1290)."""
+        if cls.is_init:
+            cls.destroy()
+        cls.engine = Engine.ckks(k, kl if kl > 0 else k + 1, M, prec, log_radix)
+        cls.N = M >> 1
+        cls.t = prec
+        cls.RNSPrimes = list(cls.engine.Q)
+        cls.RNSBPrimes = list(cls.engine.B)
+        cls.RNSProduct = _prod(cls.RNSPrimes)
+        cls.RNSBProduct = _prod(cls.RNSBPrimes)
+        cls.RNSMpi = [cls.RNSProduct // p for p in cls.RNSPrimes]
+        cls.RNSInvMpi = [pow(m % p, -1, p) for m, p in zip(cls.RNSMpi, cls.RNSPrimes)]
+        cls.is_init = True
+
+    @classmethod
     def destroy(cls):
         if cls.engine is not None:
             torch.cuda.synchronize()
@@ -557,6 +574,58 @@ def poly_rho_bfv(ctx, c: List[poly_t], a: poly_t):
 # ---------------------------------------------------------------------------
 # Sampler (sampler.h:53-101)
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# CKKS mode (polynomial.cu:530-608, 696-800)
+# ---------------------------------------------------------------------------
+def poly_approx_basis_raising_Q_to_QB(ctx, a, b, level: int):
+    """a (QB) <- b (Q) with the B residues of the approximate conversion from Q_level."""
+    assert a.init and b.base == QBase
+    poly_copy_to_device(ctx, b)
+    e = _E()
+    a.base = QBBase
+    with torch.cuda.stream(ctx.stream):
+        a.d_coefs = e.empty(QBBase)
+    e.ckks_modulus_raising(a.d_coefs, b.d_coefs, level, stream=ctx.stream)
+    a.status = RNSSTATE
+
+
+def poly_approx_basis_reduction_QB_to_Q(ctx, a, b, level: int):
+    """a (Q) residues 0..level <- approximate division of b (QB) by B."""
+    assert a.init and a.base == QBase and b.base == QBBase
+    poly_copy_to_device(ctx, a)
+    poly_copy_to_device(ctx, b)
+    _E().ckks_modulus_reduction(a.d_coefs, b.d_coefs, level, stream=ctx.stream)
+    a.status = RNSSTATE
+
+
+def poly_ckks_rescale(ctx, a, b, level: int):
+    """Divide a and b by q_level (rounding toward the residue), in place."""
+    assert a.init and a.base == QBase
+    poly_copy_to_device(ctx, a)
+    if b is not None:
+        poly_copy_to_device(ctx, b)
+    _E().ckks_rescale(a.d_coefs, b.d_coefs if b is not None else None, level, stream=ctx.stream)
+    a.status = RNSSTATE
+    if b is not None:
+        b.status = RNSSTATE
+
+
+def poly_xi_ckks(ctx, c, a):
+    assert a.init and a.base == QBase
+    poly_copy_to_device(ctx, a)
+    poly_init(ctx, c)
+    _E().ckks_xi(c.d_coefs, a.d_coefs, stream=ctx.stream)
+    c.status = RNSSTATE
+
+
+def poly_rho_ckks(ctx, c, a):
+    assert a.init and a.base in (QBase, QBBase)
+    poly_copy_to_device(ctx, a)
+    poly_init(ctx, c)
+    _E().ckks_rho(c.d_coefs, a.d_coefs, stream=ctx.stream)
+    c.status = RNSSTATE
+
+
 class Sampler:
     seed = SEED
     _counter = 0
@@ -568,6 +637,23 @@ class Sampler:
     @classmethod
     def reset(cls, ctx: Context):
         cls._counter = 0
+
+    @classmethod
+    def init_ckks(cls, k: int, kl: int, M: int, prec: int, log_radix: int = 0):
+        """CKKS build's init(k, kl, M, prec): Q = the first 63-bit prime and k - 1
+        primes of the prec-bit bucket, B = kl primes (cudaengine.cu:1192-1290)."""
+        if cls.is_init:
+            cls.destroy()
+        cls.engine = Engine.ckks(k, kl if kl > 0 else k + 1, M, prec, log_radix)
+        cls.N = M >> 1
+        cls.t = prec
+        cls.RNSPrimes = list(cls.engine.Q)
+        cls.RNSBPrimes = list(cls.engine.B)
+        cls.RNSProduct = _prod(cls.RNSPrimes)
+        cls.RNSBProduct = _prod(cls.RNSBPrimes)
+        cls.RNSMpi = [cls.RNSProduct // p for p in cls.RNSPrimes]
+        cls.RNSInvMpi = [pow(m % p, -1, p) for m, p in zip(cls.RNSMpi, cls.RNSPrimes)]
+        cls.is_init = True
 
     @classmethod
     def destroy(cls):

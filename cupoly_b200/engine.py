@@ -93,7 +93,10 @@ def dgt_op_counts(N: int) -> dict:
 class Engine:
     """One parameter set: ring degree nphi, |Q| = k, |B| = kl, plaintext modulus t."""
 
-    def __init__(self, k: int, kl: int = 0, nphi: int = 4096, t: int = 256, log_radix: int = 0):
+    def __init__(self, k: int, kl: int = 0, nphi: int = 4096, t: int = 256, log_radix: int = 0,
+                 ckks_prec: int = 0):
+        """BFV engine (63-bit primes, plaintext modulus t), or with ckks_prec in
+        {45, 48, 52, 55} a CKKS engine (cuPoly's CKKS build; t unused)."""
         if not torch.cuda.is_available():
             raise RuntimeError("cupoly_b200 needs a CUDA device")
         _lib.lib()
@@ -102,7 +105,12 @@ class Engine:
 
             log_radix = cached_log_radix(nphi)
         h = C.c_void_p()
-        call("cp_engine_create", C.byref(h), k, kl, nphi, t, log_radix)
+        if ckks_prec:
+            call("cp_ckks_engine_create", C.byref(h), k, kl, nphi, ckks_prec, log_radix)
+            t = 2
+        else:
+            call("cp_engine_create", C.byref(h), k, kl, nphi, t, log_radix)
+        self.ckks_prec = ckks_prec
         self.log_radix = log_radix
         self._h = h
         self.k = k
@@ -209,6 +217,28 @@ class Engine:
     def double_op_by_int(self, b1, a1, b2, a2, base, x1, x2, op, stream=None):
         call("cp_double_op_by_int", self._h, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), base, int(x1), int(x2), op,
              _stream(stream))
+
+    # ---- CKKS (CKKS engines) ----
+    @classmethod
+    def ckks(cls, k: int, kl: int, nphi: int, prec: int, log_radix: int = 0) -> "Engine":
+        return cls(k, kl, nphi, 2, log_radix, ckks_prec=prec)
+
+    def ckks_modulus_raising(self, out_qb, in_q, level: int, stream=None):
+        call("cp_ckks_modulus_raising", self._h, _ptr(out_qb), _ptr(in_q), level, _ptr(self.workspace()),
+             _stream(stream))
+
+    def ckks_modulus_reduction(self, out_q, in_qb, level: int, stream=None):
+        call("cp_ckks_modulus_reduction", self._h, _ptr(out_q), _ptr(in_qb), level, _ptr(self.workspace()),
+             _stream(stream))
+
+    def ckks_rescale(self, a, b, level: int, stream=None):
+        call("cp_ckks_rescale", self._h, _ptr(a), _ptr(b), level, _stream(stream))
+
+    def ckks_xi(self, out, a, stream=None):
+        call("cp_ckks_xi", self._h, _ptr(out), _ptr(a), _stream(stream))
+
+    def ckks_rho(self, out, a, stream=None):
+        call("cp_ckks_rho", self._h, _ptr(out), _ptr(a), _stream(stream))
 
     # ---- coefficient I/O (big integers <-> residues, on the device) ----
     def crt(self, out, coefs_limbs: torch.Tensor, base: int = QBase, stream=None):

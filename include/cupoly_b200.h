@@ -68,6 +68,17 @@ const char* cp_last_error(void);
  *      created on the current CUDA device.  log_radix in {3, 4} picks the DGT
  *      register radix (0 = default). */
 int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int log_radix);
+/* CKKS-mode engine: replaces CUDAEngine::init(k, kl, M, prec) of cuPoly's CKKS build
+ * (src/cuda/cudaengine.cu:1192-1290).  Q = the first 63-bit prime followed by k - 1
+ * primes of the prec-bit bucket (prec in {45, 48, 52, 55}); B = kl primes of the
+ * 45-bit (prec 45) or 55-bit bucket starting at index k - 1.  Every prime must have
+ * 2 nphi | p - 1 (CP_ERR_UNSUPPORTED otherwise).  The BFV base conversions and
+ * scalings (cp_basis_ext_*, cp_*_scaling, cp_xi/cp_rho, cp_bfv_mul*) refuse a CKKS
+ * engine with CP_ERR_UNSUPPORTED; the DGT, pointwise, sampler, CRT and wire calls
+ * work on both. */
+int cp_ckks_engine_create(cp_engine** out, int k, int kl, int nphi, int prec, int log_radix);
+/* precision bucket of a CKKS engine, 0 for a BFV engine */
+int cp_engine_ckks_prec(const cp_engine* e);
 int cp_engine_destroy(cp_engine* e);
 int cp_engine_n_residues(const cp_engine* e, int base);
 int cp_engine_nphi(const cp_engine* e);
@@ -178,6 +189,27 @@ int cp_bfv_mul_batch(const cp_engine* e, void* c, const void* a0, const void* a1
  *      0 Shoup constant multiply, 1 data x data modular multiply, 2 modular add,
  *      3 32-bit multiply-add.  sink: nthreads uint64 of device memory. ---- */
 int cp_calibrate_int(int kind, int iters, void* sink, long long nthreads, float* ms, void* stream);
+
+/* ---- CKKS operations (CKKS engines only), DGT domain in and out, level l in [0, k)
+ *      (rescale: [1, k)); Q_l = q_0 ... q_l.  They replace fast_conv_Q_to_B /
+ *      fast_conv_B_to_Q / ckks_rescale / xi_ckks_rns_rid / rho_ckks_rns_rid
+ *      (src/cuda/cudaengine.cu:800-981, 1086-1184) and poly_approx_basis_raising_Q_to_QB /
+ *      poly_approx_basis_reduction_QB_to_Q / poly_ckks_rescale / poly_xi_ckks /
+ *      poly_rho_ckks (src/arithmetic/polynomial.cu:530-608, 696-800).
+ *  raising:   out_qb Q part = in_q; B part y_j = sum_{i<=l} [x_i (Q_l/q_i)^-1]_{q_i} (Q_l/q_i) mod b_j.
+ *  reduction: out_q residues i <= l: (x_i - sum_j [y_j (B/b_j)^-1]_{b_j} (B/b_j)) B^-1 mod q_i;
+ *             residues above l are not written.
+ *  rescale:   in place on a and b (b may be NULL): x_i <- (x_i - x_l) q_l^-1 mod q_i for i < l;
+ *             residues l and above are left as they were.
+ *  xi / rho:  out_i = x_i B^-1 mod q_i / x_i B mod q_i over the Q residues.
+ *  `workspace` holds cp_workspace_bytes(e) bytes of device memory. ---- */
+int cp_ckks_modulus_raising(const cp_engine* e, void* out_qb, const void* in_q, int level, void* workspace,
+                            void* stream);
+int cp_ckks_modulus_reduction(const cp_engine* e, void* out_q, const void* in_qb, int level, void* workspace,
+                              void* stream);
+int cp_ckks_rescale(const cp_engine* e, void* a, void* b, int level, void* stream);
+int cp_ckks_xi(const cp_engine* e, void* out, const void* in, void* stream);
+int cp_ckks_rho(const cp_engine* e, void* out, const void* in, void* stream);
 
 /* ---- coefficient I/O on the device: replaces the host NTL conversions poly_crt /
  *      poly_icrt (src/arithmetic/polynomial.cu:190-296).  Coefficients are unsigned

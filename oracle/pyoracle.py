@@ -43,6 +43,67 @@ def bases(k: int, kl: int):
     return PRIMES[:k], PRIMES[k:k + kl]
 
 
+_CKKS_HEADER = os.path.join(_HERE, "..", "cupoly_b200", "csrc", "prime_table_ckks.h")
+
+
+@lru_cache(maxsize=None)
+def ckks_bucket(bits: int):
+    """The bits-bit CKKS prime bucket (cuPoly ``src/arithmetic/coprimes.cu:9-762``)."""
+    src = open(_CKKS_HEADER).read()
+    m = _re.search(r"kPrimes%d\[kNumPrimes%d\]\s*=\s*\{([^}]*)\}" % (bits, bits), src)
+    return [int(x.strip().rstrip("ULL")) for x in m.group(1).split(",") if x.strip()]
+
+
+@lru_cache(maxsize=None)
+def ckks_roots(bits: int):
+    src = open(_CKKS_HEADER).read()
+    m = _re.search(r"kRoots%d\[kNumPrimes%d\]\s*=\s*\{([^}]*)\}" % (bits, bits), src)
+    return [int(x) for x in m.group(1).split(",") if x.strip()]
+
+
+for _b in (45, 48, 52, 55):  # primitive roots of the CKKS primes, for the DGT restatement
+    PROOT.update(zip(ckks_bucket(_b), ckks_roots(_b)))
+
+
+def ckks_bases(k: int, kl: int, prec: int):
+    """CKKS Q and B (cuPoly ``src/cuda/cudaengine.cu:1192-1232``): Q = the first 63-bit
+    prime + k - 1 primes of the prec bucket; B = kl primes of the 45-bit (prec 45) or
+    55-bit bucket from index k - 1."""
+    qb = ckks_bucket(prec)
+    bb = ckks_bucket(45 if prec == 45 else 55)
+    return [PRIMES[0]] + qb[:k - 1], bb[k - 1:k - 1 + kl]
+
+
+def ckks_modulus_raising(xs, Q, B, level):
+    """B residues of fast_conv_Q_to_B (``src/cuda/cudaengine.cu:893-925``) for one
+    coefficient with residues xs over Q_l = Q[0..level]:
+    y_j = sum_i [x_i (Q_l/q_i)^-1]_{q_i} (Q_l/q_i) mod b_j."""
+    Ql = prod(Q[:level + 1])
+    out = []
+    for b in B:
+        acc = 0
+        for i in range(level + 1):
+            Mi = Ql // Q[i]
+            acc += (xs[i] * pow(Mi % Q[i], -1, Q[i]) % Q[i]) * Mi
+        out.append(acc % b)
+    return out
+
+
+def ckks_modulus_reduction(xs, ys, Q, B, level):
+    """Q residues of fast_conv_B_to_Q (``src/cuda/cudaengine.cu:802-845``):
+    z_i = (x_i - sum_j [y_j (B/b_j)^-1]_{b_j} (B/b_j)) B^-1 mod q_i, i <= level."""
+    Bp = prod(B)
+    V = sum((y * pow((Bp // b) % b, -1, b) % b) * (Bp // b) for y, b in zip(ys, B))
+    return [(xs[i] - V) * pow(Bp % Q[i], -1, Q[i]) % Q[i] for i in range(level + 1)]
+
+
+def ckks_rescale(xs, Q, level):
+    """ckks_rescale (``src/cuda/cudaengine.cu:851-889``): x_i <- (x_i - x_l) q_l^-1
+    mod q_i for i < level; residues from level on unchanged."""
+    ql = Q[level]
+    return [(xs[i] - xs[level]) * pow(ql, -1, Q[i]) % Q[i] for i in range(level)] + list(xs[level:])
+
+
 def prod(xs):
     r = 1
     for x in xs:

@@ -26,11 +26,12 @@ def splitmix64(seed: int, stream: int, n: int) -> np.ndarray:
 
 
 def uniform_mod(seed: int, stream: int, n: int, p: int) -> np.ndarray:
-    """n values uniform in [0, p) for a 63-bit prime p (rejection on 63 bits)."""
+    """n values uniform in [0, p) (rejection on bit_length(p) bits: 63 for the BFV primes)."""
     out = np.empty(0, dtype=np.uint64)
     k = 0
+    shift = np.uint64(64 - int(p).bit_length())
     while out.size < n:
-        w = splitmix64(seed, stream * 1000003 + k, 2 * n) >> np.uint64(1)
+        w = splitmix64(seed, stream * 1000003 + k, 2 * n) >> shift
         out = np.concatenate([out, w[w < np.uint64(p)]])
         k += 1
     return out[:n]
