@@ -241,8 +241,8 @@ def run_ours(args, D: Dist):
     ms = D.max(ev0.elapsed_time(ev1))
     value = D.world * P * args.steps / (ms / 1e3)
     # inverse DGT (gather) + Q->B + forward DGT(B) + 2 inverse DGTs with the tensor
-    # product fused in + fused scale->Q + forward DGT(Q) (nphi <= 16384: one kernel per DGT)
-    launches_per_step = 7
+    # product fused in + complex scaling + B->Q + forward DGT(Q) (nphi <= 16384: one kernel per DGT)
+    launches_per_step = 8
 
     # ---- e2e: C ABI with pinned host buffers, copies inside the timed region ----
     hin = [torch.empty_like(x, device="cpu").pin_memory() for x in ins]

@@ -117,6 +117,16 @@ struct Engine {
     int qb_pm, bq_pm;              // mixed-radix weights prod_{l<i} s_l mod m_j, [target][i]
     int qq_w, bb_w;                // Garner weights of Q and of B, [i][l]
     int q_pinv, q_pinv_s, b_pinv, b_pinv_s;  // (prod_{j<i} s_j)^-1 mod s_i
+    // fast base conversion (FP64 overflow count, exact fallback): S = prod of the source base
+    int fq_hinv, fq_hinv_s;        // (Q/q_i)^-1 mod q_i, [i]
+    int fq_thinv, fq_thinv_s;      // t (Q/q_i)^-1 mod q_i, [i] (complex scaling)
+    int fq_hmod;                   // (Q/q_i) mod b_j, [j][i]
+    int fq_negv;                   // (-v Q) mod b_j, [j][v], v in [0, k]
+    int fq_invd;                   // 1/q_i as IEEE-754 double bits, [i]
+    int fb_hinv, fb_hinv_s;        // (B/b_j)^-1 mod b_j, [j]
+    int fb_hmod;                   // (B/b_j) mod q_i, [i][j]
+    int fb_negv;                   // (-v B) mod q_i, [i][v], v in [0, kl]
+    int fb_invd;                   // 1/b_j as double bits, [j]
     int pow64;                     // 2^(64 l) mod p_r, [residue][kMaxLimbs]
     int pow64m;                    // 2^(64 (l + 1)) mod p_r (Montgomery form of pow64), same shape
     // CKKS (only when ckks_prec != 0); every constant with its Shoup companion

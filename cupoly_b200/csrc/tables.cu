@@ -374,6 +374,49 @@ int build_tables(Engine& e) {
     e.ho.rho_q_s = append(c2);
   }
   {
+    // fast base conversion: S = prod(src); hat_i = S / s_i
+    auto fast = [&](const std::vector<uint64_t>& src, const std::vector<uint64_t>& dst, bool with_t, int& o_hinv,
+                    int& o_hinv_s, int* o_thinv, int* o_thinv_s, int& o_hmod, int& o_negv, int& o_invd) {
+      const size_t n = src.size();
+      std::vector<uint64_t> hinv, hinv_s, thinv, thinv_s, hmod, negv, invd;
+      for (size_t i = 0; i < n; ++i) {
+        uint64_t hat = 1 % src[i];
+        for (size_t l = 0; l < n; ++l)
+          if (l != i) hat = h_mulmod(hat, src[l] % src[i], src[i]);
+        const uint64_t hi = h_invmod(hat, src[i]);
+        push_pair(hi, src[i], hinv, hinv_s);
+        if (with_t) push_pair(h_mulmod(e.t % src[i], hi, src[i]), src[i], thinv, thinv_s);
+        const double d = 1.0 / (double)src[i];
+        uint64_t bits;
+        std::memcpy(&bits, &d, 8);
+        invd.push_back(bits);
+      }
+      for (size_t j = 0; j < dst.size(); ++j) {
+        const uint64_t m = dst[j];
+        for (size_t i = 0; i < n; ++i) {
+          uint64_t hat = 1 % m;
+          for (size_t l = 0; l < n; ++l)
+            if (l != i) hat = h_mulmod(hat, src[l] % m, m);
+          hmod.push_back(hat);
+        }
+        const uint64_t Sm = prod_mod(src, m);
+        for (size_t v = 0; v <= n; ++v) negv.push_back((m - h_mulmod(v % m, Sm, m)) % m);
+      }
+      o_hinv = append(hinv);
+      o_hinv_s = append(hinv_s);
+      if (with_t) {
+        *o_thinv = append(thinv);
+        *o_thinv_s = append(thinv_s);
+      }
+      o_hmod = append(hmod);
+      o_negv = append(negv);
+      o_invd = append(invd);
+    };
+    fast(Q, B, true, e.ho.fq_hinv, e.ho.fq_hinv_s, &e.ho.fq_thinv, &e.ho.fq_thinv_s, e.ho.fq_hmod, e.ho.fq_negv,
+         e.ho.fq_invd);
+    fast(B, Q, false, e.ho.fb_hinv, e.ho.fb_hinv_s, nullptr, nullptr, e.ho.fb_hmod, e.ho.fb_negv, e.ho.fb_invd);
+  }
+  {
     std::vector<uint64_t> v;  // 2^(64 l) mod p_r for the limb-to-residue conversion
     for (auto p : e.primes) {
       const uint64_t r1 = (uint64_t)(((unsigned __int128)1 << 64) % p);

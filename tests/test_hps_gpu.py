@@ -211,3 +211,46 @@ def test_bfv_mul_batch_vs_plain_and_oracle(gpu, k, nphi, npairs):
     ref = CO.bfv_mul(*rows, e.Q, e.B, 256)
     for j in range(3):
         assert np.array_equal(got[j * npairs:(j + 1) * npairs], ref[j])
+
+
+@pytest.mark.parametrize("k", [2, 5, 6, 7, 10, 12])
+def test_scaling_exact_fallback_edges(gpu, k):
+    """Coefficients where the FP64 overflow count is not trusted take the exact path:
+    t X mod Q near 0, near Q/2 (both sides) and near Q; X small (round(t X / Q) mod B
+    near 0, so the B -> Q step falls back too).  Complex scaling and the whole
+    scale-and-convert step (fused for |Q| <= 3, two kernels above) against the oracle."""
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine
+    t = 256
+    nphi = 64
+    e = Engine(k, 0, nphi, t)
+    Qp, Bp = O.prod(e.Q), O.prod(e.B)
+    ti = pow(t, -1, Qp)
+    xs = [0, 1, 2, 3, Qp - 1, Qp - 2, (Qp - 1) // 2, (Qp + 1) // 2]
+    for z in ((Qp - 1) // 2, (Qp + 1) // 2, (Qp - 3) // 2, (Qp + 3) // 2, 1, 2, Qp - 1, Qp - 2):
+        xs.append(z * ti % Qp)                      # t X == z (mod Q)
+    xs += [Qp * m + r for m in (0, 1, 5) for r in (0, 1)]   # X in [0, QB): small and multiples of Q
+    xs += random_poly_int(5, Qp * Bp, nphi - len(xs))
+    assert len(xs) == nphi and all(0 <= x < Qp * Bp for x in xs)
+    xq = np.array([[x % q for x in xs] for q in e.Q], dtype=np.uint64)
+    yb = np.array([[x % b for x in xs] for b in e.B], dtype=np.uint64)
+    out = e.empty(1)
+    e.complex_scaling(out, _dev(fold(xq)[None]), _dev(fold(yb)[None]))
+    cs = CO.complex_scaling(xq, yb, e.Q, e.B, t)
+    assert np.array_equal(unfold(_host(out))[0], cs)
+    for x, col in zip(xs[:24], cs.T[:24]):       # definition: round(t X / Q) mod b_j
+        assert [int(v) for v in col] == [((2 * t * x + Qp) // (2 * Qp)) % b for b in e.B]
+    # scale and convert to Q in one call (DGT domain in and out)
+    dq, db = _dev(fold(xq)[None]), _dev(fold(yb)[None])
+    e.dgt(dq, 0, FORWARD)
+    e.dgt(db, 1, FORWARD)
+    oq = e.empty(0)
+    e.poly_complex_scaling_tdivq(oq, dq, db)
+    e.dgt(oq, 0, INVERSE)
+    assert np.array_equal(unfold(_host(oq))[0], CO.basis_ext(cs, e.B, e.Q))
+    # basis extensions near the boundaries
+    o1 = e.empty(1)
+    e.basis_ext_q_to_b(o1, _dev(fold(xq)[None]))
+    assert np.array_equal(unfold(_host(o1))[0], CO.basis_ext(xq, e.Q, e.B))
+    o0 = e.empty(0)
+    e.basis_ext_b_to_q(o0, _dev(fold(yb)[None]))
+    assert np.array_equal(unfold(_host(o0))[0], CO.basis_ext(yb, e.B, e.Q))
