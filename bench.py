@@ -47,7 +47,6 @@ def parse():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=10000)
-    ap.add_argument("--serving-rate", type=float, default=5000.0)
     return ap.parse_args()
 
 
@@ -244,30 +243,30 @@ def run_ours(args, D: Dist):
     # product fused in + complex scaling + B->Q + forward DGT(Q) (nphi <= 16384: one kernel per DGT)
     launches_per_step = 8
 
-    # ---- e2e: C ABI with pinned host buffers, copies inside the timed region ----
-    hin = [torch.empty_like(x, device="cpu").pin_memory() for x in ins]
-    for h, x in zip(hin, ins):
-        h.copy_(x)
-    hout = torch.empty_like(c, device="cpu").pin_memory()
-    din = [torch.empty_like(x) for x in ins]
-
-    def e2e_step():
-        for d, h in zip(din, hin):
-            d.copy_(h, non_blocking=True)
-        e.bfv_mul_batch(c, *din, P, ws)
-        hout.copy_(c, non_blocking=True)
-
-    e2e_step()
+    # ---- e2e: host-resident batches through the public API (StreamedBFV: copy-in,
+    # chain and copy-out of consecutive batches overlap on three streams); every
+    # step's H2D of its inputs and D2H of its result is inside the timed region ----
+    from cupoly_b200.batch import StreamedBFV
+    hin = [[torch.empty_like(x, device="cpu").pin_memory() for x in ins] for _ in range(2)]
+    for hs in hin:
+        for h, x in zip(hs, ins):
+            h.copy_(x)
+    hout = [torch.empty_like(c, device="cpu").pin_memory() for _ in range(2)]
+    sb = StreamedBFV(e, P)
+    sb.run([hin[0], hin[1]], [hout[0], hout[1]])  # warm-up
+    sb.join(stream)
     torch.cuda.synchronize()
     D.barrier()
     ev0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
+    sb.s_in.wait_stream(stream)
+    sb.run([hin[i & 1] for i in range(args.steps)], [hout[i & 1] for i in range(args.steps)])
+    sb.join(stream)
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = D.max(ev0.elapsed_time(ev1))
-    h2d = sum(h.numel() * 8 for h in hin)
-    d2h = hout.numel() * 8
+    h2d = sum(h.numel() * 8 for h in hin[0])
+    d2h = hout[0].numel() * 8
+    del sb
 
     # ---- plain per-call form: one cp_bfv_mul per pair ----
     PP = min(args.plain_pairs, P)
@@ -478,11 +477,20 @@ def run_ours(args, D: Dist):
         from cupoly_b200 import serving as SV
         classes = SV.default_classes()
         ex = SV.GpuExecutor(classes)
+        n_req = args.serving_requests
+        # saturation: every request offered at once (closed loop)
         sch = SV.Scheduler(classes, ex, 40 << 30)
-        reqs = sch.run(SV.poisson_requests(args.serving_requests, args.serving_rate, len(classes), 1))
-        serving = sch.stats(reqs)
-        serving["rate_req_s"] = args.serving_rate
-        serving["classes"] = "nphi 4096/8192/16384/32768, k = nphi/2048, kl = k+1, t = 256, uniform mix"
+        sat = sch.stats(sch.run(SV.poisson_requests(n_req, 1e9, len(classes), 1)))["throughput_req_s"]
+        sweep = []
+        for frac in (0.25, 0.5, 0.75, 0.9, 1.0, 1.1):
+            sch = SV.Scheduler(classes, ex, 40 << 30)
+            st = sch.stats(sch.run(SV.poisson_requests(n_req, frac * sat, len(classes), 1)))
+            sweep.append({"offered_req_s": round(frac * sat, 1), "fraction_of_saturation": frac,
+                          "throughput_req_s": st["throughput_req_s"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                          "mean_batch": st["mean_batch"], "peak_budget_bytes": st["peak_budget_bytes"]})
+        serving = {"saturated_req_s": sat, "requests_per_rate": n_req, "budget_bytes": 40 << 30, "sweep": sweep,
+                   "arrivals": "open-loop Poisson, seeded",
+                   "classes": "nphi 4096/8192/16384/32768, k = nphi/2048, kl = k+1, t = 256, uniform mix"}
         del ex, sch
         torch.cuda.empty_cache()
 

@@ -282,14 +282,22 @@ class GpuExecutor:
 def main():
     ap = argparse.ArgumentParser(description="BFV serving loop: open-loop Poisson arrivals of mixed sizes")
     ap.add_argument("--requests", type=int, default=50000)
-    ap.add_argument("--rates", default="5000,10000,20000,40000")
+    ap.add_argument("--rates", default="auto",
+                    help="comma-separated req/s, or 'auto': fractions 0.25..1.1 of the measured saturation")
     ap.add_argument("--budget-gb", type=float, default=40.0)
     ap.add_argument("--seed", type=int, default=1)
     a = ap.parse_args()
     classes = default_classes()
     ex = GpuExecutor(classes)
     out = []
-    for rate in [float(x) for x in a.rates.split(",")]:
+    if a.rates == "auto":
+        sch = Scheduler(classes, ex, int(a.budget_gb * 2 ** 30))
+        sat = sch.stats(sch.run(poisson_requests(a.requests, 1e9, len(classes), a.seed)))["throughput_req_s"]
+        print(json.dumps({"saturated_req_s": sat}), flush=True)
+        rates = [f * sat for f in (0.25, 0.5, 0.75, 0.9, 1.0, 1.1)]
+    else:
+        rates = [float(x) for x in a.rates.split(",")]
+    for rate in rates:
         sch = Scheduler(classes, ex, int(a.budget_gb * 2 ** 30))
         reqs = sch.run(poisson_requests(a.requests, rate, len(classes), a.seed))
         st = sch.stats(reqs)
