@@ -34,7 +34,36 @@ struct PassCfg {
   static constexpr int W0 = LOGNC - (NP - 1) * LOGR;
   __host__ __device__ static constexpr int width(int i) { return i == 0 ? W0 : LOGR; }
   __host__ __device__ static constexpr int field(int i) { return LOGNC - W0 - i * LOGR; }
+  // Passes i >= 1 whose twiddle table (2^(field + LOGR) entries, each read by
+  // 2^LOGR - 1 threads of the CTA) is at most 1024 entries are staged in
+  // shared memory once per CTA; the first pass reads each entry once and
+  // streams it from global memory.
+  __host__ __device__ static constexpr bool staged(int i) {
+    return i >= 1 && i < NP && field(i) > 0 && field(i) + LOGR <= 10;
+  }
+  __host__ __device__ static constexpr int soff(int i) {  // entries before pass i's staged table
+    int o = 0;
+    for (int q = 1; q < i; ++q)
+      if (staged(q)) o += 1 << (field(q) + LOGR);
+    return o;
+  }
+  __host__ __device__ static constexpr int stotal() { return soff(NP); }
 };
+
+// Copy the staged twiddle tables of the passes (offsets `off` into the residue's
+// table block) into shared memory.
+template <int LOGNC, int LOGR>
+__device__ __forceinline__ void stage_twiddles(ulonglong2* stw, const ulonglong2* tab, const int* off) {
+  using C = PassCfg<LOGNC, LOGR>;
+  constexpr int T = (1 << LOGNC) >> LOGR;
+#pragma unroll
+  for (int i = 1; i < C::NP; ++i)
+    if (C::staged(i)) {
+      const ulonglong2* src = tab + off[i];
+      ulonglong2* dst = stw + C::soff(i);
+      for (int j = threadIdx.x; j < (1 << (C::field(i) + LOGR)); j += T) dst[j] = __ldg(src + j);
+    }
+}
 
 // In-register 2^W-point Gentleman-Sande DIF (natural in, bit-reversed out).
 // rad[j] = w_R^j, R = 2^LOGR; the 2^W-point root is w_R^(2^(LOGR-W)).
@@ -106,8 +135,8 @@ __device__ __forceinline__ void gi_mul_const3(uint64_t& xr, uint64_t& xi, const 
 
 // One middle/late forward pass (I >= 1), full radix 2^LOGR, data in smem.
 template <int LOGNC, int LOGR, int I>
-__device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* tab,
-                                           const DgtTableLayout& L, uint64_t p) {
+__device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* stw,
+                                           const ulonglong2* tab, const DgtTableLayout& L, uint64_t p) {
   using C = PassCfg<LOGNC, LOGR>;
   if constexpr (I < C::NP) {
     constexpr int PF = C::field(I);
@@ -124,10 +153,10 @@ __device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* s
     }
     dif_regs<LOGR, LOGR>(xr, xi, srad, p);
     if constexpr (PF > 0) {
-      const ulonglong2* tw = tab + L.off_fwd[I] + Lw;
+      const ulonglong2* tw = C::staged(I) ? stw + C::soff(I) + Lw : tab + L.off_fwd[I] + Lw;
 #pragma unroll
       for (int v = 1; v < R; ++v) {
-        const ulonglong2 w = __ldg(tw + (v << PF));
+        const ulonglong2 w = C::staged(I) ? tw[v << PF] : __ldg(tw + (v << PF));
         xr[v] = shoup_mul(xr[v], w.x, w.y, p);
         xi[v] = shoup_mul(xi[v], w.x, w.y, p);
       }
@@ -135,13 +164,13 @@ __device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* s
 #pragma unroll
     for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
     __syncthreads();
-    fwd_passes<LOGNC, LOGR, I + 1>(sdat, srad, tab, L, p);
+    fwd_passes<LOGNC, LOGR, I + 1>(sdat, srad, stw, tab, L, p);
   }
 }
 
 template <int LOGNC, int LOGR, int I>
-__device__ __forceinline__ void inv_passes(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* tab,
-                                           const DgtTableLayout& L, uint64_t p) {
+__device__ __forceinline__ void inv_passes(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* stw,
+                                           const ulonglong2* tab, const DgtTableLayout& L, uint64_t p) {
   using C = PassCfg<LOGNC, LOGR>;
   if constexpr (I >= 1) {
     constexpr int PF = C::field(I);
@@ -157,10 +186,10 @@ __device__ __forceinline__ void inv_passes(ulonglong2* sdat, const ulonglong2* s
       xi[v] = a.y;
     }
     if constexpr (PF > 0) {
-      const ulonglong2* tw = tab + L.off_inv[I] + Lw;
+      const ulonglong2* tw = C::staged(I) ? stw + C::soff(I) + Lw : tab + L.off_inv[I] + Lw;
 #pragma unroll
       for (int v = 1; v < R; ++v) {
-        const ulonglong2 w = __ldg(tw + (v << PF));
+        const ulonglong2 w = C::staged(I) ? tw[v << PF] : __ldg(tw + (v << PF));
         xr[v] = shoup_mul(xr[v], w.x, w.y, p);
         xi[v] = shoup_mul(xi[v], w.x, w.y, p);
       }
@@ -169,14 +198,14 @@ __device__ __forceinline__ void inv_passes(ulonglong2* sdat, const ulonglong2* s
 #pragma unroll
     for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
     __syncthreads();
-    inv_passes<LOGNC, LOGR, I - 1>(sdat, srad, tab, L, p);
+    inv_passes<LOGNC, LOGR, I - 1>(sdat, srad, stw, tab, L, p);
   }
 }
 
 // Shared-memory bytes of one CTA.
 template <int LOGNC, int LOGR>
 constexpr int dgt_smem_bytes() {
-  return ((1 << LOGNC) + ((1 << LOGNC) >> 4) + (1 << LOGR)) * 16;
+  return ((1 << LOGNC) + ((1 << LOGNC) >> 4) + (1 << LOGR) + PassCfg<LOGNC, LOGR>::stotal()) * 16;
 }
 
 // Forward transform of 2^LOGNC elements per CTA, in place.
@@ -201,6 +230,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   extern __shared__ ulonglong2 smem[];
   ulonglong2* sdat = smem;
   ulonglong2* srad = smem + NC + (NC >> 4);
+  ulonglong2* stw = srad + R;
   const int tid = threadIdx.x;
   const int h = blockIdx.x & ((1 << S) - 1);
   const int pr = blockIdx.x >> S;
@@ -213,6 +243,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   ulonglong2* x = data + off;
   const ulonglong2* xs = (src_base ? src_base : data) + off;  // out of place when src_base is set
   for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
+  stage_twiddles<LOGNC, LOGR>(stw, tab, A.L.off_fwd);
   __syncthreads();
   {
     constexpr int W = C::W0, PF = LOGNC - C::W0, G = 1 << (LOGR - C::W0);
@@ -245,7 +276,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
     }
     __syncthreads();
   }
-  fwd_passes<LOGNC, LOGR, 1>(sdat, srad, tab, A.L, p);
+  fwd_passes<LOGNC, LOGR, 1>(sdat, srad, stw, tab, A.L, p);
 #pragma unroll
   for (int j = 0; j < R; ++j) {
     const int idx = tid + j * T;
@@ -284,6 +315,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   extern __shared__ ulonglong2 smem[];
   ulonglong2* sdat = smem;
   ulonglong2* srad = smem + NC + (NC >> 4);
+  ulonglong2* stw = srad + R;
   const int tid = threadIdx.x;
   const int h = blockIdx.x & ((1 << S) - 1);
   const int pr = blockIdx.x >> S;
@@ -302,6 +334,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   const size_t inner = ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
   ulonglong2* x = data + poly * poly_stride + inner;
   for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
+  stage_twiddles<LOGNC, LOGR>(stw, tab, A.L.off_inv);
   if (src.mode != 1) {
     const ulonglong2* xs = src.mode == 0
                                ? src.p[0] + poly * poly_stride + inner
@@ -322,7 +355,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
     }
   }
   __syncthreads();
-  inv_passes<LOGNC, LOGR, C::NP - 1>(sdat, srad, tab, A.L, p);
+  inv_passes<LOGNC, LOGR, C::NP - 1>(sdat, srad, stw, tab, A.L, p);
   {
     constexpr int W = C::W0, PF = LOGNC - C::W0, G = 1 << (LOGR - C::W0);
     uint64_t xr[1 << W], xi[1 << W];
