@@ -8,6 +8,26 @@ namespace cpoly {
 
 namespace {
 
+// Grid of a DGT launch.  When only one CTA fits per SM (N = 8192 in one CTA)
+// the grid is persistent -- one CTA per SM striding over the units, each
+// prefetching its next unit into L2 -- which measured 3-8 % faster on B200;
+// with two or more resident CTAs per SM one CTA per unit is faster (the
+// hardware balances the tail), so the grid is the unit count.
+template <typename K>
+unsigned persistent_grid(K kernel, int threads, int smem, std::atomic<int>& resident, long long units) {
+  int per_device = resident.load();
+  if (per_device == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    per_device = per_sm == 1 ? (sms > 0 ? sms : 1) : -1;
+    resident.store(per_device);
+  }
+  if (per_device < 0) return (unsigned)units;
+  return (unsigned)(units < per_device ? units : per_device);
+}
+
 template <int LOGNC, int LOGR>
 int run_cta(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres, int rid_off,
             int npolys, long long poly_stride, bool inverse, bool twist, cudaStream_t st, const int* rid_list) {
@@ -23,14 +43,18 @@ int run_cta(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const Inv
   }
   if (!inverse) {
     static std::atomic<unsigned long long> done{0};
+    static std::atomic<int> resident{0};
     if (int rc = ensure_smem(k_dgt_fwd<LOGNC, LOGR>, smem, done)) return rc;
-    k_dgt_fwd<LOGNC, LOGR><<<(unsigned)blocks, T, smem, st>>>(data, fsrc, A, nres, rid_off, poly_stride, S,
-                                                              twist ? 1 : 0);
+    const unsigned grid = persistent_grid(k_dgt_fwd<LOGNC, LOGR>, T, smem, resident, blocks);
+    k_dgt_fwd<LOGNC, LOGR><<<grid, T, smem, st>>>(data, fsrc, A, nres, rid_off, poly_stride, S, twist ? 1 : 0,
+                                                  (unsigned)blocks);
   } else {
     static std::atomic<unsigned long long> done{0};
+    static std::atomic<int> resident{0};
     if (int rc = ensure_smem(k_dgt_inv<LOGNC, LOGR>, smem, done)) return rc;
-    k_dgt_inv<LOGNC, LOGR><<<(unsigned)blocks, T, smem, st>>>(data, isrc, A, nres, rid_off, poly_stride, S,
-                                                              twist ? 1 : 0);
+    const unsigned grid = persistent_grid(k_dgt_inv<LOGNC, LOGR>, T, smem, resident, blocks);
+    k_dgt_inv<LOGNC, LOGR><<<grid, T, smem, st>>>(data, isrc, A, nres, rid_off, poly_stride, S, twist ? 1 : 0,
+                                                  (unsigned)blocks);
   }
   return check_launch("dgt");
 }

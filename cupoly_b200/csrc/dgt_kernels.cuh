@@ -133,6 +133,16 @@ __device__ __forceinline__ void gi_mul_const3(uint64_t& xr, uint64_t& xi, const 
   xi = add_mod(k1, k2, p);
 }
 
+// Bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) into L2 through the
+// TMA unit; a hint only, nothing waits on it.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  for (uint32_t o = 0; o < bytes; o += 32768u) {
+    const uint32_t n = bytes - o < 32768u ? bytes - o : 32768u;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<const char*>(p) + o), "r"(n)
+                 : "memory");
+  }
+}
+
 // One middle/late forward pass (I >= 1), full radix 2^LOGR, data in smem.
 template <int LOGNC, int LOGR, int I>
 __device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* stw,
@@ -224,7 +234,7 @@ constexpr int dgt_min_blocks() {
 template <int LOGNC, int LOGR>
 __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
     k_dgt_fwd(ulonglong2* __restrict__ data, const ulonglong2* __restrict__ src_base, DgtArgs A, int nres,
-              int rid_off, long long poly_stride, int S, int twist) {
+              int rid_off, long long poly_stride, int S, int twist, unsigned nunits) {
   constexpr int NC = 1 << LOGNC, R = 1 << LOGR, T = NC >> LOGR;
   using C = PassCfg<LOGNC, LOGR>;
   extern __shared__ ulonglong2 smem[];
@@ -232,16 +242,24 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   ulonglong2* srad = smem + NC + (NC >> 4);
   ulonglong2* stw = srad + R;
   const int tid = threadIdx.x;
-  const int h = blockIdx.x & ((1 << S) - 1);
-  const int pr = blockIdx.x >> S;
+  // Persistent CTAs: unit ub = (poly * nres + r) * 2^S + h, strided by the grid; each
+  // iteration prefetches the next unit's input into L2 while this one is transformed.
+  const ulonglong2* in_base = src_base ? src_base : data;  // out of place when src_base is set
+  auto unit_off = [&](unsigned ub) {
+    const int pr_ = (int)(ub >> S);
+    return (size_t)(pr_ / nres) * poly_stride + ((size_t)(pr_ % nres) << (LOGNC + S)) +
+           ((size_t)(ub & ((1u << S) - 1)) << LOGNC);
+  };
+  for (unsigned ub = blockIdx.x; ub < nunits; ub += gridDim.x) {
+  if (tid == 0 && ub + gridDim.x < nunits) prefetch_l2(in_base + unit_off(ub + gridDim.x), NC * 16u);
+  const int pr = (int)(ub >> S);
   const int r = pr % nres;
-  const int poly = pr / nres;
   const int rid = A.rid_list ? A.rid_list[pr] : rid_off + r;
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
-  const size_t off = poly * poly_stride + ((size_t)r << (LOGNC + S)) + ((size_t)h << LOGNC);
+  const size_t off = unit_off(ub);
   ulonglong2* x = data + off;
-  const ulonglong2* xs = (src_base ? src_base : data) + off;  // out of place when src_base is set
+  const ulonglong2* xs = in_base + off;
   for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
   stage_twiddles<LOGNC, LOGR>(stw, tab, A.L.off_fwd);
   __syncthreads();
@@ -282,6 +300,8 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
     const int idx = tid + j * T;
     x[idx] = sdat[pad16(idx)];
   }
+  __syncthreads();  // shared memory is rewritten by the next unit
+  }
 }
 
 __device__ __forceinline__ ulonglong2 tensor_load(const InvSrc& s, int j, size_t off, const ModConst& m) {
@@ -309,7 +329,7 @@ __device__ __forceinline__ ulonglong2 tensor_load(const InvSrc& s, int j, size_t
 template <int LOGNC, int LOGR>
 __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
     k_dgt_inv(ulonglong2* __restrict__ data, InvSrc src, DgtArgs A, int nres, int rid_off, long long poly_stride,
-              int S, int untwist) {
+              int S, int untwist, unsigned nunits) {
   constexpr int NC = 1 << LOGNC, R = 1 << LOGR, T = NC >> LOGR;
   using C = PassCfg<LOGNC, LOGR>;
   extern __shared__ ulonglong2 smem[];
@@ -317,17 +337,40 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   ulonglong2* srad = smem + NC + (NC >> 4);
   ulonglong2* stw = srad + R;
   const int tid = threadIdx.x;
-  const int h = blockIdx.x & ((1 << S) - 1);
-  const int pr = blockIdx.x >> S;
-  int r, poly;
-  if (src.mode == 1) {  // c0, c1, c2 of one (pair, residue) in adjacent CTAs
-    const int rest = pr / 3;
-    r = rest % nres;
-    poly = (pr % 3) * src.npairs + rest / nres;
-  } else {
-    r = pr % nres;
-    poly = pr / nres;
+  // Persistent CTAs over units ub = (poly-or-output * nres + r) * 2^S + h (see k_dgt_fwd).
+  auto coords = [&](unsigned ub, int& r_, int& poly_) {
+    const int pr_ = (int)(ub >> S);
+    if (src.mode == 1) {  // c0, c1, c2 of one (pair, residue) in adjacent units
+      const int rest = pr_ / 3;
+      r_ = rest % nres;
+      poly_ = (pr_ % 3) * src.npairs + rest / nres;
+    } else {
+      r_ = pr_ % nres;
+      poly_ = pr_ / nres;
+    }
+  };
+  for (unsigned ub = blockIdx.x; ub < nunits; ub += gridDim.x) {
+  if (tid == 0 && ub + gridDim.x < nunits) {  // the next unit's operands into L2
+    int rn, pn;
+    coords(ub + gridDim.x, rn, pn);
+    const size_t inner_n = ((size_t)rn << (LOGNC + S)) + ((size_t)((ub + gridDim.x) & ((1u << S) - 1)) << LOGNC);
+    if (src.mode == 0) {
+      prefetch_l2(src.p[0] + pn * poly_stride + inner_n, NC * 16u);
+    } else if (src.mode == 2) {
+      prefetch_l2(src.p[pn / src.npairs] + (pn % src.npairs) * poly_stride + inner_n, NC * 16u);
+    } else {
+      const int jt = pn / src.npairs;
+      const size_t bo = (size_t)(pn % src.npairs) * poly_stride + inner_n;
+      if (jt != 2) prefetch_l2(src.p[0] + bo, NC * 16u);
+      if (jt != 0) prefetch_l2(src.p[1] + bo, NC * 16u);
+      if (jt != 2) prefetch_l2(src.p[3] + bo, NC * 16u);
+      if (jt != 0) prefetch_l2(src.p[2] + bo, NC * 16u);
+    }
   }
+  const int h = (int)(ub & ((1u << S) - 1));
+  const int pr = (int)(ub >> S);
+  int r, poly;
+  coords(ub, r, poly);
   const int rid = A.rid_list ? A.rid_list[pr] : rid_off + r;
   const uint64_t p = A.mc[rid].p;
   const ulonglong2* tab = A.tab + (size_t)rid * A.stride;
@@ -386,6 +429,8 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
         x[idx] = make_ulonglong2(ar, ai);
       }
     }
+  }
+  __syncthreads();  // shared memory is rewritten by the next unit
   }
 }
 
