@@ -1,18 +1,22 @@
-"""Autotuner for the DGT register radix.
+"""Autotuner for the DGT plan: register radix and stage split.
 
-The in-CTA transform runs radix-2^r register passes, r in {2, 3, 4}; the best
-r depends on the transform size (registers, passes, shared-memory traffic).
-`best_log_radix(nphi)` times forward + inverse transforms of a batch for each
-candidate on the current GPU and caches the winner in a JSON file keyed by GPU
-name and nphi (the RNS width only scales the batch, so it does not change the
-choice).  Engines created with log_radix=0 from Python use the cached choice
-when one exists and the library default (radix 8) otherwise.
+The in-CTA transform runs radix-2^r register passes, r in {2, 3, 4}, over the
+largest power of two kept whole in one CTA, 2^c (c <= 13); for N = nphi / 2
+larger than 2^c the top log2(N) - c (at most 2) bits run in an element-wise
+split stage.  Which (r, c) is fastest depends on the GPU and the size (register
+pressure, passes, shared memory per CTA and hence CTAs per SM, the extra HBM
+pass of the split).  `best_plan(nphi)` times a forward + inverse transform of a
+batch for every candidate on the current GPU and caches the winner in a JSON
+file keyed by GPU name and nphi (the RNS width only scales the batch, so it
+does not change the choice).  Engines created with log_radix = 0 from Python
+use the cached plan when one exists and the library default (radix 8, c = 13)
+otherwise.
 """
 from __future__ import annotations
 
 import json
 import os
-from typing import Dict
+from typing import Dict, List, Tuple
 
 _DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "autotune.json")
 
@@ -39,29 +43,40 @@ def _key(nphi: int) -> str:
     return "%s|nphi=%d" % (_gpu_name(), nphi)
 
 
-def cached_log_radix(nphi: int) -> int:
-    """Cached choice for this GPU and nphi, or 0 when none is cached."""
+def cached_plan(nphi: int) -> Tuple[int, int]:
+    """Cached (log_radix, log_cta) for this GPU and nphi, or (0, 0) when none is cached."""
     try:
-        return int(_load().get(_key(nphi), {}).get("log_radix", 0))
+        ent = _load().get(_key(nphi), {})
+        return int(ent.get("log_radix", 0)), int(ent.get("log_cta", 0))
     except Exception:
-        return 0
+        return 0, 0
 
 
-def candidates(nphi: int):
+def cached_log_radix(nphi: int) -> int:
+    return cached_plan(nphi)[0]
+
+
+def candidates(nphi: int) -> List[Tuple[int, int]]:
+    """(log_radix, log_cta) pairs the library compiles for this size."""
     logn = max(1, (nphi // 2).bit_length() - 1)
-    lognc = min(logn, 13)
     out = []
-    for r in (2, 3, 4):
-        eff = min(r, lognc)
-        while lognc - eff > 10:  # at most 1024 threads per CTA
-            eff += 1
-        if eff not in out:
-            out.append(eff)
+    for c in (13, 12, 11):
+        if c >= logn and c != 13:
+            continue  # a cap at or above the size changes nothing: only the default is timed
+        lognc = min(logn, c)
+        if logn - lognc > 2 or (logn > lognc and lognc < 8):
+            continue  # the split stage handles at most 2 bits, of at least 256-element blocks
+        for r in (2, 3, 4):
+            eff = min(r, lognc)
+            while lognc - eff > 10:  # at most 1024 threads per CTA
+                eff += 1
+            if (eff, c) not in out:
+                out.append((eff, c))
     return out
 
 
-def best_log_radix(nphi: int, residues: int = 2048, reps: int = 5, save: bool = True) -> int:
-    """Time every candidate radix at this nphi and return (and cache) the fastest."""
+def best_plan(nphi: int, residues: int = 2048, reps: int = 5, save: bool = True) -> Tuple[int, int]:
+    """Time every candidate plan at this nphi and return (and cache) the fastest."""
     import torch
 
     from .engine import FORWARD, INVERSE, UNIFORM, Engine
@@ -69,8 +84,9 @@ def best_log_radix(nphi: int, residues: int = 2048, reps: int = 5, save: bool = 
     key = _key(nphi)
     results = {}
     npolys = max(1, residues // 2)
-    for r in candidates(nphi):
+    for r, c in candidates(nphi):
         e = Engine(2, 1, nphi, 256, r)
+        e.set_plan(r, c)
         x = e.empty(0, npolys)
         e.sample(x, 0, UNIFORM, 1, 0, npolys=npolys, to_dgt=False)
         e.dgt(x, 0, FORWARD)
@@ -83,14 +99,30 @@ def best_log_radix(nphi: int, residues: int = 2048, reps: int = 5, save: bool = 
             e.dgt(x, 0, INVERSE)
         b.record()
         torch.cuda.synchronize()
-        results[r] = a.elapsed_time(b) / reps
+        results[(r, c)] = a.elapsed_time(b) / reps
         del e, x
     best = min(results, key=results.get)
     if save:
         data = _load()
-        data[key] = {"log_radix": best, "ms_fwd_inv": {str(k): round(v, 4) for k, v in results.items()},
+        data[key] = {"log_radix": best[0], "log_cta": best[1],
+                     "ms_fwd_inv": {"r%d_c%d" % k: round(v, 4) for k, v in results.items()},
                      "residues": 2 * npolys}
         os.makedirs(os.path.dirname(cache_path()), exist_ok=True)
         with open(cache_path(), "w") as f:
             json.dump(data, f, indent=1, sort_keys=True)
     return best
+
+
+def best_log_radix(nphi: int, **kw) -> int:
+    return best_plan(nphi, **kw)[0]
+
+
+if __name__ == "__main__":
+    import argparse
+
+    ap = argparse.ArgumentParser(description="tune the DGT plan for the current GPU")
+    ap.add_argument("--nphi", default="2048,4096,8192,16384,32768,65536")
+    a = ap.parse_args()
+    for n in [int(x) for x in a.nphi.split(",")]:
+        print(json.dumps({"nphi": n, "plan": best_plan(n)}), flush=True)
+    print(json.dumps(_load(), indent=1))

@@ -36,11 +36,14 @@ class MixedPolymul:
         self.where = {}  # instance -> (nphi, first residue row)
         for nphi, g in self.groups.items():
             lr = 0
+            lc = 0
             if autotune:
-                from .autotune import best_log_radix
+                from .autotune import best_plan
 
-                lr = best_log_radix(nphi)
+                lr, lc = best_plan(nphi)
             g["engine"] = Engine(kmax, 1, nphi, 256, lr)
+            if lc:
+                g["engine"].set_plan(lr, lc)
             rids, row = [], 0
             for i in g["inst"]:
                 k = self.specs[i][1]

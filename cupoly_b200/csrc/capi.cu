@@ -172,6 +172,27 @@ int cp_ckks_engine_create(cp_engine** out, int k, int kl, int nphi, int prec, in
 
 int cp_engine_ckks_prec(const cp_engine* h) { return h ? h->e.ckks_prec : -1; }
 
+int cp_engine_set_plan(cp_engine* h, int log_radix, int log_cta) {
+  CP_REQUIRE(h, "cp_engine_set_plan: NULL engine");
+  CP_REQUIRE(log_radix == 0 || (log_radix >= 2 && log_radix <= 4), "cp_engine_set_plan: log_radix must be 0, 2, 3 or 4");
+  Engine& e = h->e;
+  const int lc = log_cta ? log_cta : kMaxLogNc;
+  CP_REQUIRE(lc >= 8 && lc <= kMaxLogNc, "cp_engine_set_plan: log_cta must be 0 or in [8, 13]");
+  CP_REQUIRE(e.logN - (e.logN < lc ? e.logN : lc) <= 2, "cp_engine_set_plan: at most 2 split bits (log N - log_cta)");
+  cudaDeviceSynchronize();
+  free_tables(e);
+  e.plan = make_plan(e.logN, log_radix ? log_radix : 3, lc);
+  return build_tables(e);
+}
+
+int cp_engine_get_plan(const cp_engine* h, int* log_radix, int* log_cta, int* split_bits) {
+  CP_REQUIRE(h, "cp_engine_get_plan: NULL engine");
+  if (log_radix) *log_radix = h->e.plan.logR;
+  if (log_cta) *log_cta = h->e.plan.logNc;
+  if (split_bits) *split_bits = h->e.plan.S;
+  return CP_OK;
+}
+
 int cp_engine_destroy(cp_engine* h) {
   if (!h) return CP_OK;
   cudaDeviceSynchronize();

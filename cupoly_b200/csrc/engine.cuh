@@ -34,7 +34,9 @@ struct DgtPlan {
   int p[kMaxPasses] = {0};
 };
 
-DgtPlan make_plan(int logN, int logR);
+// logCta caps the size kept whole in one CTA (0: kMaxLogNc); the rest of the
+// transform (at most 2 bits) runs in the element-wise split stage.
+DgtPlan make_plan(int logN, int logR, int logCta = 0);
 
 // Offsets (in 16-byte entries) inside one residue's table block.
 struct DgtTableLayout {

@@ -125,10 +125,11 @@ int Engine::n_residues(int base) const {
 }
 int Engine::rid_offset(int base) const { return base == 1 ? k : 0; }
 
-DgtPlan make_plan(int logN, int logR) {
+DgtPlan make_plan(int logN, int logR, int logCta) {
   DgtPlan P;
   P.logN = logN;
-  P.logNc = logN < kMaxLogNc ? logN : kMaxLogNc;
+  if (logCta <= 0 || logCta > kMaxLogNc) logCta = kMaxLogNc;
+  P.logNc = logN < logCta ? logN : logCta;
   P.S = logN - P.logNc;
   P.logR = logR < P.logNc ? logR : P.logNc;
   while ((P.logNc - P.logR) > 10) ++P.logR;  // at most 1024 threads per CTA

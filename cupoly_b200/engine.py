@@ -100,10 +100,11 @@ class Engine:
         if not torch.cuda.is_available():
             raise RuntimeError("cupoly_b200 needs a CUDA device")
         _lib.lib()
-        if log_radix == 0:  # use the autotuner's choice for this GPU and size when one is cached
-            from .autotune import cached_log_radix
+        log_cta = 0
+        if log_radix == 0:  # use the autotuner's plan for this GPU and size when one is cached
+            from .autotune import cached_plan
 
-            log_radix = cached_log_radix(nphi)
+            log_radix, log_cta = cached_plan(nphi)
         h = C.c_void_p()
         if ckks_prec:
             call("cp_ckks_engine_create", C.byref(h), k, kl, nphi, ckks_prec, log_radix)
@@ -111,6 +112,8 @@ class Engine:
         else:
             call("cp_engine_create", C.byref(h), k, kl, nphi, t, log_radix)
         self.ckks_prec = ckks_prec
+        if log_cta:
+            call("cp_engine_set_plan", h, log_radix, log_cta)
         self.log_radix = log_radix
         self._h = h
         self.k = k
@@ -124,6 +127,17 @@ class Engine:
         self.Q = self.primes[: self.k]
         self.B = self.primes[self.k:]
         self._ws: Optional[torch.Tensor] = None
+
+    # ---- DGT plan ----
+    def set_plan(self, log_radix: int, log_cta: int = 0):
+        """Register radix 2^log_radix and in-CTA size 2^log_cta (0: 2^13); rebuilds the tables."""
+        call("cp_engine_set_plan", self._h, log_radix, log_cta)
+        self.log_radix = log_radix
+
+    def get_plan(self):
+        r, c, s = C.c_int(), C.c_int(), C.c_int()
+        call("cp_engine_get_plan", self._h, C.byref(r), C.byref(c), C.byref(s))
+        return {"log_radix": r.value, "log_cta": c.value, "split_bits": s.value}
 
     # ---- lifecycle ----
     def close(self):

@@ -79,6 +79,13 @@ int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int l
 int cp_ckks_engine_create(cp_engine** out, int k, int kl, int nphi, int prec, int log_radix);
 /* precision bucket of a CKKS engine, 0 for a BFV engine */
 int cp_engine_ckks_prec(const cp_engine* e);
+/* DGT plan (no counterpart in cuPoly, whose split is fixed per size, include/cuPoly/cuda/dgt.h:41-50):
+ * register radix 2^log_radix and the largest size kept whole in one CTA, 2^log_cta
+ * (0 = 2^13); the remaining log2(N) - log_cta <= 2 bits run in an element-wise split
+ * stage.  Rebuilds the engine's tables (synchronises the device).  The autotuner
+ * (cupoly_b200/autotune.py) measures the candidates and caches the fastest. */
+int cp_engine_set_plan(cp_engine* e, int log_radix, int log_cta);
+int cp_engine_get_plan(const cp_engine* e, int* log_radix, int* log_cta, int* split_bits);
 int cp_engine_destroy(cp_engine* e);
 int cp_engine_n_residues(const cp_engine* e, int base);
 int cp_engine_nphi(const cp_engine* e);

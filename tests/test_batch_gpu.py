@@ -78,11 +78,38 @@ def test_autotuner_picks_a_candidate_and_caches(gpu, tmp_path, monkeypatch):
     import json
     monkeypatch.setenv("CUPOLY_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     from cupoly_b200 import autotune
-    r = autotune.best_log_radix(4096, residues=256, reps=2)
-    assert r in autotune.candidates(4096)
-    assert autotune.cached_log_radix(4096) == r
+    from cupoly_b200.engine import Engine
+    cands = autotune.candidates(16384)
+    assert (3, 13) in cands and (3, 12) in cands           # radix and stage-split choices
+    plan = autotune.best_plan(16384, residues=128, reps=2)
+    assert plan in cands
+    assert autotune.cached_plan(16384) == plan
     data = json.load(open(tmp_path / "tune.json"))
-    assert len(next(iter(data.values()))["ms_fwd_inv"]) == len(autotune.candidates(4096))
+    assert len(next(iter(data.values()))["ms_fwd_inv"]) == len(cands)
+    e = Engine(2, 0, 16384, 256)                           # picks the cached plan up
+    assert (e.get_plan()["log_radix"], e.get_plan()["log_cta"]) == plan
+
+
+@pytest.mark.parametrize("nphi,plans", [(16384, [(3, 13), (3, 12), (4, 12), (2, 11)]),
+                                        (32768, [(3, 13), (4, 13)]), (8192, [(3, 12), (3, 11), (4, 11)])])
+def test_every_plan_gives_the_same_transform(gpu, nphi, plans):
+    """Radix and stage split change the schedule, never the result: DGT-domain bytes and
+    the round trip agree across plans (and with the oracle's restatement)."""
+    import numpy as np
+
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine, from_u64, to_u64
+    from oracle import coracle
+    from tests.common import fold, random_poly_residues
+    e = Engine(2, 0, nphi, 256)
+    x = random_poly_residues(nphi, e.Q, nphi)
+    ref = coracle.dgt(fold(x)[None], e.Q)
+    for r, c in plans:
+        e.set_plan(r, c)
+        d = from_u64(fold(x)[None])
+        e.dgt(d, 0, FORWARD)
+        assert np.array_equal(to_u64(d), ref), (r, c, e.get_plan())
+        e.dgt(d, 0, INVERSE)
+        assert np.array_equal(to_u64(d)[0], fold(x)), (r, c)
 
 
 def test_streamed_bfv_matches_device_batches(gpu):
