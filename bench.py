@@ -25,7 +25,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -38,7 +37,7 @@ WORKLOAD = "BFV homomorphic-multiply kernel chain (nphi=8192, k=5, kl=6, t=256)"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--pairs", type=int, default=128, help="ciphertext pairs per step (batched form)")
@@ -95,6 +94,9 @@ class Dist:
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class Clocks:
+    """`nvidia-smi -lms 50` logging the GPU's clocks and throttle reasons for the
+    duration of a `with` block (the timed region)."""
+
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -102,29 +104,29 @@ class Clocks:
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.samples = []
-        self._stop = threading.Event()
-        self._th = None
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self._proc = None
 
     def __enter__(self):
-        self._th = threading.Thread(target=self._run, daemon=True)
-        self._th.start()
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                           "--format=csv,noheader,nounits", "-lms", "50"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.3)  # the first sample lands before the timed work starts
+        except OSError:
+            self._proc = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._th.join(timeout=10)
+        if self._proc is None:
+            return
+        time.sleep(0.1)
+        self._proc.terminate()
+        try:
+            out, _ = self._proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self._proc.kill()
+            out, _ = self._proc.communicate()
+        self.samples = [[x.strip() for x in ln.split(",")] for ln in out.splitlines() if ln.count(",") >= 8]
 
     def summary(self):
         if not self.samples:
