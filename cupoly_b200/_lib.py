@@ -57,6 +57,9 @@ SIGNATURES = {
     "cp_dgt": (_i, [_vp, _vp, _i, _i, _i, _i64, _vp]),
     "cp_dgt_list": (_i, [_vp, _vp, _vp, _i, _i, _vp]),
     "cp_mul_list": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp]),
+    "cp_polymul_workspace_bytes": (C.c_size_t, [_vp, _i, _i]),
+    "cp_polymul": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),
+    "cp_polymul_list": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "cp_add": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
     "cp_sub": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
     "cp_double_add": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),

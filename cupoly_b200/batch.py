@@ -4,10 +4,10 @@
 Z_q[x]/(x^nphi_i + 1) with per-instance ring size nphi_i and RNS width k_i.
 Instances are grouped by ring size; inside a group every residue of every
 instance is one entry of a work list (data pointer implied by its position,
-prime index = its residue number), so one forward DGT launch per operand, one
-pointwise launch and one inverse launch serve the whole group whatever the mix
-of widths.  All groups' launches are captured once in a CUDA graph and
-replayed.
+prime index = its residue number), and one fused `cp_polymul_list` serves the
+whole group whatever the mix of widths: an out-of-place forward DGT per
+operand and an inverse DGT that forms the products while loading.  All
+groups' launches are captured once in a CUDA graph and replayed.
 
 `BFVBatch`: the fused BFV multiplication chain over a fixed batch of pairs,
 captured in a CUDA graph.
@@ -80,14 +80,10 @@ class MixedPolymul:
     # ---- execution ----
     def _launch(self, stream=None):
         s = _stream(stream)
-        for g in self.groups.values():
+        for g in self.groups.values():  # fused: 2 out-of-place forward DGTs, inverse with products on load
             e, n, rid = g["engine"], g["rows"], g["rid"]
-            g["wa"].copy_(g["a"])
-            g["wb"].copy_(g["b"])
-            call("cp_dgt_list", e.handle, _ptr(g["wa"]), _ptr(rid), n, FORWARD, s)
-            call("cp_dgt_list", e.handle, _ptr(g["wb"]), _ptr(rid), n, FORWARD, s)
-            call("cp_mul_list", e.handle, _ptr(g["c"]), _ptr(g["wa"]), _ptr(g["wb"]), _ptr(rid), n, s)
-            call("cp_dgt_list", e.handle, _ptr(g["c"]), _ptr(rid), n, INVERSE, s)
+            call("cp_polymul_list", e.handle, _ptr(g["c"]), _ptr(g["a"]), _ptr(g["b"]), _ptr(g["wa"]),
+                 _ptr(g["wb"]), _ptr(rid), n, s)
 
     def run(self):
         """Eager execution (also warms up every kernel before capture)."""
@@ -111,7 +107,7 @@ class MixedPolymul:
         self.graph.replay()
 
     def launches_per_run(self) -> int:
-        return 4 * len(self.groups)
+        return 3 * len(self.groups)
 
     def algorithmic_bytes(self) -> int:
         """24 nphi k bytes per product: read a, b and write c (16 B per Gaussian element)."""

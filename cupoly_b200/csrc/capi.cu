@@ -298,6 +298,46 @@ int cp_mul_list(const cp_engine* h, void* c, const void* a, const void* b, const
   return pw_mul_list(h->e, c, a, b, rid_list, nlist, S(stream));
 }
 
+size_t cp_polymul_workspace_bytes(const cp_engine* h, int base, int npolys) {
+  if (!valid_base(h, base) || base == CP_TBASE || npolys < 0) return 0;
+  return (size_t)2 * npolys * h->e.n_residues(base) * h->e.N * 16;
+}
+
+int cp_polymul(const cp_engine* h, void* c, const void* a, const void* b, int base, int npolys, void* workspace,
+               void* stream) {
+  CP_REQUIRE(valid_base(h, base) && base != CP_TBASE, "cp_polymul: bad engine or base");
+  CP_REQUIRE(c && a && b && workspace && npolys >= 0, "cp_polymul: bad argument");
+  if (npolys == 0) return CP_OK;
+  const Engine& e = h->e;
+  ulonglong2* wa = reinterpret_cast<ulonglong2*>(workspace);
+  ulonglong2* wb = wa + (size_t)npolys * e.n_residues(base) * e.N;
+  cudaStream_t st = S(stream);
+  if (int rc = launch_dgt_ex(e, wa, a, nullptr, base, npolys, 0, false, st)) return rc;
+  if (int rc = launch_dgt_ex(e, wb, b, nullptr, base, npolys, 0, false, st)) return rc;
+  InvSrc is{};
+  is.p[0] = wa;
+  is.p[1] = wb;
+  is.mode = 3;
+  is.npairs = 1;
+  return launch_dgt_ex(e, c, nullptr, &is, base, npolys, 0, true, st);
+}
+
+int cp_polymul_list(const cp_engine* h, void* c, const void* a, const void* b, void* wa, void* wb,
+                    const int* rid_list, int nlist, void* stream) {
+  CP_REQUIRE(h && c && a && b && wa && wb && rid_list && nlist >= 0, "cp_polymul_list: bad argument");
+  if (nlist == 0) return CP_OK;
+  const Engine& e = h->e;
+  cudaStream_t st = S(stream);
+  if (int rc = launch_dgt_list_ex(e, wa, a, nullptr, rid_list, nlist, false, st)) return rc;
+  if (int rc = launch_dgt_list_ex(e, wb, b, nullptr, rid_list, nlist, false, st)) return rc;
+  InvSrc is{};
+  is.p[0] = reinterpret_cast<const ulonglong2*>(wa);
+  is.p[1] = reinterpret_cast<const ulonglong2*>(wb);
+  is.mode = 3;
+  is.npairs = 1;
+  return launch_dgt_list_ex(e, c, nullptr, &is, rid_list, nlist, true, st);
+}
+
 #define PW_CHECK(name) CP_REQUIRE(valid_base(h, base) && base != CP_TBASE, name ": bad engine or base")
 
 int cp_add(const cp_engine* h, void* c, const void* a, const void* b, int base, void* stream) {

@@ -180,6 +180,13 @@ int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly
 // transformed with engine prime rid_list[i] (a device array).  Residues of
 // different polynomials and widths share one launch.
 int launch_dgt_list(const Engine& e, void* data_v, const int* rid_list, int nlist, bool inverse, cudaStream_t st) {
+  return launch_dgt_list_ex(e, data_v, nullptr, nullptr, rid_list, nlist, inverse, st);
+}
+
+// Work-list form with sources: forward from `fsrc` (nullptr: in place); inverse
+// reading per `isrc_p` (nullptr: in place; mode 3 forms products on load).
+int launch_dgt_list_ex(const Engine& e, void* data_v, const void* fsrc_v, const InvSrc* isrc_p, const int* rid_list,
+                       int nlist, bool inverse, cudaStream_t st) {
   if (nlist <= 0) return 0;
   RunFn fn = pick(e.plan.logNc, e.plan.logR);
   if (!fn) {
@@ -187,19 +194,24 @@ int launch_dgt_list(const Engine& e, void* data_v, const int* rid_list, int nlis
     return 3;
   }
   ulonglong2* data = reinterpret_cast<ulonglong2*>(data_v);
+  const ulonglong2* fsrc = reinterpret_cast<const ulonglong2*>(fsrc_v);
   InvSrc isrc{};
-  isrc.p[0] = data;
-  isrc.mode = 0;
-  isrc.npairs = 1;
+  if (isrc_p) {
+    isrc = *isrc_p;
+  } else {
+    isrc.p[0] = data;
+    isrc.mode = 0;
+    isrc.npairs = 1;
+  }
   const long long stride = e.N;
   const int S = e.plan.S;
   if (!inverse) {
     if (S > 0) {
-      int rc = launch_split(e, data, nullptr, 1, 0, nlist, stride, false, st, rid_list);
+      int rc = launch_split(e, data, fsrc, 1, 0, nlist, stride, false, st, rid_list);
       if (rc) return rc;
       return fn(e, data, nullptr, isrc, 1, 0, nlist, stride, false, false, st, rid_list);
     }
-    return fn(e, data, nullptr, isrc, 1, 0, nlist, stride, false, true, st, rid_list);
+    return fn(e, data, fsrc, isrc, 1, 0, nlist, stride, false, true, st, rid_list);
   }
   int rc = fn(e, data, nullptr, isrc, 1, 0, nlist, stride, true, S == 0, st, rid_list);
   if (rc || S == 0) return rc;

@@ -354,8 +354,9 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
     int rn, pn;
     coords(ub + gridDim.x, rn, pn);
     const size_t inner_n = ((size_t)rn << (LOGNC + S)) + ((size_t)((ub + gridDim.x) & ((1u << S) - 1)) << LOGNC);
-    if (src.mode == 0) {
+    if (src.mode == 0 || src.mode == 3) {
       prefetch_l2(src.p[0] + pn * poly_stride + inner_n, NC * 16u);
+      if (src.mode == 3) prefetch_l2(src.p[1] + pn * poly_stride + inner_n, NC * 16u);
     } else if (src.mode == 2) {
       prefetch_l2(src.p[pn / src.npairs] + (pn % src.npairs) * poly_stride + inner_n, NC * 16u);
     } else {
@@ -378,7 +379,18 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   ulonglong2* x = data + poly * poly_stride + inner;
   for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
   stage_twiddles<LOGNC, LOGR>(stw, tab, A.L.off_inv);
-  if (src.mode != 1) {
+  if (src.mode == 3) {
+    const size_t base = poly * poly_stride + inner;
+    const ModConst m = A.mc[rid];
+#pragma unroll 4
+    for (int j = 0; j < R; ++j) {
+      const int idx = tid + j * T;
+      const ulonglong2 a = src.p[0][base + idx], b = src.p[1][base + idx];
+      uint64_t cr, ci;
+      gi_mul(cr, ci, a.x, a.y, b.x, b.y, m);
+      sdat[pad16(idx)] = make_ulonglong2(cr, ci);
+    }
+  } else if (src.mode != 1) {
     const ulonglong2* xs = src.mode == 0
                                ? src.p[0] + poly * poly_stride + inner
                                : src.p[poly / src.npairs] + (poly % src.npairs) * poly_stride + inner;

@@ -64,7 +64,10 @@ struct DgtArgs {
 //  mode 1: the BFV tensor product of two ciphertexts (a0, a1) x (b0, b1) =
 //          p[0..3], computed while loading; output polynomial j * npairs + q
 //          is c_j of pair q: c0 = a0 b0, c1 = a0 b1 + a1 b0, c2 = a1 b1;
-//  mode 2: gather: output polynomial j * npairs + q reads polynomial q of p[j].
+//  mode 2: gather: output polynomial j * npairs + q reads polynomial q of p[j];
+//  mode 3: product: the Gaussian product p[0] * p[1] (both in the output's
+//          layout), formed while loading -- pointwise multiply fused into the
+//          inverse transform.
 struct InvSrc {
   const ulonglong2* p[4];
   int mode;

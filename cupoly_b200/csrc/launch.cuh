@@ -54,6 +54,8 @@ int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly
 int launch_dgt_ex(const Engine& e, void* dst, const void* fsrc, const InvSrc* isrc, int base, int npolys,
                   long long poly_stride, bool inverse, cudaStream_t st);
 int launch_dgt_list(const Engine& e, void* data, const int* rid_list, int nlist, bool inverse, cudaStream_t st);
+int launch_dgt_list_ex(const Engine& e, void* data, const void* fsrc, const InvSrc* isrc, const int* rid_list,
+                       int nlist, bool inverse, cudaStream_t st);
 // Residues rid_off .. rid_off + nres - 1 only (src nullptr: in place).
 int launch_dgt_part(const Engine& e, void* dst, const void* src, int rid_off, int nres, int npolys,
                     long long poly_stride, bool inverse, cudaStream_t st);

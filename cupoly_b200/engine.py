@@ -208,6 +208,15 @@ class Engine:
     def mul(self, c, a, b, base, stream=None):
         call("cp_mul", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
 
+    def polymul_workspace(self, base: int, npolys: int) -> torch.Tensor:
+        n = _lib.lib().cp_polymul_workspace_bytes(self._h, base, npolys)
+        return torch.empty(((n + 15) // 16, 2), dtype=torch.int64, device="cuda")
+
+    def polymul(self, c, a, b, base, workspace, npolys=None, stream=None):
+        """c = a b mod (x^nphi + 1) per residue, coefficient domain in and out (fused: 3 launches)."""
+        n = c.shape[0] if npolys is None else npolys
+        call("cp_polymul", self._h, _ptr(c), _ptr(a), _ptr(b), base, n, _ptr(workspace), _stream(stream))
+
     def mul_batch(self, c, a, b, base, npolys=None, stream=None):
         n = c.shape[0] if npolys is None else npolys
         call("cp_mul_batch", self._h, _ptr(c), _ptr(a), _ptr(b), base, n, _stream(stream))

@@ -115,6 +115,20 @@ int cp_dgt_list(const cp_engine* e, void* data, const int* rid_list, int nlist, 
 int cp_mul_list(const cp_engine* e, void* c, const void* a, const void* b, const int* rid_list, int nlist,
                 void* stream);
 
+/* ---- fused negacyclic polymul, coefficient domain in and out (no counterpart in cuPoly,
+ *      whose poly_mul composes upload DGTs, mul_dgt and a download IDGT,
+ *      src/arithmetic/polynomial.cu:892-914 with :105-188): c = a b mod (x^nphi + 1, q_r)
+ *      per residue, as forward DGT of a and b out of place into the workspace, then an
+ *      inverse DGT that forms the Gaussian products while loading (3 launches).  c may
+ *      alias a or b.  cp_polymul: npolys polynomials over `base`, workspace of
+ *      cp_polymul_workspace_bytes bytes.  cp_polymul_list: work-list form (see
+ *      cp_dgt_list), wa and wb each nlist x N x 16 bytes. ---- */
+size_t cp_polymul_workspace_bytes(const cp_engine* e, int base, int npolys);
+int cp_polymul(const cp_engine* e, void* c, const void* a, const void* b, int base, int npolys, void* workspace,
+               void* stream);
+int cp_polymul_list(const cp_engine* e, void* c, const void* a, const void* b, void* wa, void* wb,
+                    const int* rid_list, int nlist, void* stream);
+
 /* ---- pointwise, DGT domain: replace DGTEngine::execute_{add,sub,double_add,
  *      mul_dgt_gi,mul_dgt_u64,muladd,dr2}_dgt (src/cuda/dgt.cu:1096-1499) ---- */
 int cp_add(const cp_engine* e, void* c, const void* a, const void* b, int base, void* stream);

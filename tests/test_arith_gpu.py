@@ -191,3 +191,22 @@ def test_engines_coexist(gpu):
         t = from_u64(x)
         e.dgt(t, 0, FORWARD)
         assert np.array_equal(to_u64(t), CO.dgt(x, e.Q))
+
+
+@pytest.mark.parametrize("k,nphi,npolys", [(2, 4096, 3), (5, 8192, 2), (3, 16384, 1), (1, 32, 4), (4, 65536, 1)])
+def test_fused_polymul_vs_oracle(gpu, k, nphi, npolys):
+    """cp_polymul (out-of-place forward DGTs, inverse forming the products on load)
+    against the oracle's negacyclic product per prime; c may alias an input."""
+    from cupoly_b200.engine import Engine, QBase, from_u64, to_u64
+    from oracle import coracle
+    e = Engine(k, 0, nphi, 256)
+    a = np.stack([random_poly_residues(7 * i + k, e.Q, nphi) for i in range(npolys)])
+    b = np.stack([random_poly_residues(7 * i + k + 100, e.Q, nphi) for i in range(npolys)])
+    ref = coracle.polymul(a, b, e.Q)
+    da, db = from_u64(fold(a)), from_u64(fold(b))
+    c = e.empty(QBase, npolys)
+    ws = e.polymul_workspace(QBase, npolys)
+    e.polymul(c, da, db, QBase, ws)
+    assert np.array_equal(unfold(to_u64(c)), ref)
+    e.polymul(da, da, db, QBase, ws)                    # in place over a
+    assert np.array_equal(unfold(to_u64(da)), ref)
