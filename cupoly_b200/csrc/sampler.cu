@@ -56,6 +56,7 @@ enum Kind : int {
   UNIFORM = 5,            // uniform mod q_i, independently per residue
   TERNARY = 6,            // uniform {-1, 0, +1}
   GAUSSIAN = 7,           // discrete Gaussian sigma = 3.19, |x| <= 19, signed
+  SIGNED_DG = 8,          // CKKS engines' DISCRETE_GAUSSIAN: nearbyint(3.2 Z), signed (internal)
 };
 
 __device__ __forceinline__ uint64_t cdt_lookup(uint64_t u63, const uint64_t* cdt) {
@@ -92,6 +93,11 @@ __device__ __forceinline__ bool small_value(int kind, uint32_t c, uint32_t sid, 
       return true;
     }
     case DISCRETE_GAUSSIAN: v = (int64_t)cdt_lookup(u63, c_cdt_folded); return true;
+    case SIGNED_DG: {  // |nearbyint(3.2 Z)| with a symmetric sign is nearbyint(3.2 Z)
+      const int64_t m = (int64_t)cdt_lookup(u63, c_cdt_folded);
+      v = (r.v[2] & 1u) ? -m : m;
+      return true;
+    }
     case GAUSSIAN: {
       const int64_t m = (int64_t)cdt_lookup(u63, c_cdt_signed);
       v = (r.v[2] & 1u) ? -m : m;
@@ -228,6 +234,13 @@ int sample_poly(const Engine& e, void* out_v, int base, int kind, uint64_t seed,
     return CP_ERR_INVALID_;
   }
   if (int rc = upload_cdt()) return rc;
+  // cuPoly's CKKS build samples the small distributions signed (src/cuda/sampler.cu:
+  // 73-106, 459-493): narrow {0, 1, 2} with 2 -> p - 1, i.e. uniform {-1, 0, +1}, and
+  // the discrete Gaussian without the absolute value.
+  if (e.ckks_prec) {
+    if (kind == NARROW) kind = TERNARY;
+    else if (kind == DISCRETE_GAUSSIAN) kind = SIGNED_DG;
+  }
   int* err = e.d_err;
   auto* out = reinterpret_cast<ulonglong2*>(out_v);
   const long long ps = (long long)nres * e.N;

@@ -259,6 +259,8 @@ int cp_import_residues(const cp_engine* e, void* poly, const void* host_in, size
                        int* domain_out, void* stream);
 
 /* ---- sampler: replaces Sampler::sample(ctx, p, kind) (src/cuda/sampler.cu:576-645).
+ *      On a CKKS engine CP_NARROW is uniform {-1, 0, +1} and CP_DISCRETE_GAUSSIAN is
+ *      nearbyint(3.2 Z) signed, as in cuPoly's CKKS build (sampler.cu:73-106, 459-493).
  *      npolys consecutive polynomials over `base` with stream ids stream_id ..
  *      stream_id + npolys - 1; to_dgt != 0 applies the forward DGT (cuPoly does). */
 int cp_sample(const cp_engine* e, void* out, int base, int kind, uint64_t seed, uint32_t stream_id, int npolys,

@@ -437,6 +437,7 @@ def load_cdt(name):
 
 # Distribution kinds of the device sampler (values of enum cp_distribution).
 DISCRETE_GAUSSIAN, HAMMINGWEIGHT, NARROW, ZO, BINARY, UNIFORM, TERNARY, GAUSSIAN = range(8)
+SIGNED_DG = 8  # CKKS engines: DISCRETE_GAUSSIAN without the absolute value (device-internal kind)
 
 
 def _cdt_lookup(u63, cdt):
@@ -471,6 +472,9 @@ def sample_small(kind, c, sid, seed):
     if kind == GAUSSIAN:
         m = _cdt_lookup(u63, load_cdt("kCdtSigned"))
         return -m if (r[2] & 1) else m
+    if kind == SIGNED_DG:
+        m = _cdt_lookup(u63, load_cdt("kCdtFolded"))
+        return -m if (r[2] & 1) else m
     raise ValueError(kind)
 
 
@@ -503,8 +507,12 @@ def sample_hamming(nphi, sid, seed, h=64):
     return out
 
 
-def sample_poly(kind, primes, nphi, sid, seed):
-    """(nres, nphi) coefficient rows the device sampler produces."""
+def sample_poly(kind, primes, nphi, sid, seed, ckks=False):
+    """(nres, nphi) coefficient rows the device sampler produces.  On a CKKS engine the
+    small kinds are signed, as in cuPoly's CKKS build (``src/cuda/sampler.cu:73-106,
+    459-493``): NARROW is uniform {-1, 0, 1} and DISCRETE_GAUSSIAN is nearbyint(3.2 Z)."""
+    if ckks:
+        kind = {NARROW: TERNARY, DISCRETE_GAUSSIAN: SIGNED_DG}.get(kind, kind)
     rows = []
     if kind == UNIFORM:
         return [[sample_uniform(c, r, p, sid, seed) for c in range(nphi)] for r, p in enumerate(primes)]

@@ -208,3 +208,24 @@ def test_ckks_host_mirror(gpu):
 
 def Q_mod(cp, i):
     return cp.CUDAEngine.RNSPrimes[i]
+
+
+def test_ckks_sampler_is_signed_like_cupolys_ckks_build(gpu):
+    """On a CKKS engine NARROW is uniform {-1, 0, 1} and DISCRETE_GAUSSIAN is signed
+    (cuPoly's CKKS build, src/cuda/sampler.cu:73-106, 459-493); bit-exact against the
+    oracle's restatement, symmetric in distribution."""
+    from cupoly_b200.engine import DISCRETE_GAUSSIAN, NARROW, QBase
+    e = _eng(3, 4, 4096, 48)
+    for kind in (NARROW, DISCRETE_GAUSSIAN):
+        x = e.empty(QBase)
+        e.sample(x, QBase, kind, 77, 5, to_dgt=False)
+        got = unfold(_host(x))[0]
+        ref = np.array(O.sample_poly(kind, e.Q, 4096, 5, 77, ckks=True), dtype=np.uint64)
+        assert np.array_equal(got, ref)
+        q0 = e.Q[0]
+        v = np.where(got[0] > q0 // 2, got[0].astype(object) - q0, got[0].astype(object)).astype(np.int64)
+        assert (v < 0).any() and (v > 0).any() and abs(v.mean()) < 0.2
+        if kind == NARROW:
+            assert set(np.unique(v)) <= {-1, 0, 1}
+        else:
+            assert np.abs(v).max() <= 19
