@@ -1,8 +1,17 @@
-"""Build recipe of the in-tree shared library ``cupoly_b200/lib/libcupoly_b200.so``.
+"""Build recipe of the in-tree shared libraries.
 
-Every ``csrc/*.cu`` file is compiled for sm_100a only and linked with nvcc into
-one shared object exporting the C ABI of ``include/cupoly_b200.h``.  The
-library does not link against PyTorch.
+``cupoly_b200/lib/libcupoly_b200.so``: every ``csrc/*.cu`` file compiled for
+sm_100a only and linked with nvcc into one shared object exporting the C ABI of
+``include/cupoly_b200.h``.
+
+``cupoly_b200/lib/libcupoly.so``: the C++ host layer (``host/*.cpp``, cuPoly's
+``CUDAEngine`` / ``poly_t`` / ``poly_*`` API of ``include/cuPoly/``) compiled
+with g++ over that ABI, with the in-repo big integer standing in for NTL's ZZ
+(``include/ntl_shim``).  C++ programs written against cuPoly build with
+``-I include -I include/ntl_shim -I <cuda>/include -L cupoly_b200/lib -lcupoly
+-lcupoly_b200``.
+
+Neither library links against PyTorch.
 
     python -m cupoly_b200.build          # incremental
     python -m cupoly_b200.build --force  # rebuild everything
@@ -22,6 +31,9 @@ LIBDIR = os.path.join(HERE, "lib")
 OBJDIR = os.path.join(HERE, "lib", "obj")
 LIBNAME = "libcupoly_b200.so"
 LIBPATH = os.path.join(LIBDIR, LIBNAME)
+HOSTDIR = os.path.join(HERE, "host")
+INCDIR = os.path.abspath(os.path.join(HERE, "..", "include"))
+CXXLIB = os.path.join(LIBDIR, "libcupoly.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
@@ -58,6 +70,40 @@ def _compile(src: str, force: bool) -> str:
     return obj
 
 
+def cuda_home() -> str:
+    return os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
+
+
+def cxx_flags():
+    """Compile flags of a C++ program using the cuPoly host layer."""
+    return ["-std=c++17", "-I", INCDIR, "-I", os.path.join(INCDIR, "ntl_shim"), "-I",
+            os.path.join(cuda_home(), "include")]
+
+
+def cxx_link_flags():
+    """Link flags of a C++ program using the cuPoly host layer (rpaths to the in-tree libraries)."""
+    cudalib = os.path.join(cuda_home(), "lib64")
+    return ["-L", LIBDIR, "-Wl,-rpath," + LIBDIR, "-lcupoly", "-lcupoly_b200", "-L", cudalib,
+            "-Wl,-rpath," + cudalib, "-lcudart"]
+
+
+def build_host(force: bool = False) -> str:
+    """Compile the C++ host layer into lib/libcupoly.so (needs libcupoly_b200.so)."""
+    srcs = sorted(os.path.join(HOSTDIR, f) for f in os.listdir(HOSTDIR) if f.endswith(".cpp"))
+    headers = []
+    for root, _, files in os.walk(INCDIR):
+        headers += [os.path.join(root, f) for f in files if f.endswith(".h")]
+    if force or _stale(CXXLIB, srcs + headers + [LIBPATH]):
+        cxx = shutil.which("g++") or "g++"
+        cmd = [cxx, "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", "-Wno-unused-parameter"] + cxx_flags() + srcs + \
+            ["-o", CXXLIB, "-L", LIBDIR, "-Wl,-rpath,$ORIGIN", "-lcupoly_b200", "-L",
+             os.path.join(cuda_home(), "lib64"), "-Wl,-rpath," + os.path.join(cuda_home(), "lib64"), "-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("g++ failed for the host layer:\n%s\n%s" % (r.stdout, r.stderr))
+    return CXXLIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJDIR, exist_ok=True)
     sources = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
@@ -68,8 +114,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+    build_host(force)
     if verbose:
         print(LIBPATH)
+        print(CXXLIB)
     return LIBPATH
 
 

@@ -572,9 +572,6 @@ def poly_rho_bfv(ctx, c: List[poly_t], a: poly_t):
 
 
 # ---------------------------------------------------------------------------
-# Sampler (sampler.h:53-101)
-# ---------------------------------------------------------------------------
-# ---------------------------------------------------------------------------
 # CKKS mode (polynomial.cu:530-608, 696-800)
 # ---------------------------------------------------------------------------
 def poly_approx_basis_raising_Q_to_QB(ctx, a, b, level: int):
@@ -626,6 +623,9 @@ def poly_rho_ckks(ctx, c, a):
     c.status = RNSSTATE
 
 
+# ---------------------------------------------------------------------------
+# Sampler (sampler.h:53-101)
+# ---------------------------------------------------------------------------
 class Sampler:
     seed = SEED
     _counter = 0
@@ -637,23 +637,6 @@ class Sampler:
     @classmethod
     def reset(cls, ctx: Context):
         cls._counter = 0
-
-    @classmethod
-    def init_ckks(cls, k: int, kl: int, M: int, prec: int, log_radix: int = 0):
-        """CKKS build's init(k, kl, M, prec): Q = the first 63-bit prime and k - 1
-        primes of the prec-bit bucket, B = kl primes (cudaengine.cu:1192-1290)."""
-        if cls.is_init:
-            cls.destroy()
-        cls.engine = Engine.ckks(k, kl if kl > 0 else k + 1, M, prec, log_radix)
-        cls.N = M >> 1
-        cls.t = prec
-        cls.RNSPrimes = list(cls.engine.Q)
-        cls.RNSBPrimes = list(cls.engine.B)
-        cls.RNSProduct = _prod(cls.RNSPrimes)
-        cls.RNSBProduct = _prod(cls.RNSBPrimes)
-        cls.RNSMpi = [cls.RNSProduct // p for p in cls.RNSPrimes]
-        cls.RNSInvMpi = [pow(m % p, -1, p) for m, p in zip(cls.RNSMpi, cls.RNSPrimes)]
-        cls.is_init = True
 
     @classmethod
     def destroy(cls):
