@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-next", action="store_true", help="skip the CRT / xi-rho / wire / CKKS measurements")
     ap.add_argument("--serving-requests", type=int, default=10000)
     return ap.parse_args()
 
@@ -203,6 +204,95 @@ def run_reference(args, D: Dist):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def _timed(fn, reps: int) -> float:
+    """Average milliseconds of fn() over reps calls, CUDA events on the current stream."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def next_rows(seed: int, hbm_peak: float):
+    """Throughput of the calls after the multiplication chain, each with its algorithmic bytes
+    (what an ideal kernel reads and writes once) over the measured time:
+    device CRT / ICRT (512 polynomials, nphi 8192, k 5: limbs and residues both above L2 size),
+    xi and rho (one polynomial per call, as cuPoly's API), the binary wire form (host side,
+    128 polynomials), and the CKKS calls (nphi 16384, k 8, kl 9, 52-bit primes, one polynomial
+    per call, level k - 1)."""
+    import time
+
+    import torch
+
+    from cupoly_b200.engine import FORWARD, QBBase, QBase, UNIFORM, Engine
+
+    out = {}
+    e = Engine(K_Q, K_B, NPHI, T_PLAIN)
+    n, k, N = e.nphi, e.k, e.N
+    P = 512
+    x = e.empty(QBase, P)
+    e.sample(x, QBase, UNIFORM, seed, 1 << 20, npolys=P, to_dgt=False)
+    limbs = torch.zeros((P, n, k), dtype=torch.int64, device="cuda")
+    ms_icrt = _timed(lambda: e.icrt(limbs, x, QBase), 5)
+    y = e.empty(QBase, P)
+    ms_crt = _timed(lambda: e.crt(y, limbs, QBase), 5)
+    assert torch.equal(x, y), "CRT(ICRT(x)) != x"
+    byt = P * n * k * 8 * 2  # limbs read + residues written (and the reverse)
+    out["crt"] = {"config": "nphi=%d, k=%d, %d polys, %d-limb coefficients" % (n, k, P, k),
+                  "coeffs_per_s": round(P * n / (ms_crt / 1e3), 1), "GB_per_s": round(byt / ms_crt / 1e6, 1),
+                  "frac_hbm": round(byt / ms_crt / 1e6 / hbm_peak, 4)}
+    out["icrt"] = {"config": out["crt"]["config"], "coeffs_per_s": round(P * n / (ms_icrt / 1e3), 1),
+                   "GB_per_s": round(byt / ms_icrt / 1e6, 1), "frac_hbm": round(byt / ms_icrt / 1e6 / hbm_peak, 4)}
+    del limbs, y
+    xi = e.empty(QBase, k)
+    ms_xi = _timed(lambda: e.xi(xi, x[0:1]), 50)
+    ms_rho = _timed(lambda: e.rho(xi, x[0:1]), 50)
+    out["xi_rho"] = {"config": "nphi=%d, k=%d, one polynomial per call -> k polynomials" % (n, k),
+                     "xi_us_per_call": round(ms_xi * 1e3, 2), "rho_us_per_call": round(ms_rho * 1e3, 2),
+                     "GB_per_s": round((k * N * 16 * (1 + k)) / ms_xi / 1e6, 1)}
+    W = 128
+    blob = torch.empty(e.wire_bytes(QBase, W), dtype=torch.uint8, pin_memory=True).numpy()
+    z = e.empty(QBase, W)
+    t_exp, t_imp = [], []
+    for _ in range(3):  # first round warms the buffers; best of the other two
+        t0 = time.perf_counter()
+        e.export_residues(x[:W], QBase, 0, out=blob)
+        t1 = time.perf_counter()
+        e.import_residues(z, blob, QBase)
+        t2 = time.perf_counter()
+        t_exp.append(t1 - t0)
+        t_imp.append(t2 - t1)
+    assert torch.equal(z, x[:W])
+    out["wire"] = {"config": "%d polys (%d bytes, pinned host buffer)" % (W, blob.size),
+                   "export_GB_per_s": round(blob.size / min(t_exp[1:]) / 1e9, 2),
+                   "import_GB_per_s": round(blob.size / min(t_imp[1:]) / 1e9, 2),
+                   "note": "host wall clock per call: export = header + device-to-host copy; import = header "
+                           "and primes checked, every residue checked below its prime on the host, host-to-device copy"}
+    del x, xi, z, e
+    c = Engine.ckks(8, 9, 16384, 52)
+    lvl = 7
+    a = c.empty(QBase)
+    c.sample(a, QBase, UNIFORM, seed, 3, npolys=1, to_dgt=True)
+    qb = c.empty(QBBase)
+    r = c.empty(QBase)
+    ms_raise = _timed(lambda: c.ckks_modulus_raising(qb, a, lvl), 20)
+    ms_red = _timed(lambda: c.ckks_modulus_reduction(r, qb, lvl), 20)
+    ms_resc = _timed(lambda: c.ckks_rescale(r, None, lvl), 20)
+    c.check()
+    out["ckks"] = {"config": "nphi=16384, k=8, kl=9, prec 52, level 7, one polynomial per call, DGT domain",
+                   "modulus_raising_us": round(ms_raise * 1e3, 1), "modulus_reduction_us": round(ms_red * 1e3, 1),
+                   "rescale_us": round(ms_resc * 1e3, 1)}
+    del a, qb, r, c
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args, D: Dist):
     import torch
 
@@ -468,6 +558,9 @@ def run_ours(args, D: Dist):
         del buf, eL
         torch.cuda.empty_cache()
 
+    # ---- the rows after the chain: coefficient I/O, xi / rho, wire format, CKKS ----
+    nxt = next_rows(seed, hbm_peak) if (D.rank == 0 and not args.no_next) else None
+
     # ---- serving loop: open-loop Poisson arrivals, nphi in {4096..32768}, k = nphi/2048 ----
     serving = None
     if not args.no_serving and D.rank == 0:
@@ -530,6 +623,7 @@ def run_ours(args, D: Dist):
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback",
                          "int": int_roof},
             "large": large,
+            "next_rows": nxt,
             "serving": serving,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

@@ -121,6 +121,9 @@ __global__ void __launch_bounds__(256) k_sample(ulonglong2* __restrict__ out, co
   if (kind == UNIFORM) {
     for (int r = 0; r < nres; ++r) {
       const uint64_t p = mc[rid_off + r].p;
+      // candidates of bitlen(p) bits: every prime of the tables lies within 0.01 % below
+      // its power of two, so a candidate is accepted with probability > 0.9999
+      const uint64_t mask = ~0ull >> __clzll((long long)p);
       uint64_t val[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -128,8 +131,8 @@ __global__ void __launch_bounds__(256) k_sample(ulonglong2* __restrict__ out, co
         bool ok = false;
         for (uint32_t d = 0; d < 8 && !ok; ++d) {
           const Philox q = philox4x32_10(c, (uint32_t)r * 8u + d, sid, (uint32_t)kind, k0, k1);
-          const uint64_t u0 = ((uint64_t)(q.v[1] & 0x7FFFFFFFu) << 32) | q.v[0];
-          const uint64_t u1 = ((uint64_t)(q.v[3] & 0x7FFFFFFFu) << 32) | q.v[2];
+          const uint64_t u0 = (((uint64_t)q.v[1] << 32) | q.v[0]) & mask;
+          const uint64_t u1 = (((uint64_t)q.v[3] << 32) | q.v[2]) & mask;
           if (u0 < p) {
             val[h] = u0;
             ok = true;

@@ -280,18 +280,30 @@ class Engine:
     def wire_bytes(self, base: int, npolys: int = 1) -> int:
         return int(_lib.lib().cp_wire_bytes(self._h, base, npolys))
 
-    def export_residues(self, x, base: int, domain: int, stream=None) -> bytes:
-        """Binary wire form of x (npolys, nres, N, 2); domain 0 coefficient, 1 DGT."""
+    def export_residues(self, x, base: int, domain: int, stream=None, out: Optional[np.ndarray] = None):
+        """Binary wire form of x (npolys, nres, N, 2); domain 0 coefficient, 1 DGT.  Returns
+        bytes, or fills and returns `out` (a uint8 array of wire_bytes, e.g. reused or pinned
+        host memory, which avoids the allocation and the copy into a bytes object)."""
         n = self.wire_bytes(base, x.shape[0])
+        if out is not None:
+            if out.dtype != np.uint8 or out.size < n or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError("export_residues: out must be a contiguous uint8 array of wire_bytes")
+            call("cp_export_residues", self._h, C.c_void_p(out.ctypes.data), out.size, _ptr(x), base, x.shape[0],
+                 domain, _stream(stream))
+            return out
         buf = C.create_string_buffer(n)
         call("cp_export_residues", self._h, buf, n, _ptr(x), base, x.shape[0], domain, _stream(stream))
         return buf.raw
 
-    def import_residues(self, x, data: bytes, base: int, stream=None) -> int:
-        """Fill x (npolys, nres, N, 2) from the wire form; returns the recorded domain."""
+    def import_residues(self, x, data, base: int, stream=None) -> int:
+        """Fill x (npolys, nres, N, 2) from the wire form (bytes or a uint8 array); returns the
+        recorded domain."""
         dom = C.c_int(-1)
-        call("cp_import_residues", self._h, _ptr(x), data, len(data), base, x.shape[0], C.byref(dom),
-             _stream(stream))
+        if isinstance(data, np.ndarray):
+            src, size = C.c_void_p(np.ascontiguousarray(data).ctypes.data), data.size
+        else:
+            src, size = data, len(data)
+        call("cp_import_residues", self._h, _ptr(x), src, size, base, x.shape[0], C.byref(dom), _stream(stream))
         return dom.value
 
     # ---- HPS (coefficient domain) ----

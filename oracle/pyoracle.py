@@ -479,12 +479,14 @@ def sample_small(kind, c, sid, seed):
 
 
 def sample_uniform(c, r, p, sid, seed):
-    """Uniform residue mod p of coefficient c in residue r (rejection on 63 bits)."""
+    """Uniform residue mod p of coefficient c in residue r: rejection on candidates of
+    bitlen(p) bits (63 for the BFV primes, 45..55 for the CKKS buckets)."""
     k0, k1 = seed & _M, (seed >> 32) & _M
+    mask = (1 << p.bit_length()) - 1
     for d in range(8):
         q = philox4x32_10((c, r * 8 + d, sid, UNIFORM), (k0, k1))
-        u0 = ((q[1] & 0x7FFFFFFF) << 32) | q[0]
-        u1 = ((q[3] & 0x7FFFFFFF) << 32) | q[2]
+        u0 = ((q[1] << 32) | q[0]) & mask
+        u1 = ((q[3] << 32) | q[2]) & mask
         if u0 < p:
             return u0
         if u1 < p:

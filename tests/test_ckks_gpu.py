@@ -229,3 +229,21 @@ def test_ckks_sampler_is_signed_like_cupolys_ckks_build(gpu):
             assert set(np.unique(v)) <= {-1, 0, 1}
         else:
             assert np.abs(v).max() <= 19
+
+
+@pytest.mark.parametrize("prec", [45, 52, 55])
+def test_ckks_uniform_sampler_over_narrow_primes(gpu, prec):
+    """UNIFORM on a CKKS engine: candidates of bitlen(q_i) bits, so the 45..55-bit primes
+    accept as readily as the 63-bit ones (no rejection-limit error); bit-exact against the
+    oracle, every residue below its prime, mean near q_i / 2."""
+    from cupoly_b200.engine import QBase, UNIFORM
+    e = _eng(3, 4, 2048, prec)
+    x = e.empty(QBase, 4)
+    e.sample(x, QBase, UNIFORM, 91, 11, npolys=4, to_dgt=False)
+    e.check()  # raises if any coefficient hit the rejection limit
+    got = unfold(_host(x[3:4]))[0]
+    ref = np.array(O.sample_poly(UNIFORM, e.Q, 2048, 14, 91, ckks=True), dtype=np.uint64)
+    assert np.array_equal(got, ref)
+    for r, q in enumerate(e.Q):
+        assert int(got[r].max()) < q
+        assert abs(float(np.mean(got[r].astype(np.float64))) / q - 0.5) < 0.03
