@@ -407,6 +407,166 @@ def simple_scaling_exact(xq, Q, t):
 
 
 # ----------------------------------------------------------------------------
+# cuPoly's floating-point HPS path, restated word for word (disagreement counts)
+# ----------------------------------------------------------------------------
+# cuPoly estimates the CRT overflow and the HPS rounding in double precision.
+# These functions reproduce its kernels' arithmetic from IEEE-754 semantics:
+# round-to-nearest-even (Python float arithmetic, float(int), float(Fraction)),
+# round-down (exact rational, then the next double below when the nearest is
+# above), llrint = nearest-even, 64-bit wrap-around for cuPoly's addmod / submod
+# macros (include/cuPoly/cuda/dgt.h:74-82).  Where that path is exact they equal
+# the *_exact functions above; where it is not, the difference shows.
+_U64 = (1 << 64) - 1
+FPERROR = 1e-9  # include/cuPoly/settings.h
+
+
+def _rd(r) -> float:
+    """The largest double <= the rational r."""
+    from fractions import Fraction
+    import math
+
+    f = float(r)
+    if Fraction(f) > r:
+        f = math.nextafter(f, -math.inf)
+    return f
+
+
+def _fma_rd(a: float, b: float, c: float) -> float:
+    from fractions import Fraction
+
+    return _rd(Fraction(a) * Fraction(b) + Fraction(c))
+
+
+def _drcp_rd(d: float) -> float:
+    from fractions import Fraction
+
+    return _rd(1 / Fraction(d))
+
+
+def _addmod64(a, b, p):
+    """cuPoly's addmod on 64-bit words: a + b, minus p when a + b >= p (wrapping)."""
+    s = (a + b) & _U64
+    return (s - p) & _U64 if s >= p else s
+
+
+def _submod64(a, b, p):
+    """cuPoly's submod on 64-bit words: a - b, or a + (p - b) when a < b (wrapping)."""
+    return (a + (p - b)) & _U64 if a < b else (a - b) & _U64
+
+
+def _v_rule(value: float) -> int:
+    """Overflow count from the double sum: the nearest integer when within FPERROR of
+    it, else the floor (``src/cuda/cudaengine.cu:532-533, 700-701``)."""
+    import math
+
+    r = round(value)
+    return r if abs(value - r) <= FPERROR else math.floor(value)
+
+
+def cupoly_float_ext_q_to_b(xs, Q, B):
+    """cuPoly's Q -> B conversion of one coefficient (``cudaengine.cu:483-649``):
+    aux_i = x_i [(Q/q_i)^-1]_{q_i}; v from fma_rd(aux_i, rcp_rd(q_i)) summed in double;
+    y_j = sum_i aux_i (Q/q_i mod b_j) - v (Q mod b_j) with cuPoly's addmod / submod."""
+    Qp = prod(Q)
+    aux = [x * pow(Qp // q % q, -1, q) % q for x, q in zip(xs, Q)]
+    value = 0.0
+    for a, q in zip(aux, Q):
+        value = _fma_rd(float(a), _drcp_rd(float(q)), value)
+    v = _v_rule(value)
+    out = []
+    for b in B:
+        acc = 0
+        for a, q in zip(aux, Q):
+            acc = _addmod64(acc, a * (Qp // q % b) % b, b)
+        out.append(_submod64(acc, v * (Qp % b) % b, b))
+    return out
+
+
+def cupoly_float_ext_b_to_q(ys, Q, B):
+    """cuPoly's B -> Q conversion of one coefficient (``cudaengine.cu:659-796``): as
+    the Q -> B one, with v from aux_j / (double) b_j summed in round-to-nearest."""
+    Bp = prod(B)
+    aux = [y * pow(Bp // b % b, -1, b) % b for y, b in zip(ys, B)]
+    value = 0.0
+    for a, b in zip(aux, B):
+        value += float(a) / float(b)
+    v = _v_rule(value)
+    out = []
+    for q in Q:
+        acc = 0
+        for a, b in zip(aux, B):
+            acc = _addmod64(acc, a * (Bp // b % q) % q, q)
+        out.append(_submod64(acc, v * (Bp % q) % q, q))
+    return out
+
+
+@lru_cache(maxsize=None)
+def _cupoly_omega(Q, B, t):
+    """omega_int, the 128-bit omega_frac and lambda of ``cudaengine.cu:1466-1492``:
+    omega_{l,j} = t [(QB/q_l)^-1]_{q_l} B / q_l split into floor mod b_j and a 128-bit
+    fraction (floor of frac * 2^128; cuPoly rounds a 512-bit RR, which differs from
+    the floor by at most one unit of 2^-128); lambda_j = t [(QB/b_j)^-1]_{b_j} (B/b_j)
+    mod b_j."""
+    Qp, Bp = prod(Q), prod(B)
+    lam = tuple(t * pow(Bp * Qp // b % b, -1, b) * (Bp // b) % b for b in B)
+    om_int, om_frac = {}, {}
+    for j, b in enumerate(B):
+        for l, q in enumerate(Q):
+            aux = t * pow(Qp * Bp // q % q, -1, q) * Bp
+            ti = aux // q
+            om_int[l, j] = ti % b
+            om_frac[l, j] = ((aux - ti * q) << 128) // q
+    return om_int, om_frac, lam
+
+
+def cupoly_float_complex_scaling(xq, yb, Q, B, t):
+    """cuPoly's polynomial_complex_scaling for one coefficient (``cudaengine.cu:382-440``):
+    per B prime, sum over Q of x omega_int mod b_j plus the integer part of
+    omega_frac x (__umul128hi = floor(omega_frac x / 2^64), 128 bits), the fraction
+    parts accumulated in double by fma_rn (exact products: lo 2^-64) and added back by
+    llrint, plus x_B lambda_j; cuPoly's addmod throughout (so a B residue can stay
+    non-canonical when an integer part reaches b_j)."""
+    om_int, om_frac, lam = _cupoly_omega(tuple(Q), tuple(B), t)
+    out = []
+    for j, b in enumerate(B):
+        result, acc = 0, 0.0
+        for l, x in enumerate(xq):
+            vint = x * om_int[l, j] % b
+            c = (om_frac[l, j] * x) >> 64
+            hi, lo = c >> 64, c & _U64
+            acc = float(lo) * 2.0 ** -64 + acc
+            result = _addmod64(result, _addmod64(vint, hi, b), b)
+        result = _addmod64(result, round(acc), b)
+        result = _addmod64(result, yb[j] * lam[j] % b, b)
+        out.append(result)
+    return out
+
+
+def cupoly_float_complex_scaling_tdivq(xq, yb, Q, B, t):
+    """``poly_complex_scaling_tDivQ`` on cuPoly's float path: the scaling above, then
+    its float B -> Q conversion (``polynomial.cu:350-404``)."""
+    return cupoly_float_ext_b_to_q(cupoly_float_complex_scaling(xq, yb, Q, B, t), Q, B)
+
+
+def cupoly_float_simple_scaling(xq, Q, t):
+    """cuPoly's simple_scaling for one coefficient, t a power of two (``cudaengine.cu:323-362``,
+    tomega from ``:1494-1509``): integer parts masked mod t, fraction parts summed in double."""
+    assert t > 0 and t & (t - 1) == 0
+    Qp = prod(Q)
+    result, acc = 0, 0.0
+    for x, q in zip(xq, Q):
+        aux = t * pow(Qp // q % q, -1, q)
+        ti = aux // q
+        frac = ((aux - ti * q) << 128) // q
+        vint = (x * ti) & _U64 & (t - 1)
+        c = (frac * x) >> 64
+        hi, lo = c >> 64, c & _U64
+        acc = acc + float(lo) * 2.0 ** -64
+        result = (result + ((vint + (hi & (t - 1))) & (t - 1))) & _U64
+    return (result + round(acc)) & (t - 1)
+
+
+# ----------------------------------------------------------------------------
 # Sampler: Philox4x32-10 and the distributions of the device sampler
 # ----------------------------------------------------------------------------
 _M = 0xFFFFFFFF

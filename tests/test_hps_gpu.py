@@ -254,3 +254,58 @@ def test_scaling_exact_fallback_edges(gpu, k):
     o0 = e.empty(0)
     e.basis_ext_b_to_q(o0, _dev(fold(yb)[None]))
     assert np.array_equal(unfold(_host(o0))[0], CO.basis_ext(yb, e.B, e.Q))
+
+
+@pytest.mark.parametrize("k,t", [(2, 256), (5, 256), (5, 65536)])
+def test_device_matches_cupolys_float_path_where_it_is_exact(gpu, k, t):
+    """Against a word-for-word restatement of cuPoly's double-precision HPS kernels
+    (oracle/pyoracle.py cupoly_float_*): on random coefficients the device's Q -> B,
+    B -> Q, complex and simple scaling agree with cuPoly's path everywhere; at X = Q - 1
+    and next to the half-integer rounding boundary, the only places cuPoly's path
+    differs from the exact value, the device gives the exact one."""
+    from cupoly_b200.engine import Engine
+    nphi = 512
+    e = Engine(k, 0, nphi, t)
+    Q, B = list(e.Q), list(e.B)
+    Qp, Bp = O.prod(Q), O.prod(B)
+    rng = np.random.default_rng(k * 1000 + t)
+    Xs = [int(rng.integers(0, 1 << 62)) * (1 << 62) % Qp for _ in range(nphi)]
+    Xs[0], Xs[1] = Qp - 1, Qp - 2
+    ti = pow(t, -1, Qp)
+    Zs = [int(rng.integers(0, 1 << 62)) * (1 << 60) % (Qp * Bp) for _ in range(nphi)]
+    for i, h in enumerate(((Qp - 1) // 2, (Qp + 1) // 2, (Qp - 3) // 2, (Qp + 3) // 2)):
+        Zs[i] = (h * ti) % Qp + Qp * (i + 1)
+    xq = np.array([[X % q for X in Xs] for q in Q], dtype=np.uint64)
+    yb = np.array([[X % b for X in Xs] for b in B], dtype=np.uint64)  # X < Q < B: a valid B value too
+    zq = np.array([[Z % q for Z in Zs] for q in Q], dtype=np.uint64)
+    zb = np.array([[Z % b for Z in Zs] for b in B], dtype=np.uint64)
+    ob, oq, oc, ot = e.empty(1), e.empty(0), e.empty(1), e.empty(3)
+    e.basis_ext_q_to_b(ob, _dev(fold(xq)[None]))
+    e.basis_ext_b_to_q(oq, _dev(fold(yb)[None]))
+    e.complex_scaling(oc, _dev(fold(zq)[None]), _dev(fold(zb)[None]))
+    e.simple_scaling(ot, _dev(fold(xq)[None]))
+    ob, oq, oc = (unfold(_host(x))[0] for x in (ob, oq, oc))
+    ot = unfold(_host(ot))[0, 0]
+    edge_c = {0, 1, 2, 3}
+    diff = {"q_to_b": [], "b_to_q": [], "complex": [], "simple": []}
+    for c in range(nphi):
+        xs, ys = [int(v) for v in xq[:, c]], [int(v) for v in yb[:, c]]
+        zqs, zbs = [int(v) for v in zq[:, c]], [int(v) for v in zb[:, c]]
+        if [int(v) for v in ob[:, c]] != O.cupoly_float_ext_q_to_b(xs, Q, B):
+            diff["q_to_b"].append(c)
+        if [int(v) for v in oq[:, c]] != O.cupoly_float_ext_b_to_q(ys, Q, B):
+            diff["b_to_q"].append(c)
+        if [int(v) for v in oc[:, c]] != O.cupoly_float_complex_scaling(zqs, zbs, Q, B, t):
+            diff["complex"].append(c)
+        if t & (t - 1) == 0 and int(ot[c]) != O.cupoly_float_simple_scaling(xs, Q, t):
+            diff["simple"].append(c)
+    # cuPoly misreads X = Q - 1 (and Q - 2) as negative; the device is exact there
+    assert set(diff["q_to_b"]) <= {0, 1} and 0 in diff["q_to_b"]
+    assert [int(v) for v in ob[:, 0]] == [(Qp - 1) % b for b in B]
+    assert set(diff["b_to_q"]) <= {0, 1}
+    # scaling: disagreements only at the engineered half-integer edges, where the device is exact
+    assert set(diff["complex"]) <= edge_c
+    for c in diff["complex"]:
+        assert [int(v) for v in oc[:, c]] == O.complex_scaling_exact([int(v) for v in zq[:, c]],
+                                                                      [int(v) for v in zb[:, c]], Q, B, t)
+    assert set(diff["simple"]) <= {0, 1}

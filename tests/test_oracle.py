@@ -179,3 +179,49 @@ def test_sampler_restatement_support():
 def test_fold_unfold():
     x = np.arange(16, dtype=np.uint64).reshape(2, 8)
     assert (unfold(fold(x)) == x).all()
+
+
+@pytest.mark.parametrize("k", [1, 2, 5, 10])
+def test_cupoly_float_path_equals_exact_on_random_inputs(k):
+    """The restatement of cuPoly's double-precision HPS path (overflow count with FPERROR,
+    128-bit fractions summed in double) gives the exact values on random inputs."""
+    import random
+    rng = random.Random(k)
+    Q, B = O.bases(k, k + 1)
+    Qp, Bp = O.prod(Q), O.prod(B)
+    for _ in range(150):
+        X, Y, Z = rng.randrange(Qp), rng.randrange(Bp), rng.randrange(Qp * Bp)
+        xs, ys = [X % q for q in Q], [Y % b for b in B]
+        zq, zb = [Z % q for q in Q], [Z % b for b in B]
+        assert O.cupoly_float_ext_q_to_b(xs, Q, B) == O.basis_extension_exact(xs, Q, B)
+        assert O.cupoly_float_ext_b_to_q(ys, Q, B) == O.basis_extension_exact(ys, B, Q)
+        assert O.cupoly_float_complex_scaling(zq, zb, Q, B, 256) == O.complex_scaling_exact(zq, zb, Q, B, 256)
+        assert O.cupoly_float_complex_scaling_tdivq(zq, zb, Q, B, 256) == \
+            O.complex_scaling_tdivq_exact(zq, zb, Q, B, 256)
+        assert O.cupoly_float_simple_scaling(xs, Q, 256) == O.simple_scaling_exact(xs, Q, 256)
+
+
+def test_cupoly_float_path_is_off_at_its_edges():
+    """Where cuPoly's float path is wrong: X = Q - 1 reads as X - Q (v rounded up within
+    FPERROR), and t X / Q within 1/Q of a half-integer rounds the wrong way about half
+    the time -- each time by exactly one.  The exact definitions used here and on the
+    device are right at both."""
+    import random
+    rng = random.Random(7)
+    for k in (1, 3, 5):
+        Q, B = O.bases(k, k + 1)
+        Qp, Bp = O.prod(Q), O.prod(B)
+        xs = [(Qp - 1) % q for q in Q]
+        assert O.cupoly_float_ext_q_to_b(xs, Q, B) == [(Qp - 1 - Qp) % b for b in B]
+        assert O.basis_extension_exact(xs, Q, B) == [(Qp - 1) % b for b in B]
+        ti, wrong = pow(256, -1, Qp), 0
+        for h in ((Qp - 1) // 2, (Qp + 1) // 2, (Qp - 3) // 2, (Qp + 3) // 2):
+            for _ in range(3):
+                Z = (h * ti) % Qp + Qp * rng.randrange(Bp)  # 256 Z = h mod Q: next to a half-integer
+                zq, zb = [Z % q for q in Q], [Z % b for b in B]
+                f = O.cupoly_float_complex_scaling(zq, zb, Q, B, 256)
+                ex = O.complex_scaling_exact(zq, zb, Q, B, 256)
+                if f != ex:
+                    wrong += 1
+                    assert all((a - e) % b in (1, b - 1) for a, e, b in zip(f, ex, B))
+        assert wrong > 0
