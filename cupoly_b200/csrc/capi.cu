@@ -308,6 +308,7 @@ int cp_polymul(const cp_engine* h, void* c, const void* a, const void* b, int ba
   CP_REQUIRE(valid_base(h, base) && base != CP_TBASE, "cp_polymul: bad engine or base");
   CP_REQUIRE(c && a && b && workspace && npolys >= 0, "cp_polymul: bad argument");
   if (npolys == 0) return CP_OK;
+  NvtxRange range("cp_polymul");
   const Engine& e = h->e;
   ulonglong2* wa = reinterpret_cast<ulonglong2*>(workspace);
   ulonglong2* wb = wa + (size_t)npolys * e.n_residues(base) * e.N;
@@ -522,6 +523,7 @@ int cp_bfv_mul(const cp_engine* h, void* c0, void* c1, void* c2, const void* a0,
                const void* b1, void* ws, void* stream) {
   CP_BFV_ONLY(h, "cp_bfv_mul");
   CP_REQUIRE(h && c0 && c1 && c2 && a0 && a1 && b0 && b1 && ws, "cp_bfv_mul: bad argument");
+  NvtxRange range("cp_bfv_mul");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
   const size_t qe = (size_t)e.k * e.N, be = (size_t)e.kl * e.N;
@@ -553,6 +555,7 @@ int cp_bfv_mul_batch(const cp_engine* h, void* c, const void* a0, const void* a1
   CP_BFV_ONLY(h, "cp_bfv_mul_batch");
   CP_REQUIRE(h && c && a0 && a1 && b0 && b1 && ws && npairs >= 0, "cp_bfv_mul_batch: bad argument");
   if (npairs == 0) return CP_OK;
+  NvtxRange range("cp_bfv_mul_batch");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
   const size_t P = (size_t)npairs;
@@ -570,13 +573,20 @@ int cp_bfv_mul_batch(const cp_engine* h, void* c, const void* a0, const void* a1
   gather.p[3] = reinterpret_cast<const ulonglong2*>(b1);
   gather.mode = 2;
   gather.npairs = npairs;
-  CP_TRY(launch_dgt_ex(e, X, nullptr, &gather, CP_QBASE, 4 * npairs, 0, true, st));
+  {
+    NvtxRange r("inverse DGT over Q (4P)");
+    CP_TRY(launch_dgt_ex(e, X, nullptr, &gather, CP_QBASE, 4 * npairs, 0, true, st));
+  }
   // 2. exact Q -> B extension, forward DGT over B
-  CP_TRY(hps_basis_ext(e, XB, X, true, 4 * npairs, st));
-  CP_TRY(launch_dgt(e, XB, CP_BBASE, 4 * npairs, 0, false, st));
+  {
+    NvtxRange r("Q -> B, forward DGT over B (4P)");
+    CP_TRY(hps_basis_ext(e, XB, X, true, 4 * npairs, st));
+    CP_TRY(launch_dgt(e, XB, CP_BBASE, 4 * npairs, 0, false, st));
+  }
   // 3. tensor product computed inside the inverse DGTs (Q side from the inputs, B side from XB)
   InvSrc tq = gather;
   tq.mode = 1;
+  NvtxRange r3("tensor products + inverse DGTs (3P over Q and B)");
   CP_TRY(launch_dgt_ex(e, CQ, nullptr, &tq, CP_QBASE, 3 * npairs, 0, true, st));
   InvSrc tb{};
   for (int v = 0; v < 4; ++v) tb.p[v] = XB + v * P * be;
@@ -584,6 +594,7 @@ int cp_bfv_mul_batch(const cp_engine* h, void* c, const void* a0, const void* a1
   tb.npairs = npairs;
   CP_TRY(launch_dgt_ex(e, CB, nullptr, &tb, CP_BBASE, 3 * npairs, 0, true, st));
   // 4. round(t X / Q) and B -> Q, then forward DGT of the outputs
+  NvtxRange r4("scale t/Q, B -> Q, forward DGT over Q (3P)");
   CP_TRY(hps_scale_to_q(e, c, CQ, CB, U, 3 * npairs, st));
   return launch_dgt(e, c, CP_QBASE, 3 * npairs, 0, false, st);
 }

@@ -2,12 +2,24 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <atomic>
 #include <string>
 
 #include "engine.cuh"
 
 namespace cpoly {
+
+// NVTX range for the duration of a scope: names the composite calls and the stages
+// of the batched chain on a profiler timeline (header-only NVTX 3; without a tool
+// attached a push / pop is a check of one function pointer).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Status codes of the C ABI (mirrored in include/cupoly_b200.h).
 enum : int {

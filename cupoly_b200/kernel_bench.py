@@ -1,0 +1,168 @@
+"""Per-kernel throughput on the current GPU, each against the HBM roofline.
+
+    python -m cupoly_b200.kernel_bench [--only NAME[,NAME...]] [--reps R] [--peak GBS]
+
+One JSON line per workload: average milliseconds per launch (CUDA events on the
+launching stream, after a warm-up launch), the algorithmic bytes one launch must
+move (each input read once, each output written once), the achieved GB/s and its
+fraction of the HBM peak (`--peak`, default the copy bandwidth recorded in
+MEASURED_PEAKS.json at the repository root when present, else 6650 GB/s).  Every
+workload's data exceeds the 126 MB L2, so successive launches stream from HBM.
+
+Workloads (names for --only):
+  dgt_fwd, dgt_inv   forward / inverse DGT, nphi 8192, 3072 residues (512 polynomials over B, in place)
+  mul                DGT-domain pointwise product, nphi 8192, k 5, 512 polynomials
+  polymul            fused negacyclic product (cp_polymul), nphi 4096, k 2, 2048 polynomials
+  basis_ext          exact Q -> B conversion, nphi 8192, k 5 -> 6, 512 polynomials
+  complex_scaling    round(t X / Q) mod B, nphi 8192, k 5, kl 6, 384 polynomials
+  crt, icrt          coefficient limbs <-> residues, nphi 8192, k 5, 512 polynomials
+  sample_ternary, sample_gaussian, sample_uniform
+                     2^24 coefficients x 16 residues (nphi 32768, k 16, 512 polynomials)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+import torch
+
+from .engine import (FORWARD, GAUSSIAN, INVERSE, QBase, BBase, TERNARY, UNIFORM, Engine)
+
+_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _peak() -> float:
+    try:
+        with open(os.path.join(_ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
+
+def _time(fn, reps: int) -> float:
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def workloads():
+    """name -> builder; a builder returns (launch function, algorithmic bytes, description)."""
+    W = {}
+
+    def dgt(direction):
+        def build():
+            e = Engine(5, 6, 8192, 256)
+            x = e.empty(BBase, 512)  # 512 x 6 = 3072 residues: the chain's forward DGT over B
+            e.sample(x, BBase, UNIFORM, 1, 0, npolys=512, to_dgt=False)
+            nres = 512 * 6
+            return (lambda: e.dgt(x, BBase, direction), nres * e.N * 16 * 2,
+                    "%s DGT, nphi 8192, %d residues" % ("forward" if direction == FORWARD else "inverse", nres), e)
+        return build
+
+    W["dgt_fwd"] = dgt(FORWARD)
+    W["dgt_inv"] = dgt(INVERSE)
+
+    def mul():
+        e = Engine(5, 6, 8192, 256)
+        P = 512
+        a, b, c = e.empty(QBase, P), e.empty(QBase, P), e.empty(QBase, P)
+        e.sample(a, QBase, UNIFORM, 2, 0, npolys=P, to_dgt=False)
+        e.sample(b, QBase, UNIFORM, 2, P, npolys=P, to_dgt=False)
+        return (lambda: e.mul_batch(c, a, b, QBase, P), 3 * P * 5 * e.N * 16,
+                "pointwise Gaussian product, nphi 8192, k 5, %d polys" % P, e)
+
+    W["mul"] = mul
+
+    def polymul():
+        e = Engine(2, 3, 4096, 256)
+        P = 2048
+        a, b, c = e.empty(QBase, P), e.empty(QBase, P), e.empty(QBase, P)
+        e.sample(a, QBase, UNIFORM, 3, 0, npolys=P, to_dgt=False)
+        e.sample(b, QBase, UNIFORM, 3, P, npolys=P, to_dgt=False)
+        ws = e.polymul_workspace(QBase, P)
+        return (lambda: e.polymul(c, a, b, QBase, ws, P), 3 * P * 2 * e.N * 16,
+                "fused polymul (3 launches), nphi 4096, k 2, %d polys; bytes = a, b read + c written" % P, e)
+
+    W["polymul"] = polymul
+
+    def basis_ext():
+        e = Engine(5, 6, 8192, 256)
+        P = 512
+        x, y = e.empty(QBase, P), e.empty(BBase, P)
+        e.sample(x, QBase, UNIFORM, 4, 0, npolys=P, to_dgt=False)
+        return (lambda: e.basis_ext_q_to_b(y, x, P), P * (5 + 6) * e.N * 16,
+                "exact Q -> B, nphi 8192, k 5 -> 6, %d polys" % P, e)
+
+    W["basis_ext"] = basis_ext
+
+    def complex_scaling():
+        e = Engine(5, 6, 8192, 256)
+        P = 384
+        x, xb, y = e.empty(QBase, P), e.empty(BBase, P), e.empty(BBase, P)
+        e.sample(x, QBase, UNIFORM, 5, 0, npolys=P, to_dgt=False)
+        e.sample(xb, BBase, UNIFORM, 5, P, npolys=P, to_dgt=False)
+        return (lambda: e.complex_scaling(y, x, xb, P), P * (5 + 6 + 6) * e.N * 16,
+                "round(t X / Q) mod B, nphi 8192, k 5, kl 6, %d polys" % P, e)
+
+    W["complex_scaling"] = complex_scaling
+
+    def crt(inverse):
+        def build():
+            e = Engine(5, 6, 8192, 256)
+            P = 512
+            x = e.empty(QBase, P)
+            e.sample(x, QBase, UNIFORM, 6, 0, npolys=P, to_dgt=False)
+            limbs = torch.zeros((P, e.nphi, 5), dtype=torch.int64, device="cuda")
+            e.icrt(limbs, x, QBase)
+            fn = (lambda: e.icrt(limbs, x, QBase)) if inverse else (lambda: e.crt(x, limbs, QBase))
+            return (fn, 2 * P * e.nphi * 5 * 8,
+                    "%s, nphi 8192, k 5, %d polys, 5-limb coefficients" % ("ICRT" if inverse else "CRT", P), e)
+        return build
+
+    W["crt"] = crt(False)
+    W["icrt"] = crt(True)
+
+    def sample(kind, name):
+        def build():
+            e = Engine(16, 17, 32768, 65537)
+            P = 512
+            x = e.empty(QBase, P)
+            return (lambda: e.sample(x, QBase, kind, 7, 0, npolys=P, to_dgt=False), P * 16 * e.N * 16,
+                    "%s sampling, 2^24 coefficients x 16 residues (bytes written)" % name, e)
+        return build
+
+    W["sample_ternary"] = sample(TERNARY, "ternary")
+    W["sample_gaussian"] = sample(GAUSSIAN, "Gaussian")
+    W["sample_uniform"] = sample(UNIFORM, "uniform mod q_i")
+    return W
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--only", default="")
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--peak", type=float, default=0.0)
+    a = ap.parse_args()
+    peak = a.peak or _peak()
+    W = workloads()
+    names = [n for n in a.only.split(",") if n] or list(W)
+    for n in names:
+        fn, byt, desc, e = W[n]()
+        ms = _time(fn, a.reps)
+        e.check()
+        gbs = byt / ms / 1e6
+        print(json.dumps({"kernel": n, "workload": desc, "ms": round(ms, 4), "bytes": byt, "GB_per_s": round(gbs, 1),
+                          "peak_GB_per_s": peak, "frac_hbm": round(gbs / peak, 4)}), flush=True)
+        del fn, e
+        torch.cuda.empty_cache()
+
+
+if __name__ == "__main__":
+    main()
