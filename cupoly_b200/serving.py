@@ -18,6 +18,14 @@ size class (its DGT/HPS tables resident in HBM) and a few preallocated batch
 
 The scheduler is host logic with a pluggable executor; `GpuExecutor` runs the
 batches through the C ABI, `FakeExecutor` (tests) completes them on a timer.
+
+Failures end requests, never the loop: a request naming no size class is
+rejected on arrival; one cancelled before its batch launches leaves the queue or
+its pool (its budget returns at once), one cancelled later completes as
+cancelled; one that waits in its queue longer than `queue_timeout_s` is
+rejected; an executor error at launch, poll or finish (a CUDA or ABI error, a
+kernel's error flag) fails that batch's requests, frees their budget and
+returns the pool to service.
 """
 from __future__ import annotations
 
@@ -61,6 +69,9 @@ class Request:
     done: float = -1.0
     slot: int = -1
     pool: int = -1
+    status: str = "pending"  # -> done | failed | cancelled | rejected
+    error: str = ""
+    cancelled: bool = False  # set by the client at any time; honoured before launch, result dropped after
 
     @property
     def latency(self) -> float:
@@ -79,17 +90,19 @@ class Pool:
 
 class Scheduler:
     def __init__(self, classes: Sequence[SizeClass], executor, budget_bytes: int, pools_per_class: int = 3,
-                 max_inflight: int = 2):
+                 max_inflight: int = 2, queue_timeout_s: Optional[float] = None):
         self.classes = list(classes)
         self.ex = executor
         self.budget = int(budget_bytes)
         self.used = 0
         self.peak_used = 0
         self.max_inflight = max_inflight
+        self.queue_timeout = queue_timeout_s
         self.pools: List[List[Pool]] = [[Pool(c, i, cl.max_batch) for i in range(pools_per_class)]
                                         for c, cl in enumerate(self.classes)]
         self.batches = 0
         self.batch_sizes: List[int] = []
+        self.failed_batches = 0
         for cl in self.classes:
             if cl.request_bytes() > self.budget:
                 raise ValueError("budget smaller than one request of nphi=%d" % cl.nphi)
@@ -105,8 +118,48 @@ class Scheduler:
                 return p
         return idle[0] if idle else None
 
+    def _end(self, r: Request, status: str, t: float, error: str = "") -> None:
+        r.status, r.done, r.error = status, t, error
+
+    def _release(self, pool: Pool, status: str, t: float, error: str = "") -> int:
+        """End every request of `pool`, free their budget, return the pool to service."""
+        rb = self.classes[pool.cls].request_bytes()
+        for r in pool.reqs:
+            self._end(r, "cancelled" if (status == "done" and r.cancelled) else status, t, error)
+            self.used -= rb
+        n = len(pool.reqs)
+        pool.reqs, pool.busy, pool.handle = [], False, None
+        return n
+
+    def _launch(self, c: int, pool: Pool, t: float) -> int:
+        """Launch `pool` after dropping its cancelled requests; returns how many requests ended."""
+        ended = 0
+        keep = [r for r in pool.reqs if not r.cancelled]
+        if len(keep) != len(pool.reqs):
+            rb = self.classes[c].request_bytes()
+            for r in pool.reqs:
+                if r.cancelled:
+                    self._end(r, "cancelled", t)
+                    self.used -= rb
+                    ended += 1
+            for i, r in enumerate(keep):
+                r.slot = i
+            pool.reqs = keep
+        if not pool.reqs:
+            return ended
+        try:
+            pool.handle = self.ex.launch(c, pool)
+        except Exception as exc:  # noqa: BLE001 -- any executor error fails this batch only
+            self.failed_batches += 1
+            return ended + self._release(pool, "failed", t, "launch: %s" % exc)
+        pool.busy = True
+        self.batches += 1
+        self.batch_sizes.append(len(pool.reqs))
+        return ended
+
     def run(self, requests: Sequence[Request], clock=time.perf_counter, time_limit_s: float = 600.0):
-        """Serve `requests` (arrival times relative to start); returns them completed."""
+        """Serve `requests` (arrival times relative to start); returns them, each ended
+        with a status (done, failed, cancelled or rejected)."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         queues = [collections.deque() for _ in self.classes]
         n, nxt, done = len(reqs), 0, 0
@@ -117,21 +170,53 @@ class Scheduler:
                 raise TimeoutError("serving loop exceeded %.0f s" % time_limit_s)
             progressed = False
             while nxt < n and reqs[nxt].arrival <= now:
-                queues[reqs[nxt].cls].append(reqs[nxt])
+                r = reqs[nxt]
                 nxt += 1
                 progressed = True
+                if not (isinstance(r.cls, int) and 0 <= r.cls < len(self.classes)):
+                    self._end(r, "rejected", now, "unknown size class %r" % (r.cls,))
+                    done += 1
+                else:
+                    queues[r.cls].append(r)
             # completions
             for c in range(len(self.classes)):
                 for p in self.pools[c]:
-                    if p.busy and self.ex.poll(p.handle):
-                        t_done = clock() - t0
-                        self.ex.finish(p)
-                        for r in p.reqs:
-                            r.done = t_done
-                            self.used -= self.classes[c].request_bytes()
-                        done += len(p.reqs)
-                        p.reqs, p.busy, p.handle = [], False, None
+                    if not p.busy:
+                        continue
+                    try:
+                        ready = self.ex.poll(p.handle)
+                    except Exception as exc:  # noqa: BLE001
+                        self.failed_batches += 1
+                        done += self._release(p, "failed", clock() - t0, "poll: %s" % exc)
                         progressed = True
+                        continue
+                    if ready:
+                        t_done = clock() - t0
+                        try:
+                            self.ex.finish(p)
+                        except Exception as exc:  # noqa: BLE001
+                            self.failed_batches += 1
+                            done += self._release(p, "failed", t_done, "finish: %s" % exc)
+                        else:
+                            done += self._release(p, "done", t_done)
+                        progressed = True
+            # queue hygiene: cancellations and queue timeouts end requests before admission
+            for q in queues:
+                if any(r.cancelled or (self.queue_timeout is not None and now - r.arrival > self.queue_timeout)
+                       for r in q):
+                    kept = collections.deque()
+                    for r in q:
+                        if r.cancelled:
+                            self._end(r, "cancelled", now)
+                            done += 1
+                        elif self.queue_timeout is not None and now - r.arrival > self.queue_timeout:
+                            self._end(r, "rejected", now, "queue timeout")
+                            done += 1
+                        else:
+                            kept.append(r)
+                    q.clear()
+                    q.extend(kept)
+                    progressed = True
             # admission and launch
             for c, cl in enumerate(self.classes):
                 q = queues[c]
@@ -148,20 +233,14 @@ class Scheduler:
                         progressed = True
                     self.peak_used = max(self.peak_used, self.used)
                     if pool.reqs and (len(pool.reqs) == pool.capacity or self._inflight(c) < self.max_inflight):
-                        pool.handle = self.ex.launch(c, pool)
-                        pool.busy = True
-                        self.batches += 1
-                        self.batch_sizes.append(len(pool.reqs))
+                        done += self._launch(c, pool, now)
                         progressed = True
                     else:
                         break
                 # a filling pool left partly full launches once an in-flight batch finishes
                 pool = self._filling(c)
                 if pool is not None and pool.reqs and self._inflight(c) < self.max_inflight:
-                    pool.handle = self.ex.launch(c, pool)
-                    pool.busy = True
-                    self.batches += 1
-                    self.batch_sizes.append(len(pool.reqs))
+                    done += self._launch(c, pool, now)
                     progressed = True
             if not progressed:
                 busy = any(p.busy for ps in self.pools for p in ps)
@@ -172,12 +251,16 @@ class Scheduler:
         return reqs
 
     def stats(self, reqs: Sequence[Request]) -> Dict:
-        lat = np.array([r.latency for r in reqs]) * 1e3
-        span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
-        return {"requests": len(reqs), "throughput_req_s": round(len(reqs) / span, 1),
+        ok = [r for r in reqs if r.status == "done"]
+        lat = np.array([r.latency for r in ok]) * 1e3 if ok else np.zeros(1)
+        span = (max(r.done for r in ok) - min(r.arrival for r in ok)) if ok else float("inf")
+        counts = collections.Counter(r.status for r in reqs)
+        return {"requests": len(reqs), "completed": len(ok), "throughput_req_s": round(len(ok) / span, 1),
                 "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
                 "max_ms": round(float(lat.max()), 3), "batches": self.batches,
                 "mean_batch": round(float(np.mean(self.batch_sizes)), 2) if self.batch_sizes else 0,
+                "failed": counts.get("failed", 0), "cancelled": counts.get("cancelled", 0),
+                "rejected": counts.get("rejected", 0), "failed_batches": self.failed_batches,
                 "peak_budget_bytes": self.peak_used, "budget_bytes": self.budget}
 
 
@@ -263,6 +346,8 @@ class GpuExecutor:
         return ev.query()
 
     def finish(self, pool):
+        # a kernel's error flag (e.g. a sampler rejection limit) fails the batch
+        self.engines[pool.cls].check(self.pool_bufs[pool.cls][pool.index]["stream"])
         if not self.keep:
             return
         b = self.pool_bufs[pool.cls][pool.index]

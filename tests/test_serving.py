@@ -99,3 +99,89 @@ def test_served_result_matches_oracle(gpu):
         got = unfold(to_u64(got))
         for j in range(3):
             assert np.array_equal(got[j], ref[j][0])
+
+
+class _Flaky(FakeExecutor):
+    """Fake executor whose launch / poll / finish raise for chosen batches (by launch order)."""
+
+    def __init__(self, delay, fail_launch=(), fail_poll=(), fail_finish=()):
+        super().__init__(delay)
+        self.fail = {"launch": set(fail_launch), "poll": set(fail_poll), "finish": set(fail_finish)}
+        self.count = 0
+        self.batch_of = {}
+
+    def launch(self, c, pool):
+        i = self.count
+        self.count += 1
+        if i in self.fail["launch"]:
+            raise RuntimeError("injected launch failure (CUDA out of memory)")
+        h = super().launch(c, pool)
+        self.batch_of[pool.index, c] = i
+        return (i, h)
+
+    def poll(self, handle):
+        i, h = handle
+        if i in self.fail["poll"]:
+            raise RuntimeError("injected poll failure")
+        return super().poll(h)
+
+    def finish(self, pool):
+        if self.batch_of[pool.index, pool.cls] in self.fail["finish"]:
+            raise RuntimeError("injected kernel error flag")
+
+
+def test_executor_failures_fail_only_their_batch():
+    """A launch, poll or finish error ends that batch's requests as failed, frees their
+    budget and leaves the loop serving everyone else."""
+    cls = [SizeClass(4096, 2, 3, 256, 4)]
+    ex = _Flaky(lambda c, b: 0.001, fail_launch=[1], fail_poll=[3], fail_finish=[5])
+    sch = Scheduler(cls, ex, budget_bytes=10 ** 12, max_inflight=1)
+    reqs = sch.run([Request(i, 0, 0.0005 * i) for i in range(80)])
+    st = sch.stats(reqs)
+    assert st["failed_batches"] == 3 and st["failed"] > 0
+    assert st["failed"] + st["completed"] == 80
+    assert all(r.status in ("done", "failed") for r in reqs)
+    assert all(r.error for r in reqs if r.status == "failed")
+    assert sch.used == 0  # every reservation returned
+    assert {r.error.split(":")[0] for r in reqs if r.status == "failed"} == {"launch", "poll", "finish"}
+
+
+def test_malformed_and_cancelled_requests():
+    """A request naming no size class is rejected on arrival; one cancelled before its
+    batch launches never reaches the executor; one cancelled after launch completes as
+    cancelled; the budget is whole again at the end."""
+    cls = [SizeClass(4096, 2, 3, 256, 4)]
+    reqs = [Request(i, 0, 0.0002 * i) for i in range(30)]
+    reqs[3].cls = 9
+    reqs[5].cancelled = True
+    reqs[6].cancelled = True
+
+    class CancelOnLaunch(FakeExecutor):
+        def launch(self, c, pool):
+            for r in pool.reqs:
+                if r.rid == 20:
+                    r.cancelled = True  # the client gives up while its batch runs
+            return super().launch(c, pool)
+
+    ex = CancelOnLaunch(lambda c, b: 0.002)
+    sch = Scheduler(cls, ex, budget_bytes=10 ** 12)
+    out = {r.rid: r for r in sch.run(reqs)}
+    assert out[3].status == "rejected" and "size class" in out[3].error
+    assert out[5].status == out[6].status == "cancelled"
+    launched = {rid for _, _, rids in ex.launched for rid in rids}
+    assert 5 not in launched and 6 not in launched and 3 not in launched
+    assert 20 in launched and out[20].status == "cancelled"
+    assert sum(r.status == "done" for r in out.values()) == 26
+    assert sch.used == 0
+
+
+def test_queue_timeout_rejects_requests_that_wait_too_long():
+    cls = [SizeClass(4096, 2, 3, 256, 1)]
+    ex = FakeExecutor(lambda c, b: 0.01)
+    budget = cls[0].request_bytes()  # one request at a time
+    sch = Scheduler(cls, ex, budget_bytes=budget, max_inflight=1, queue_timeout_s=0.025)
+    reqs = sch.run([Request(i, 0, 0.0) for i in range(10)])
+    st = sch.stats(reqs)
+    assert st["rejected"] > 0 and st["completed"] >= 2
+    assert all(r.error == "queue timeout" for r in reqs if r.status == "rejected")
+    assert sch.peak_used <= budget and sch.used == 0
