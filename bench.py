@@ -358,6 +358,37 @@ def run_ours(args, D: Dist):
     e2e_ms = D.max(ev0.elapsed_time(ev1))
     h2d = sum(h.numel() * 8 for h in hin[0])
     d2h = hout[0].numel() * 8
+    # the host link alone: one step's copies in, out, and both at once (pinned memory)
+    s_a, s_b = torch.cuda.Stream(), torch.cuda.Stream()
+    dev_in = sb.bufs[0]["ins"]
+    dev_out = sb.bufs[0]["out"]
+
+    def link(copy_in: bool, copy_out: bool, reps: int = 5) -> float:
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s_a.wait_stream(stream)
+        s_b.wait_stream(stream)
+        for _ in range(reps):
+            if copy_in:
+                with torch.cuda.stream(s_a):
+                    for d, h in zip(dev_in, hin[0]):
+                        d.copy_(h, non_blocking=True)
+            if copy_out:
+                with torch.cuda.stream(s_b):
+                    hout[0].copy_(dev_out, non_blocking=True)
+        stream.wait_stream(s_a)
+        stream.wait_stream(s_b)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    t_in, t_out, t_both = link(True, False), link(False, True), link(True, True)
+    pcie = {"h2d_GB_per_s": round(h2d / t_in / 1e6, 1), "d2h_GB_per_s": round(d2h / t_out / 1e6, 1),
+            "both_ms_per_step": round(t_both, 3),
+            "bound_hom_mul_per_s": round(P / (max(t_both, ms / args.steps) / 1e3), 1),
+            "note": "one step's input copies (pinned host -> device) and output copy, alone and at once; "
+                    "the bound is the slower of the concurrent copies and the device step"}
     del sb
 
     # ---- plain per-call form: one cp_bfv_mul per pair ----
@@ -600,7 +631,7 @@ def run_ours(args, D: Dist):
                        "kl": K_B, "t": T_PLAIN, "parallelism": "replicas x%d" % D.world,
                        "l2": "inputs larger than L2 (%.0f MB read per step)" % (4 * P * K_Q * e.N * 16 / 1e6)},
             "e2e": {"value": round(D.world * P * args.steps / (e2e_ms / 1e3), 2), "unit": "hom-mul/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "host_link": pcie},
             "plain": {"value": round(plain_value, 2), "unit": "hom-mul/s",
                       "form": "one cp_bfv_mul call per pair (cuPoly's per-call composition)", "pairs": PP},
             "batched_over_plain": round(value / D.world / plain_value, 2),

@@ -87,6 +87,7 @@ SIGNATURES = {
     "cp_bfv_mul_batch_workspace_bytes": (C.c_size_t, [_vp, _i]),
     "cp_bfv_mul_batch": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
     "cp_calibrate_int": (_i, [_i, _i, _vp, C.c_longlong, C.POINTER(C.c_float), _vp]),
+    "cp_modarith_eval": (_i, [_i, _vp, _vp, _vp, _vp, C.c_longlong, C.c_uint64, _vp]),
     "cp_crt": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp]),
     "cp_icrt": (_i, [_vp, _vp, _i, _vp, _i, _i, _vp]),
     "cp_wire_bytes": (C.c_size_t, [_vp, _i, _i]),

@@ -151,36 +151,38 @@ class StreamedBFV:
     Each batch is four pinned host tensors (npairs, k, N, 2) in the DGT domain and
     its result a pinned host tensor (3 npairs, k, N, 2).  Three CUDA streams run
     the host-to-device copy of batch i + 1, the chain on batch i and the
-    device-to-host copy of batch i - 1 at the same time (two device buffer
-    sets), so throughput is bound by the slowest of the three instead of their
-    sum.
+    device-to-host copy of batch i - 1 at the same time over `nbuf` device buffer
+    sets, so throughput is bound by the slowest of the three instead of their
+    sum.  A copy-in waits only for the chain that last read its input buffers,
+    and a chain only for the copy-out that last read its output buffer.
     """
 
-    def __init__(self, engine: Engine, npairs: int):
+    def __init__(self, engine: Engine, npairs: int, nbuf: int = 3):
         self.e = engine
         self.P = npairs
+        self.nbuf = nbuf
         self.bufs = [{"ins": [engine.empty(QBase, npairs) for _ in range(4)],
-                      "out": engine.empty(QBase, 3 * npairs)} for _ in range(2)]
+                      "out": engine.empty(QBase, 3 * npairs)} for _ in range(nbuf)]
         self.ws = engine.bfv_mul_batch_workspace(npairs)
         self.s_in, self.s_comp, self.s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
-        self.ev_in = [torch.cuda.Event() for _ in range(2)]
-        self.ev_comp = [torch.cuda.Event() for _ in range(2)]
-        self.ev_out = [torch.cuda.Event() for _ in range(2)]
-        self.ev_used = [torch.cuda.Event() for _ in range(2)]
+        self.ev_in = [torch.cuda.Event() for _ in range(nbuf)]
+        self.ev_comp = [torch.cuda.Event() for _ in range(nbuf)]
+        self.ev_out = [torch.cuda.Event() for _ in range(nbuf)]
 
     def run(self, host_batches, host_outputs):
         """host_batches[i] = [a0, a1, b0, b1] (pinned); host_outputs[i] receives c."""
         for i, (hin, hout) in enumerate(zip(host_batches, host_outputs)):
-            b = i & 1
+            b = i % self.nbuf
             buf = self.bufs[b]
-            if i >= 2:  # buffer set b: inputs consumed by step i - 2, output copied out
-                self.s_in.wait_event(self.ev_used[b])
+            reuse = i >= self.nbuf
+            if reuse:  # input buffers of set b were last read by the chain of step i - nbuf
+                self.s_in.wait_event(self.ev_comp[b])
             with torch.cuda.stream(self.s_in):
                 for d, h in zip(buf["ins"], hin):
                     d.copy_(h, non_blocking=True)
                 self.ev_in[b].record(self.s_in)
             self.s_comp.wait_event(self.ev_in[b])
-            if i >= 2:
+            if reuse:  # output buffer of set b was last read by the copy-out of step i - nbuf
                 self.s_comp.wait_event(self.ev_out[b])
             self.e.bfv_mul_batch(buf["out"], *buf["ins"], self.P, self.ws, stream=self.s_comp)
             self.ev_comp[b].record(self.s_comp)
@@ -188,7 +190,6 @@ class StreamedBFV:
             with torch.cuda.stream(self.s_out):
                 hout.copy_(buf["out"], non_blocking=True)
                 self.ev_out[b].record(self.s_out)
-                self.ev_used[b].record(self.s_out)
 
     def join(self, stream):
         """Make `stream` wait for everything issued so far."""

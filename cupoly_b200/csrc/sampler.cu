@@ -119,33 +119,29 @@ __global__ void __launch_bounds__(256) k_sample(ulonglong2* __restrict__ out, co
   const uint32_t sid = ids ? ids[blockIdx.y] : sid0 + blockIdx.y;
   out += blockIdx.y * poly_stride;
   if (kind == UNIFORM) {
+    // one Philox block per draw serves both coefficients of element j: words 0-1 are
+    // the candidate for coefficient j, words 2-3 for j + N; each keeps its first
+    // candidate below p (candidates of bitlen(p) bits: every prime of the tables lies
+    // within 0.01 % below its power of two, so a draw is accepted with p > 0.9999)
     for (int r = 0; r < nres; ++r) {
       const uint64_t p = mc[rid_off + r].p;
-      // candidates of bitlen(p) bits: every prime of the tables lies within 0.01 % below
-      // its power of two, so a candidate is accepted with probability > 0.9999
       const uint64_t mask = ~0ull >> __clzll((long long)p);
-      uint64_t val[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const uint32_t c = (uint32_t)(j + h * N);
-        bool ok = false;
-        for (uint32_t d = 0; d < 8 && !ok; ++d) {
-          const Philox q = philox4x32_10(c, (uint32_t)r * 8u + d, sid, (uint32_t)kind, k0, k1);
-          const uint64_t u0 = (((uint64_t)q.v[1] << 32) | q.v[0]) & mask;
-          const uint64_t u1 = (((uint64_t)q.v[3] << 32) | q.v[2]) & mask;
-          if (u0 < p) {
-            val[h] = u0;
-            ok = true;
-          } else if (u1 < p) {
-            val[h] = u1;
-            ok = true;
-          }
+      uint64_t val[2] = {0, 0};
+      bool ok0 = false, ok1 = false;
+      for (uint32_t d = 0; d < 16 && !(ok0 && ok1); ++d) {
+        const Philox q = philox4x32_10((uint32_t)j, (uint32_t)r * 16u + d, sid, (uint32_t)kind, k0, k1);
+        const uint64_t u0 = (((uint64_t)q.v[1] << 32) | q.v[0]) & mask;
+        const uint64_t u1 = (((uint64_t)q.v[3] << 32) | q.v[2]) & mask;
+        if (!ok0 && u0 < p) {
+          val[0] = u0;
+          ok0 = true;
         }
-        if (!ok) {
-          atomicExch(err, 1);
-          val[h] = 0;
+        if (!ok1 && u1 < p) {
+          val[1] = u1;
+          ok1 = true;
         }
       }
+      if (!(ok0 && ok1)) atomicExch(err, 1);
       out[(size_t)r * N + j] = make_ulonglong2(val[0], val[1]);
     }
     return;

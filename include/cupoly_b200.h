@@ -211,6 +211,21 @@ int cp_bfv_mul_batch(const cp_engine* e, void* c, const void* a0, const void* a1
  *      3 32-bit multiply-add.  sink: nthreads uint64 of device memory. ---- */
 int cp_calibrate_int(int kind, int iters, void* sink, long long nthreads, float* ms, void* stream);
 
+/* ---- the modular primitives, elementwise (no counterpart in cuPoly's API; its tests call the
+ *      device functions directly: TestDGT.{mod, addmod, submod, mulmod, powmod, GIAdd, GISub,
+ *      GIMul}, tests/unit_tests/test_bfv_mode.cu:243-438).  Device arrays of n words (GI ops:
+ *      n elements of two words); p odd, 3 <= p < 2^63.  Operand ranges as the kernels use them:
+ *      ADD / SUB a, b < p; NEG a < p; MULMOD a < p, any b; SHOUP any a, b < p,
+ *      c = floor(b 2^64 / p); RED128 (a = high word, b = low word) < min(2^127, p 2^64);
+ *      POW a < p, exponent b; GIMUL a, b < p; GIMUL_CONST3 a < p, b < p the constant, c three Shoup
+ *      companions per element of (w_re, w_im - w_re, w_re + w_im). ---- */
+enum cp_modop {
+  CP_MODOP_ADD = 0, CP_MODOP_SUB = 1, CP_MODOP_NEG = 2, CP_MODOP_MULMOD = 3, CP_MODOP_SHOUP = 4,
+  CP_MODOP_RED128 = 5, CP_MODOP_POW = 6, CP_MODOP_GIMUL = 7, CP_MODOP_GIMUL_CONST3 = 8
+};
+int cp_modarith_eval(int op, const uint64_t* a, const uint64_t* b, const uint64_t* c, uint64_t* out, long long n,
+                     uint64_t p, void* stream);
+
 /* ---- CKKS operations (CKKS engines only), DGT domain in and out, level l in [0, k)
  *      (rescale: [1, k)); Q_l = q_0 ... q_l.  They replace fast_conv_Q_to_B /
  *      fast_conv_B_to_Q / ckks_rescale / xi_ckks_rns_rid / rho_ckks_rns_rid

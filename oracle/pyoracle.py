@@ -638,19 +638,21 @@ def sample_small(kind, c, sid, seed):
     raise ValueError(kind)
 
 
-def sample_uniform(c, r, p, sid, seed):
-    """Uniform residue mod p of coefficient c in residue r: rejection on candidates of
-    bitlen(p) bits (63 for the BFV primes, 45..55 for the CKKS buckets)."""
+def sample_uniform_pair(j, r, p, sid, seed):
+    """Uniform residues mod p of coefficients j and j + N (Gaussian element j) in residue r:
+    draw d = 0, 1, ... gives one candidate of bitlen(p) bits for each coefficient (words 0-1
+    for j, words 2-3 for j + N); each coefficient keeps its first candidate below p."""
     k0, k1 = seed & _M, (seed >> 32) & _M
     mask = (1 << p.bit_length()) - 1
-    for d in range(8):
-        q = philox4x32_10((c, r * 8 + d, sid, UNIFORM), (k0, k1))
-        u0 = ((q[1] << 32) | q[0]) & mask
-        u1 = ((q[3] << 32) | q[2]) & mask
-        if u0 < p:
-            return u0
-        if u1 < p:
-            return u1
+    v = [None, None]
+    for d in range(16):
+        q = philox4x32_10((j, r * 16 + d, sid, UNIFORM), (k0, k1))
+        u = (((q[1] << 32) | q[0]) & mask, ((q[3] << 32) | q[2]) & mask)
+        for h in (0, 1):
+            if v[h] is None and u[h] < p:
+                v[h] = u[h]
+        if v[0] is not None and v[1] is not None:
+            return v
     raise RuntimeError("rejection limit")
 
 
@@ -677,7 +679,12 @@ def sample_poly(kind, primes, nphi, sid, seed, ckks=False):
         kind = {NARROW: TERNARY, DISCRETE_GAUSSIAN: SIGNED_DG}.get(kind, kind)
     rows = []
     if kind == UNIFORM:
-        return [[sample_uniform(c, r, p, sid, seed) for c in range(nphi)] for r, p in enumerate(primes)]
+        N = nphi // 2
+        rows = []
+        for r, p in enumerate(primes):
+            pairs = [sample_uniform_pair(j, r, p, sid, seed) for j in range(N)]
+            rows.append([v[0] for v in pairs] + [v[1] for v in pairs])
+        return rows
     if kind == HAMMINGWEIGHT:
         hw = sample_hamming(nphi, sid, seed)
         vals = [hw.get(c, 0) for c in range(nphi)]

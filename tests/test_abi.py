@@ -63,3 +63,15 @@ def test_status_error_raises():
     with pytest.raises(_lib.CupolyError) as ei:
         _lib.call("cp_add", None, None, None, None, 0, None)
     assert ei.value.code == 1
+
+
+def test_modarith_eval_checks_arguments_before_any_cuda_call():
+    L = _lib.lib()
+    buf = (C.c_uint64 * 4)()
+    p = 9223372036801560577
+    assert L.cp_modarith_eval(99, buf, buf, None, buf, 4, p, None) == 1          # unknown op
+    assert L.cp_modarith_eval(0, buf, buf, None, buf, 4, p + 1, None) == 1       # even modulus
+    assert L.cp_modarith_eval(0, buf, buf, None, buf, 4, 2 ** 63 + 1, None) == 1  # modulus >= 2^63
+    assert L.cp_modarith_eval(4, buf, buf, None, buf, 4, p, None) == 1           # SHOUP without companions
+    assert "missing operand" in L.cp_last_error().decode()
+    assert L.cp_modarith_eval(0, buf, buf, None, buf, 0, p, None) == 0           # nothing to do
