@@ -18,6 +18,11 @@ Workloads (names for --only):
   crt, icrt          coefficient limbs <-> residues, nphi 8192, k 5, 512 polynomials
   sample_ternary, sample_gaussian, sample_uniform
                      2^24 coefficients x 16 residues (nphi 32768, k 16, 512 polynomials)
+  bfv_chain, bfv_chain_target, bfv_chain_large
+                     the batched BFV multiplication chain (cp_bfv_mul_batch) at nphi 8192 / k 5 /
+                     128 pairs, nphi 16384 / k 10 / 32 pairs and nphi 32768 / k 16 / t 65537 / 64
+                     pairs; bytes = 4 operands read + 3 results written over Q per pair (the
+                     algorithmic bytes of one homomorphic multiplication)
 """
 from __future__ import annotations
 
@@ -138,6 +143,21 @@ def workloads():
                     "%s sampling, 2^24 coefficients x 16 residues (bytes written)" % name, e)
         return build
 
+    def chain(nphi, k, t, P):
+        def build():
+            e = Engine(k, k + 1, nphi, t)
+            ins = [e.empty(QBase, P) for _ in range(4)]
+            for v, x in enumerate(ins):
+                e.sample(x, QBase, UNIFORM, 8, v * P, npolys=P, to_dgt=True)
+            c = e.empty(QBase, 3 * P)
+            ws = e.bfv_mul_batch_workspace(P)
+            return (lambda: e.bfv_mul_batch(c, *ins, P, ws), P * 7 * k * e.N * 16,
+                    "batched BFV multiplication, nphi %d, k %d, kl %d, t %d, %d pairs per call" % (nphi, k, k + 1, t, P), e)
+        return build
+
+    W["bfv_chain"] = chain(8192, 5, 256, 128)
+    W["bfv_chain_target"] = chain(16384, 10, 256, 32)
+    W["bfv_chain_large"] = chain(32768, 16, 65537, 64)
     W["sample_ternary"] = sample(TERNARY, "ternary")
     W["sample_gaussian"] = sample(GAUSSIAN, "Gaussian")
     W["sample_uniform"] = sample(UNIFORM, "uniform mod q_i")
