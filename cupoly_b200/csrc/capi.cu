@@ -181,9 +181,21 @@ int cp_engine_set_plan(cp_engine* h, int log_radix, int log_cta) {
   CP_REQUIRE(e.logN - (e.logN < lc ? e.logN : lc) <= 2, "cp_engine_set_plan: at most 2 split bits (log N - log_cta)");
   cudaDeviceSynchronize();
   free_tables(e);
+  const int cluster = e.plan.cluster;  // the split-stage form survives a plan change
   e.plan = make_plan(e.logN, log_radix ? log_radix : 3, lc);
+  e.plan.cluster = cluster;
   return build_tables(e);
 }
+
+int cp_engine_set_split_mode(cp_engine* h, int mode) {
+  CP_REQUIRE(h, "cp_engine_set_split_mode: NULL engine");
+  CP_REQUIRE(mode == 0 || mode == 1, "cp_engine_set_split_mode: mode must be 0 (split kernel) or 1 (cluster)");
+  cudaDeviceSynchronize();  // transforms in flight keep the form they were launched with
+  h->e.plan.cluster = mode;
+  return CP_OK;
+}
+
+int cp_engine_get_split_mode(const cp_engine* h) { return h ? h->e.plan.cluster : -1; }
 
 int cp_engine_get_plan(const cp_engine* h, int* log_radix, int* log_cta, int* split_bits) {
   CP_REQUIRE(h, "cp_engine_get_plan: NULL engine");

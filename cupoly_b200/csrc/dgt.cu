@@ -62,6 +62,84 @@ int run_cta(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const Inv
 using RunFn = int (*)(const Engine&, ulonglong2*, const ulonglong2*, const InvSrc&, int, int, int, long long, bool,
                       bool, cudaStream_t, const int*);
 
+constexpr int kNoCluster = -1;  // the cluster form cannot be scheduled on this device: use the split kernel
+
+// Transform with the split stage inside a thread-block cluster of 2^CL CTAs (one CTA
+// per unit: the cluster's CTAs are the chunks of one residue).  Returns kNoCluster,
+// having launched nothing, when the device cannot co-schedule such a cluster.
+template <int LOGNC, int LOGR, int CL>
+int run_cluster(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres,
+                int rid_off, int npolys, long long poly_stride, bool inverse, bool, cudaStream_t st,
+                const int* rid_list) {
+  constexpr int T = (1 << LOGNC) >> LOGR;
+  constexpr int smem = dgt_smem_bytes<LOGNC, LOGR>();
+  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc, rid_list};
+  const long long blocks = (long long)npolys * nres << CL;
+  if (blocks <= 0) return 0;
+  if (blocks > 0x7fffffffLL) {
+    set_error("dgt: grid too large");
+    return 1;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)blocks);
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 1u << CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  static std::atomic<unsigned long long> done_f{0}, done_i{0};
+  static std::atomic<int> ok_f{0}, ok_i{0};  // 0 unknown, 1 schedulable, -1 not
+  auto schedulable = [&](auto kernel, std::atomic<int>& ok) {
+    int v = ok.load();
+    if (v == 0) {
+      int n = 0;
+      const cudaError_t err = cudaOccupancyMaxActiveClusters(&n, kernel, &cfg);
+      v = (err == cudaSuccess && n > 0) ? 1 : -1;
+      if (err != cudaSuccess) cudaGetLastError();  // clear the sticky-free error of the query
+      ok.store(v);
+    }
+    return v > 0;
+  };
+  cudaError_t err;
+  if (!inverse) {
+    if (int rc = ensure_smem(k_dgt_fwd<LOGNC, LOGR, CL>, smem, done_f)) return rc;
+    if (!schedulable(k_dgt_fwd<LOGNC, LOGR, CL>, ok_f)) return kNoCluster;
+    err = cudaLaunchKernelEx(&cfg, k_dgt_fwd<LOGNC, LOGR, CL>, data, fsrc, A, nres, rid_off, poly_stride, CL, 1,
+                             (unsigned)blocks);
+  } else {
+    if (int rc = ensure_smem(k_dgt_inv<LOGNC, LOGR, CL>, smem, done_i)) return rc;
+    if (!schedulable(k_dgt_inv<LOGNC, LOGR, CL>, ok_i)) return kNoCluster;
+    err = cudaLaunchKernelEx(&cfg, k_dgt_inv<LOGNC, LOGR, CL>, data, isrc, A, nres, rid_off, poly_stride, CL, 0,
+                             (unsigned)blocks);
+  }
+  if (err != cudaSuccess) return cuda_fail("dgt (cluster)", err);
+  return check_launch("dgt (cluster)");
+}
+
+// (logNc, logR, split bits) -> cluster instantiation, or nullptr.
+RunFn pick_cluster(int logNc, int logR, int S) {
+#define CP_CASE(A, B, C) \
+  if (logNc == A && logR == B && S == C) return &run_cluster<A, B, C>;
+  CP_CASE(11, 3, 1) CP_CASE(11, 3, 2) CP_CASE(12, 3, 1) CP_CASE(12, 3, 2) CP_CASE(13, 3, 1) CP_CASE(13, 3, 2)
+#undef CP_CASE
+  return nullptr;
+}
+
+// The plan's split stage inside a cluster, when the plan asks for it and a kernel exists;
+// returns kNoCluster otherwise (nothing launched).
+int try_cluster(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres, int rid_off,
+                int npolys, long long poly_stride, bool inverse, cudaStream_t st, const int* rid_list) {
+  if (!e.plan.cluster || e.plan.S == 0) return kNoCluster;
+  RunFn fc = pick_cluster(e.plan.logNc, e.plan.logR, e.plan.S);
+  if (!fc) return kNoCluster;
+  return fc(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, inverse, false, st, rid_list);
+}
+
 // (logNc, effective logR) -> instantiation.
 RunFn pick(int logNc, int logR) {
 #define CP_CASE(A, B) \
@@ -128,6 +206,10 @@ int launch_dgt_ex(const Engine& e, void* dst_v, const void* fsrc_v, const InvSrc
     isrc.npairs = 1;
   }
   const int S = e.plan.S;
+  {
+    const int rc = try_cluster(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, inverse, st, nullptr);
+    if (rc != kNoCluster) return rc;
+  }
   if (!inverse) {
     if (S > 0) {
       int rc = launch_split(e, data, fsrc, nres, rid_off, npolys, poly_stride, false, st);
@@ -158,6 +240,10 @@ int launch_dgt_part(const Engine& e, void* dst_v, const void* src_v, int rid_off
   isrc.mode = 0;
   isrc.npairs = 1;
   const int S = e.plan.S;
+  {
+    const int rc = try_cluster(e, data, src, isrc, nres, rid_off, npolys, poly_stride, inverse, st, nullptr);
+    if (rc != kNoCluster) return rc;
+  }
   if (!inverse) {
     if (S > 0) {
       int rc = launch_split(e, data, src, nres, rid_off, npolys, poly_stride, false, st);
@@ -205,6 +291,10 @@ int launch_dgt_list_ex(const Engine& e, void* data_v, const void* fsrc_v, const 
   }
   const long long stride = e.N;
   const int S = e.plan.S;
+  {
+    const int rc = try_cluster(e, data, fsrc, isrc, 1, 0, nlist, stride, inverse, st, rid_list);
+    if (rc != kNoCluster) return rc;
+  }
   if (!inverse) {
     if (S > 0) {
       int rc = launch_split(e, data, fsrc, 1, 0, nlist, stride, false, st, rid_list);

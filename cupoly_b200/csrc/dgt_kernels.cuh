@@ -20,6 +20,7 @@
 // first (forward) or last (inverse) and the CTA kernel handles the
 // 2^S sub-transforms.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "engine.cuh"
@@ -212,6 +213,128 @@ __device__ __forceinline__ void inv_passes(ulonglong2* sdat, const ulonglong2* s
   }
 }
 
+// Split stage inside a thread-block cluster of 2^CL CTAs (one per chunk of 2^LOGNC
+// elements of one residue).  Forward: every CTA holds its chunk of the twisted input
+// in shared memory; the radix-2^CL DIF over the chunks runs at the positions
+// [h SPAN, (h + 1) SPAN) owned by CTA h, reading each chunk's element from its
+// owner's shared memory and writing output chunk `pos` back into CTA pos's shared
+// memory (distributed shared memory), with the split twiddles -- the arithmetic of
+// k_dgt_split, without its HBM pass.  Every thread reads and then rewrites the
+// same slot of every peer, and no other thread touches that slot, so the only
+// ordering needed is the cluster barrier on each side.
+template <int LOGNC, int LOGR, int CL>
+__device__ __forceinline__ void cluster_split_fwd(ulonglong2* sdat, int h, const ulonglong2* tab,
+                                                  const DgtTableLayout& L, uint64_t p) {
+  namespace cg = cooperative_groups;
+  constexpr int K = 1 << CL, NC = 1 << LOGNC, T = NC >> LOGR, SPAN = NC / K, R = 1 << LOGR;
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();  // every chunk twisted and in place
+  ulonglong2* peer[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) peer[q] = cl.map_shared_rank(sdat, q);
+  for (int t = threadIdx.x; t < SPAN; t += T) {
+    const int Lw = h * SPAN + t;
+    uint64_t xr[K], xi[K];
+#pragma unroll
+    for (int hh = 0; hh < K; ++hh) {
+      const ulonglong2 a = peer[hh][pad16(Lw)];
+      xr[hh] = a.x;
+      xi[hh] = a.y;
+    }
+#pragma unroll
+    for (int s = 0; s < CL; ++s) {
+      const int m = K >> (s + 1);
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if ((i & m) == 0) {
+          const int j = i & (m - 1);
+          const uint64_t ar = xr[i], ai = xi[i], br = xr[i + m], bi = xi[i + m];
+          xr[i] = add_mod(ar, br, p);
+          xi[i] = add_mod(ai, bi, p);
+          if (j == 0) {
+            xr[i + m] = sub_mod(ar, br, p);
+            xi[i + m] = sub_mod(ai, bi, p);
+          } else {
+            const ulonglong2 w = __ldg(tab + L.off_rad + ((j << s) * (R >> CL)));
+            xr[i + m] = shoup_mul(ar + p - br, w.x, w.y, p);
+            xi[i + m] = shoup_mul(ai + p - bi, w.x, w.y, p);
+          }
+        }
+    }
+#pragma unroll
+    for (int pos = 0; pos < K; ++pos) {
+      uint64_t ar = xr[pos], ai = xi[pos];
+      if (pos) {
+        const ulonglong2 w = __ldg(tab + L.off_split_fwd + pos * NC + Lw);
+        ar = shoup_mul(ar, w.x, w.y, p);
+        ai = shoup_mul(ai, w.x, w.y, p);
+      }
+      peer[pos][pad16(Lw)] = make_ulonglong2(ar, ai);
+    }
+  }
+  cl.sync();  // every position transformed before the in-CTA passes read them
+}
+
+// Inverse: every CTA holds its chunk's sub-transform output in shared memory; CTA h
+// combines the chunks at its positions (split twiddles, radix-2^CL DIT, untwist, as
+// k_dgt_split) and writes the results to global memory at xg[Lw + hh 2^LOGNC].  The
+// closing barrier keeps every CTA's shared memory alive until its peers have read it.
+template <int LOGNC, int LOGR, int CL>
+__device__ __forceinline__ void cluster_split_inv(ulonglong2* sdat, int h, const ulonglong2* tab,
+                                                  const DgtTableLayout& L, uint64_t p, ulonglong2* xg) {
+  namespace cg = cooperative_groups;
+  constexpr int K = 1 << CL, NC = 1 << LOGNC, T = NC >> LOGR, SPAN = NC / K, R = 1 << LOGR;
+  cg::cluster_group cl = cg::this_cluster();
+  cl.sync();  // every chunk's sub-transform in place
+  const ulonglong2* peer[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) peer[q] = cl.map_shared_rank(sdat, q);
+  for (int t = threadIdx.x; t < SPAN; t += T) {
+    const int Lw = h * SPAN + t;
+    uint64_t xr[K], xi[K];
+#pragma unroll
+    for (int pos = 0; pos < K; ++pos) {
+      const ulonglong2 a = peer[pos][pad16(Lw)];
+      uint64_t ar = a.x, ai = a.y;
+      if (pos) {
+        const ulonglong2 w = __ldg(tab + L.off_split_inv + pos * NC + Lw);
+        ar = shoup_mul(ar, w.x, w.y, p);
+        ai = shoup_mul(ai, w.x, w.y, p);
+      }
+      xr[pos] = ar;
+      xi[pos] = ai;
+    }
+#pragma unroll
+    for (int s = CL - 1; s >= 0; --s) {
+      const int m = K >> (s + 1);
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if ((i & m) == 0) {
+          const int j = i & (m - 1);
+          const uint64_t ar = xr[i], ai = xi[i];
+          uint64_t br = xr[i + m], bi = xi[i + m];
+          if (j != 0) {
+            const ulonglong2 w = __ldg(tab + L.off_rad + R - ((j << s) * (R >> CL)));
+            br = shoup_mul(br, w.x, w.y, p);
+            bi = shoup_mul(bi, w.x, w.y, p);
+          }
+          xr[i] = add_mod(ar, br, p);
+          xi[i] = add_mod(ai, bi, p);
+          xr[i + m] = sub_mod(ar, br, p);
+          xi[i + m] = sub_mod(ai, bi, p);
+        }
+    }
+#pragma unroll
+    for (int hh = 0; hh < K; ++hh) {
+      const int n = Lw + hh * NC;
+      uint64_t ar = xr[hh], ai = xi[hh];
+      gi_mul_const3(ar, ai, tab + L.off_untwist + 3 * n, p);
+      xg[n] = make_ulonglong2(ar, ai);
+    }
+  }
+  cl.sync();
+}
+
 // Shared-memory bytes of one CTA.
 template <int LOGNC, int LOGR>
 constexpr int dgt_smem_bytes() {
@@ -231,7 +354,10 @@ constexpr int dgt_min_blocks() {
   return b < 1 ? 1 : (b > 16 ? 16 : b);
 }
 
-template <int LOGNC, int LOGR>
+// CL > 0: the split stage of 2^CL chunks runs inside the kernel's thread-block
+// cluster (launched with cluster dimension 2^CL, one CTA per unit, S = CL); the
+// input is read untwisted and the twist applied here (cluster_split_fwd).
+template <int LOGNC, int LOGR, int CL = 0>
 __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
     k_dgt_fwd(ulonglong2* __restrict__ data, const ulonglong2* __restrict__ src_base, DgtArgs A, int nres,
               int rid_off, long long poly_stride, int S, int twist, unsigned nunits) {
@@ -263,6 +389,16 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   for (int j = tid; j < R; j += T) srad[j] = tab[A.L.off_rad + j];
   stage_twiddles<LOGNC, LOGR>(stw, tab, A.L.off_fwd);
   __syncthreads();
+  if constexpr (CL > 0) {  // chunk h of the twisted input, then the split stage across the cluster
+    const int h = (int)(ub & ((1u << CL) - 1));
+    for (int j = tid; j < NC; j += T) {
+      const ulonglong2 a = xs[j];
+      uint64_t ar = a.x, ai = a.y;
+      gi_mul_const3(ar, ai, tab + A.L.off_twist + 3 * ((size_t)j + ((size_t)h << LOGNC)), p);
+      sdat[pad16(j)] = make_ulonglong2(ar, ai);
+    }
+    cluster_split_fwd<LOGNC, LOGR, CL>(sdat, h, tab, A.L, p);
+  }
   {
     constexpr int W = C::W0, PF = LOGNC - C::W0, G = 1 << (LOGR - C::W0);
     uint64_t xr[R], xi[R];
@@ -272,9 +408,9 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
 #pragma unroll
       for (int v = 0; v < (1 << W); ++v) {
         const int idx = Lw + (v << PF);
-        const ulonglong2 a = xs[idx];
+        const ulonglong2 a = CL > 0 ? sdat[pad16(idx)] : xs[idx];
         uint64_t ar = a.x, ai = a.y;
-        if (twist) gi_mul_const3(ar, ai, tab + A.L.off_twist + 3 * idx, p);
+        if (CL == 0 && twist) gi_mul_const3(ar, ai, tab + A.L.off_twist + 3 * idx, p);
         xr[g * (1 << W) + v] = ar;
         xi[g * (1 << W) + v] = ai;
       }
@@ -326,7 +462,9 @@ __device__ __forceinline__ ulonglong2 tensor_load(const InvSrc& s, int j, size_t
 // In tensor mode (src.mode 1) the CTAs of c0, c1, c2 of one (pair, residue)
 // are adjacent, so each operand residue is fetched from HBM once and served
 // from L2 to the other outputs.
-template <int LOGNC, int LOGR>
+// CL > 0: as k_dgt_fwd, the split stage (twiddles, radix-2^CL DIT, untwist) runs
+// inside the cluster after the in-CTA passes (cluster_split_inv).
+template <int LOGNC, int LOGR, int CL = 0>
 __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, LOGR>()))
     k_dgt_inv(ulonglong2* __restrict__ data, InvSrc src, DgtArgs A, int nres, int rid_off, long long poly_stride,
               int S, int untwist, unsigned nunits) {
@@ -437,11 +575,17 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
       for (int v = 0; v < (1 << W); ++v) {
         const int idx = Lw + (v << PF);
         uint64_t ar = xr[v], ai = xi[v];
-        if (untwist) gi_mul_const3(ar, ai, tab + A.L.off_untwist + 3 * idx, p);
-        x[idx] = make_ulonglong2(ar, ai);
+        if constexpr (CL > 0) {
+          sdat[pad16(idx)] = make_ulonglong2(ar, ai);  // each thread rewrites the slots it read
+        } else {
+          if (untwist) gi_mul_const3(ar, ai, tab + A.L.off_untwist + 3 * idx, p);
+          x[idx] = make_ulonglong2(ar, ai);
+        }
       }
     }
   }
+  if constexpr (CL > 0)
+    cluster_split_inv<LOGNC, LOGR, CL>(sdat, h, tab, A.L, p, data + poly * poly_stride + ((size_t)r << (LOGNC + CL)));
   __syncthreads();  // shared memory is rewritten by the next unit
   }
 }

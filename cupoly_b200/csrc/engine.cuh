@@ -28,6 +28,8 @@ struct DgtPlan {
   int logN = 0;     // full transform size (N = nphi / 2)
   int logNc = 0;    // size handled inside one CTA
   int S = 0;        // split bits handled by the element-wise split stage
+  int cluster = 0;  // 1: run the split stage inside a 2^S-CTA thread-block cluster through
+                    // distributed shared memory (no separate HBM pass) when compiled for the plan
   int logR = 0;     // register radix
   int npass = 0;
   int w[kMaxPasses] = {0};

@@ -134,6 +134,13 @@ class Engine:
         call("cp_engine_set_plan", self._h, log_radix, log_cta)
         self.log_radix = log_radix
 
+    def set_split_mode(self, mode: int):
+        """0: split stage as its own kernel (HBM pass); 1: inside a thread-block cluster (DSMEM)."""
+        call("cp_engine_set_split_mode", self._h, int(mode))
+
+    def get_split_mode(self) -> int:
+        return int(_lib.lib().cp_engine_get_split_mode(self._h))
+
     def get_plan(self):
         r, c, s = C.c_int(), C.c_int(), C.c_int()
         call("cp_engine_get_plan", self._h, C.byref(r), C.byref(c), C.byref(s))

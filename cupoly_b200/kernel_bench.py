@@ -1,6 +1,6 @@
 """Per-kernel throughput on the current GPU, each against the HBM roofline.
 
-    python -m cupoly_b200.kernel_bench [--only NAME[,NAME...]] [--reps R] [--peak GBS]
+    python -m cupoly_b200.kernel_bench [--only NAME[,NAME...]] [--reps R] [--peak GBS] [--split-mode 0|1]
 
 One JSON line per workload: average milliseconds per launch (CUDA events on the
 launching stream, after a warm-up launch), the algorithmic bytes one launch must
@@ -8,6 +8,7 @@ move (each input read once, each output written once), the achieved GB/s and its
 fraction of the HBM peak (`--peak`, default the copy bandwidth recorded in
 MEASURED_PEAKS.json at the repository root when present, else 6650 GB/s).  Every
 workload's data exceeds the 126 MB L2, so successive launches stream from HBM.
+`--split-mode` sets the split-stage form of every engine (cp_engine_set_split_mode).
 
 Workloads (names for --only):
   dgt_fwd, dgt_inv   forward / inverse DGT, nphi 8192, 3072 residues (512 polynomials over B, in place)
@@ -57,13 +58,23 @@ def _time(fn, reps: int) -> float:
     return a.elapsed_time(b) / reps
 
 
+_SPLIT_MODE = None
+
+
+def _engine(*args) -> Engine:
+    e = Engine(*args)
+    if _SPLIT_MODE is not None:
+        e.set_split_mode(_SPLIT_MODE)
+    return e
+
+
 def workloads():
     """name -> builder; a builder returns (launch function, algorithmic bytes, description)."""
     W = {}
 
     def dgt(direction):
         def build():
-            e = Engine(5, 6, 8192, 256)
+            e = _engine(5, 6, 8192, 256)
             x = e.empty(BBase, 512)  # 512 x 6 = 3072 residues: the chain's forward DGT over B
             e.sample(x, BBase, UNIFORM, 1, 0, npolys=512, to_dgt=False)
             nres = 512 * 6
@@ -75,7 +86,7 @@ def workloads():
     W["dgt_inv"] = dgt(INVERSE)
 
     def mul():
-        e = Engine(5, 6, 8192, 256)
+        e = _engine(5, 6, 8192, 256)
         P = 512
         a, b, c = e.empty(QBase, P), e.empty(QBase, P), e.empty(QBase, P)
         e.sample(a, QBase, UNIFORM, 2, 0, npolys=P, to_dgt=False)
@@ -86,7 +97,7 @@ def workloads():
     W["mul"] = mul
 
     def polymul():
-        e = Engine(2, 3, 4096, 256)
+        e = _engine(2, 3, 4096, 256)
         P = 2048
         a, b, c = e.empty(QBase, P), e.empty(QBase, P), e.empty(QBase, P)
         e.sample(a, QBase, UNIFORM, 3, 0, npolys=P, to_dgt=False)
@@ -98,7 +109,7 @@ def workloads():
     W["polymul"] = polymul
 
     def basis_ext():
-        e = Engine(5, 6, 8192, 256)
+        e = _engine(5, 6, 8192, 256)
         P = 512
         x, y = e.empty(QBase, P), e.empty(BBase, P)
         e.sample(x, QBase, UNIFORM, 4, 0, npolys=P, to_dgt=False)
@@ -108,7 +119,7 @@ def workloads():
     W["basis_ext"] = basis_ext
 
     def complex_scaling():
-        e = Engine(5, 6, 8192, 256)
+        e = _engine(5, 6, 8192, 256)
         P = 384
         x, xb, y = e.empty(QBase, P), e.empty(BBase, P), e.empty(BBase, P)
         e.sample(x, QBase, UNIFORM, 5, 0, npolys=P, to_dgt=False)
@@ -120,7 +131,7 @@ def workloads():
 
     def crt(inverse):
         def build():
-            e = Engine(5, 6, 8192, 256)
+            e = _engine(5, 6, 8192, 256)
             P = 512
             x = e.empty(QBase, P)
             e.sample(x, QBase, UNIFORM, 6, 0, npolys=P, to_dgt=False)
@@ -136,7 +147,7 @@ def workloads():
 
     def sample(kind, name):
         def build():
-            e = Engine(16, 17, 32768, 65537)
+            e = _engine(16, 17, 32768, 65537)
             P = 512
             x = e.empty(QBase, P)
             return (lambda: e.sample(x, QBase, kind, 7, 0, npolys=P, to_dgt=False), P * 16 * e.N * 16,
@@ -145,7 +156,7 @@ def workloads():
 
     def chain(nphi, k, t, P):
         def build():
-            e = Engine(k, k + 1, nphi, t)
+            e = _engine(k, k + 1, nphi, t)
             ins = [e.empty(QBase, P) for _ in range(4)]
             for v, x in enumerate(ins):
                 e.sample(x, QBase, UNIFORM, 8, v * P, npolys=P, to_dgt=True)
@@ -169,7 +180,10 @@ def main():
     ap.add_argument("--only", default="")
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--peak", type=float, default=0.0)
+    ap.add_argument("--split-mode", type=int, choices=[0, 1], default=None)
     a = ap.parse_args()
+    global _SPLIT_MODE
+    _SPLIT_MODE = a.split_mode
     peak = a.peak or _peak()
     W = workloads()
     names = [n for n in a.only.split(",") if n] or list(W)

@@ -86,6 +86,14 @@ int cp_engine_ckks_prec(const cp_engine* e);
  * (cupoly_b200/autotune.py) measures the candidates and caches the fastest. */
 int cp_engine_set_plan(cp_engine* e, int log_radix, int log_cta);
 int cp_engine_get_plan(const cp_engine* e, int* log_radix, int* log_cta, int* split_bits);
+/* Form of the split stage of transforms larger than one CTA (plans with split bits > 0; no
+ * counterpart in cuPoly, whose two-pass split always goes through HBM):
+ * 0 = a separate element-wise kernel with its own HBM pass (default);
+ * 1 = inside a thread-block cluster of 2^split_bits CTAs, the chunks exchanged through
+ *     distributed shared memory.  Results are identical; where the cluster form has no kernel
+ *     for the plan or the device cannot co-schedule the cluster, mode 1 falls back to 0. */
+int cp_engine_set_split_mode(cp_engine* e, int mode);
+int cp_engine_get_split_mode(const cp_engine* e);
 int cp_engine_destroy(cp_engine* e);
 int cp_engine_n_residues(const cp_engine* e, int base);
 int cp_engine_nphi(const cp_engine* e);

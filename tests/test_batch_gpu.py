@@ -140,3 +140,57 @@ def test_streamed_bfv_matches_device_batches(gpu):
     torch.cuda.synchronize()
     for o, r in zip(outs, ref):
         assert torch.equal(o, r)
+
+
+@pytest.mark.parametrize("nphi,plans", [(16384, [(3, 11), (3, 12)]), (32768, [(3, 12), (3, 13)]),
+                                        (65536, [(3, 13)])])
+def test_cluster_split_stage_gives_the_same_transform(gpu, nphi, plans):
+    """The split stage inside a thread-block cluster (chunks exchanged through distributed
+    shared memory) gives the bytes of the separate split kernel and of the oracle, forward
+    and inverse, for 2- and 4-CTA clusters."""
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine, from_u64, to_u64
+    from oracle import coracle
+    e = Engine(2, 0, nphi, 256)
+    x = random_poly_residues(nphi + 1, e.Q, nphi)
+    ref = coracle.dgt(fold(x)[None], e.Q)
+    for r, c in plans:
+        e.set_plan(r, c)
+        for mode in (1, 0):
+            e.set_split_mode(mode)
+            assert e.get_split_mode() == mode and e.get_plan()["split_bits"] > 0
+            d = from_u64(fold(x)[None])
+            e.dgt(d, 0, FORWARD)
+            assert np.array_equal(to_u64(d), ref), (r, c, mode)
+            e.dgt(d, 0, INVERSE)
+            assert np.array_equal(to_u64(d)[0], fold(x)), (r, c, mode)
+
+
+def test_cluster_split_stage_in_the_fused_calls(gpu):
+    """The batched BFV chain (gather and tensor-product inverse DGTs) and the fused polymul
+    (out-of-place forward, product-on-load inverse) give identical bytes in both split
+    forms; the plans split 2 bits (nphi 16384, c11) and 1 bit (nphi 32768, c13)."""
+    import torch
+
+    from cupoly_b200.engine import QBase, UNIFORM, Engine
+    for nphi, k, t, c in ((16384, 3, 256, 11), (32768, 2, 65537, 13)):
+        e = Engine(k, 0, nphi, t)
+        e.set_plan(3, c)
+        P = 2
+        ins = []
+        for j in range(4):
+            x = e.empty(QBase, P)
+            e.sample(x, QBase, UNIFORM, 5, 16 * j, npolys=P, to_dgt=True)
+            ins.append(x)
+        ws = e.bfv_mul_batch_workspace(P)
+        pws = e.polymul_workspace(QBase, P)
+        out = {}
+        for mode in (0, 1):
+            e.set_split_mode(mode)
+            c3 = e.empty(QBase, 3 * P)
+            e.bfv_mul_batch(c3, *ins, P, ws)
+            pm = e.empty(QBase, P)
+            e.polymul(pm, ins[0], ins[1], QBase, pws, P)
+            torch.cuda.synchronize()
+            out[mode] = (c3.clone(), pm.clone())
+        assert torch.equal(out[0][0], out[1][0]), nphi
+        assert torch.equal(out[0][1], out[1][1]), nphi
