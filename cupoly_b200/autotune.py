@@ -8,9 +8,12 @@ pressure, passes, shared memory per CTA and hence CTAs per SM, the extra HBM
 pass of the split).  `best_plan(nphi)` times a forward + inverse transform of a
 batch for every candidate on the current GPU and caches the winner in a JSON
 file keyed by GPU name and nphi (the RNS width only scales the batch, so it
-does not change the choice).  Engines created with log_radix = 0 from Python
-use the cached plan when one exists and the library default (radix 8, c = 13)
-otherwise.
+does not change the choice).  Plans with a split stage are timed in both of its
+forms (a separate element-wise kernel, or inside a thread-block cluster through
+distributed shared memory; cp_engine_set_split_mode); the cluster form is cached
+with the plan only when it is more than 2 % faster.  Engines created with log_radix = 0 from Python use the
+cached plan when one exists and the library default (radix 8, c = 13, split
+kernel) otherwise.
 """
 from __future__ import annotations
 
@@ -52,6 +55,14 @@ def cached_plan(nphi: int) -> Tuple[int, int]:
         return 0, 0
 
 
+def cached_split_mode(nphi: int) -> int:
+    """Cached split-stage form for this GPU and nphi (0 split kernel, 1 cluster); 0 when none."""
+    try:
+        return int(_load().get(_key(nphi), {}).get("split_mode", 0))
+    except Exception:
+        return 0
+
+
 def cached_log_radix(nphi: int) -> int:
     return cached_plan(nphi)[0]
 
@@ -89,28 +100,32 @@ def best_plan(nphi: int, residues: int = 2048, reps: int = 5, save: bool = True)
         e.set_plan(r, c)
         x = e.empty(0, npolys)
         e.sample(x, 0, UNIFORM, 1, 0, npolys=npolys, to_dgt=False)
-        e.dgt(x, 0, FORWARD)
-        e.dgt(x, 0, INVERSE)
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(reps):
+        for mode in ((0, 1) if e.get_plan()["split_bits"] > 0 else (0,)):
+            e.set_split_mode(mode)
             e.dgt(x, 0, FORWARD)
             e.dgt(x, 0, INVERSE)
-        b.record()
-        torch.cuda.synchronize()
-        results[(r, c)] = a.elapsed_time(b) / reps
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                e.dgt(x, 0, FORWARD)
+                e.dgt(x, 0, INVERSE)
+            b.record()
+            torch.cuda.synchronize()
+            results[(r, c, mode)] = a.elapsed_time(b) / reps
         del e, x
-    best = min(results, key=results.get)
+    # the cluster form must win by more than the run-to-run spread (2 %) to be chosen
+    best = min(results, key=lambda k: results[k] * (1.02 if k[2] else 1.0))
     if save:
         data = _load()
-        data[key] = {"log_radix": best[0], "log_cta": best[1],
-                     "ms_fwd_inv": {"r%d_c%d" % k: round(v, 4) for k, v in results.items()},
+        data[key] = {"log_radix": best[0], "log_cta": best[1], "split_mode": best[2],
+                     "ms_fwd_inv": {("r%d_c%d_cluster" if k[2] else "r%d_c%d") % k[:2]: round(v, 4)
+                                    for k, v in results.items()},
                      "residues": 2 * npolys}
         os.makedirs(os.path.dirname(cache_path()), exist_ok=True)
         with open(cache_path(), "w") as f:
             json.dump(data, f, indent=1, sort_keys=True)
-    return best
+    return best[:2]
 
 
 def best_log_radix(nphi: int, **kw) -> int:

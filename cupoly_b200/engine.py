@@ -100,11 +100,12 @@ class Engine:
         if not torch.cuda.is_available():
             raise RuntimeError("cupoly_b200 needs a CUDA device")
         _lib.lib()
-        log_cta = 0
+        log_cta, split_mode = 0, 0
         if log_radix == 0:  # use the autotuner's plan for this GPU and size when one is cached
-            from .autotune import cached_plan
+            from .autotune import cached_plan, cached_split_mode
 
             log_radix, log_cta = cached_plan(nphi)
+            split_mode = cached_split_mode(nphi)
         h = C.c_void_p()
         if ckks_prec:
             call("cp_ckks_engine_create", C.byref(h), k, kl, nphi, ckks_prec, log_radix)
@@ -114,6 +115,8 @@ class Engine:
         self.ckks_prec = ckks_prec
         if log_cta:
             call("cp_engine_set_plan", h, log_radix, log_cta)
+        if split_mode:
+            call("cp_engine_set_split_mode", h, split_mode)
         self.log_radix = log_radix
         self._h = h
         self.k = k

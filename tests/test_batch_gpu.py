@@ -85,7 +85,9 @@ def test_autotuner_picks_a_candidate_and_caches(gpu, tmp_path, monkeypatch):
     assert plan in cands
     assert autotune.cached_plan(16384) == plan
     data = json.load(open(tmp_path / "tune.json"))
-    assert len(next(iter(data.values()))["ms_fwd_inv"]) == len(cands)
+    ent = next(iter(data.values()))
+    assert len(ent["ms_fwd_inv"]) == len(cands) + sum(1 for _, c in cands if c < 13)  # split plans: both forms
+    assert ent["split_mode"] in (0, 1)
     e = Engine(2, 0, 16384, 256)                           # picks the cached plan up
     assert (e.get_plan()["log_radix"], e.get_plan()["log_cta"]) == plan
 
