@@ -13,7 +13,11 @@
 //    192-bit dot product with one final reduction.
 //  * ICRT: the mixed-radix digits d_i of X (exact, word-size), then
 //    X = d_0 + q_0 (d_1 + q_1 (d_2 + ...)) by multi-limb Horner; X in [0, Q).
+#include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "../../include/cupoly_b200.h"
 #include "launch.cuh"
@@ -245,17 +249,35 @@ int cp_import_residues(const cp_engine* h, void* poly, const void* host_in, size
   CRT_REQUIRE(std::memcmp(in + sizeof(hd), primes, (size_t)nres * 8) == 0,
               "cp_import_residues: primes differ from the engine's");
   const uint64_t* body = reinterpret_cast<const uint64_t*>(in + sizeof(hd) + (size_t)nres * 8);
-  // every residue must be canonical: a malformed request is refused before it reaches the GPU
-  for (long long pl = 0; pl < npolys; ++pl)
-    for (int r = 0; r < nres; ++r) {
-      const uint64_t q = primes[r];
-      const uint64_t* row = body + ((size_t)pl * nres + r) * 2 * e.N;
-      for (int j = 0; j < 2 * e.N; ++j)
-        if (row[j] >= q) {
-          set_error("cp_import_residues: residue not reduced modulo its prime");
-          return CP_ERR_INVALID;
-        }
+  // every residue must be canonical: a malformed request is refused before it reaches the GPU.
+  // Rows (polynomial, residue) are checked on up to 16 host threads for large payloads.
+  const long long rows = (long long)npolys * nres;
+  const size_t row_words = (size_t)2 * e.N;
+  std::atomic<bool> bad{false};
+  auto check_rows = [&](long long lo, long long hi) {
+    for (long long y = lo; y < hi && !bad.load(std::memory_order_relaxed); ++y) {
+      const uint64_t q = primes[y % nres];
+      const uint64_t* row = body + (size_t)y * row_words;
+      uint64_t worst = 0;
+      for (size_t j = 0; j < row_words; ++j) worst = row[j] > worst ? row[j] : worst;
+      if (worst >= q) bad.store(true);
     }
+  };
+  const size_t bytes = (size_t)rows * row_words * 8;
+  const unsigned hw = std::thread::hardware_concurrency();
+  const long long nthreads = bytes < ((size_t)4 << 20) ? 1 : std::min<long long>(std::min(hw ? hw : 1u, 16u), rows);
+  if (nthreads <= 1) {
+    check_rows(0, rows);
+  } else {
+    std::vector<std::thread> pool;
+    for (long long t = 0; t < nthreads; ++t)
+      pool.emplace_back(check_rows, rows * t / nthreads, rows * (t + 1) / nthreads);
+    for (auto& th : pool) th.join();
+  }
+  if (bad.load()) {
+    set_error("cp_import_residues: residue not reduced modulo its prime");
+    return CP_ERR_INVALID;
+  }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cudaError_t err = cudaMemcpyAsync(poly, body, (size_t)npolys * nres * e.N * 16, cudaMemcpyHostToDevice, st);
   if (err == cudaSuccess) err = cudaStreamSynchronize(st);

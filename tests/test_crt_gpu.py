@@ -151,3 +151,30 @@ def test_host_mirror_exports_and_device_crt(gpu):
     f = cp.poly_import_binary(ctx, cp.poly_export_binary(ctx, b))
     assert [cp.poly_get_coeff(ctx, f, i) for i in range(256)] == ref
     cp.CUDAEngine.destroy()
+
+
+def test_wire_import_checks_large_payloads_on_host_threads(gpu):
+    """Payloads over 4 MB are checked on several host threads: a residue at or above its
+    prime anywhere (first, middle or last row) is still refused before any copy."""
+    import torch
+
+    from cupoly_b200.engine import Engine, QBase, UNIFORM
+    e = Engine(5, 0, 8192, 256)
+    P = 16
+    x = e.empty(QBase, P)
+    e.sample(x, QBase, UNIFORM, 3, 0, npolys=P, to_dgt=False)
+    data = e.export_residues(x, QBase, 0)
+    assert len(data) > 4 << 20
+    y = e.empty(QBase, P)
+    assert e.import_residues(y, data, QBase) == 0 and torch.equal(x, y)
+    body = 64 + 5 * 8
+    row = 2 * e.N * 8
+    nrows = P * 5
+    y.zero_()
+    for r in (0, nrows // 2, nrows - 1):
+        bad = bytearray(data)
+        off = body + r * row + row - 8  # last word of row r
+        bad[off:off + 8] = e.Q[r % 5].to_bytes(8, "little")
+        with pytest.raises(Exception, match="reduced"):
+            e.import_residues(y, bytes(bad), QBase)
+    assert int(y.abs().sum()) == 0  # nothing copied by the refused calls
