@@ -461,14 +461,22 @@ static int d2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
     if (rc_) return rc_;     \
   } while (0)
 
+// Inverse DGT of one polynomial over `base` from `src` into `dst` (out of place: the
+// kernel reads the source directly, no copy first).
+static int inv_dgt_from(const Engine& e, void* dst, const void* src, int base, cudaStream_t st) {
+  InvSrc is{};
+  is.p[0] = reinterpret_cast<const ulonglong2*>(src);
+  is.mode = 0;
+  is.npairs = 1;
+  return launch_dgt_ex(e, dst, nullptr, &is, base, 1, 0, true, st);
+}
+
 int cp_poly_basis_extension_q_to_b(const cp_engine* h, void* out_b, const void* in_q, void* ws, void* stream) {
   CP_BFV_ONLY(h, "cp_poly_basis_extension_q_to_b");
   CP_REQUIRE(h && out_b && in_q && ws, "cp_poly_basis_extension_q_to_b: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
-  const size_t qb = (size_t)e.k * e.N * 16;
-  CP_TRY(d2d(ws, in_q, qb, st));
-  CP_TRY(launch_dgt(e, ws, CP_QBASE, 1, 0, true, st));
+  CP_TRY(inv_dgt_from(e, ws, in_q, CP_QBASE, st));
   CP_TRY(hps_basis_ext(e, out_b, ws, true, 1, st));
   return launch_dgt(e, out_b, CP_BBASE, 1, 0, false, st);
 }
@@ -480,8 +488,7 @@ int cp_poly_basis_extension_q_to_qb(const cp_engine* h, void* out_qb, const void
   cudaStream_t st = S(stream);
   const size_t qb = (size_t)e.k * e.N * 16;
   char* ob = reinterpret_cast<char*>(out_qb) + qb;
-  CP_TRY(d2d(ws, in_q, qb, st));
-  CP_TRY(launch_dgt(e, ws, CP_QBASE, 1, 0, true, st));
+  CP_TRY(inv_dgt_from(e, ws, in_q, CP_QBASE, st));
   CP_TRY(hps_basis_ext(e, ob, ws, true, 1, st));
   CP_TRY(launch_dgt(e, ob, CP_BBASE, 1, 0, false, st));
   return d2d(out_qb, in_q, qb, st);
@@ -492,8 +499,7 @@ int cp_poly_basis_extension_b_to_q(const cp_engine* h, void* out_q, const void* 
   CP_REQUIRE(h && out_q && in_b && ws, "cp_poly_basis_extension_b_to_q: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
-  CP_TRY(d2d(ws, in_b, (size_t)e.kl * e.N * 16, st));
-  CP_TRY(launch_dgt(e, ws, CP_BBASE, 1, 0, true, st));
+  CP_TRY(inv_dgt_from(e, ws, in_b, CP_BBASE, st));
   CP_TRY(hps_basis_ext(e, out_q, ws, false, 1, st));
   return launch_dgt(e, out_q, CP_QBASE, 1, 0, false, st);
 }
@@ -508,15 +514,13 @@ int cp_poly_complex_scaling_tdivq(const cp_engine* h, void* out_q, void* in_q, v
   ulonglong2* w = reinterpret_cast<ulonglong2*>(ws);
   void* xq = in_q;
   void* xb = in_b;
-  if (!(flags & CP_DESTROY_INPUTS)) {
+  if (!(flags & CP_DESTROY_INPUTS)) {  // inputs kept: transform out of place into the workspace
     xq = w;
     xb = w + qe;
-    CP_TRY(d2d(xq, in_q, qe * 16, st));
-    CP_TRY(d2d(xb, in_b, be * 16, st));
   }
   void* u = w + qe + be;
-  CP_TRY(launch_dgt(e, xq, CP_QBASE, 1, 0, true, st));
-  CP_TRY(launch_dgt(e, xb, CP_BBASE, 1, 0, true, st));
+  CP_TRY(inv_dgt_from(e, xq, in_q, CP_QBASE, st));
+  CP_TRY(inv_dgt_from(e, xb, in_b, CP_BBASE, st));
   CP_TRY(hps_scale_to_q(e, out_q, xq, xb, u, 1, st));
   return launch_dgt(e, out_q, CP_QBASE, 1, 0, false, st);
 }
@@ -526,8 +530,7 @@ int cp_poly_simple_scaling_tdivq(const cp_engine* h, void* out_t, const void* in
   CP_REQUIRE(h && out_t && in_q && ws, "cp_poly_simple_scaling_tdivq: bad argument");
   const Engine& e = h->e;
   cudaStream_t st = S(stream);
-  CP_TRY(d2d(ws, in_q, (size_t)e.k * e.N * 16, st));
-  CP_TRY(launch_dgt(e, ws, CP_QBASE, 1, 0, true, st));
+  CP_TRY(inv_dgt_from(e, ws, in_q, CP_QBASE, st));
   return hps_simple_scaling(e, out_t, ws, st);
 }
 
