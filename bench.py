@@ -284,11 +284,21 @@ def next_rows(seed: int, hbm_peak: float):
     ms_raise = _timed(lambda: c.ckks_modulus_raising(qb, a, lvl), 20)
     ms_red = _timed(lambda: c.ckks_modulus_reduction(r, qb, lvl), 20)
     ms_resc = _timed(lambda: c.ckks_rescale(r, None, lvl), 20)
+    PB = 64
+    ab = c.empty(QBase, PB)
+    c.sample(ab, QBase, UNIFORM, seed, 4, npolys=PB, to_dgt=True)
+    qbb, rb, wsb = c.empty(QBBase, PB), c.empty(QBase, PB), c.ckks_batch_workspace(PB)
+    mb_raise = _timed(lambda: c.ckks_modulus_raising_batch(qbb, ab, lvl, wsb), 5)
+    mb_red = _timed(lambda: c.ckks_modulus_reduction_batch(rb, qbb, lvl, wsb), 5)
+    mb_resc = _timed(lambda: c.ckks_rescale_batch(rb, lvl), 5)
     c.check()
-    out["ckks"] = {"config": "nphi=16384, k=8, kl=9, prec 52, level 7, one polynomial per call, DGT domain",
+    out["ckks"] = {"config": "nphi=16384, k=8, kl=9, prec 52, level 7, DGT domain",
                    "modulus_raising_us": round(ms_raise * 1e3, 1), "modulus_reduction_us": round(ms_red * 1e3, 1),
-                   "rescale_us": round(ms_resc * 1e3, 1)}
-    del a, qb, r, c
+                   "rescale_us": round(ms_resc * 1e3, 1),
+                   "batched_64_us_per_poly": {"modulus_raising": round(mb_raise * 1e3 / PB, 2),
+                                              "modulus_reduction": round(mb_red * 1e3 / PB, 2),
+                                              "rescale": round(mb_resc * 1e3 / PB, 2)}}
+    del a, qb, r, c, ab, qbb, rb, wsb
     torch.cuda.empty_cache()
     return out
 

@@ -46,6 +46,10 @@ SIGNATURES = {
     "cp_ckks_modulus_raising": (_i, [_vp, _vp, _vp, _i, _vp, _vp]),
     "cp_ckks_modulus_reduction": (_i, [_vp, _vp, _vp, _i, _vp, _vp]),
     "cp_ckks_rescale": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "cp_ckks_batch_workspace_bytes": (C.c_size_t, [_vp, _i]),
+    "cp_ckks_modulus_raising_batch": (_i, [_vp, _vp, _vp, _i, _i, _vp, _vp]),
+    "cp_ckks_modulus_reduction_batch": (_i, [_vp, _vp, _vp, _i, _i, _vp, _vp]),
+    "cp_ckks_rescale_batch": (_i, [_vp, _vp, _i, _i, _vp]),
     "cp_ckks_xi": (_i, [_vp, _vp, _vp, _vp]),
     "cp_ckks_rho": (_i, [_vp, _vp, _vp, _vp]),
     "cp_engine_destroy": (_i, [_vp]),

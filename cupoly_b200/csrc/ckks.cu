@@ -31,10 +31,14 @@ struct CkArgs {
 };
 
 // B residues of the coefficient-domain Q residues 0..level (rows of N elements).
+// Polynomial blockIdx.y at strides out_stride / in_stride (elements).
 __global__ void __launch_bounds__(128) k_ckks_raise(ulonglong2* __restrict__ outB, const ulonglong2* __restrict__ inQ,
-                                                    CkArgs a, int o_inv, int o_inv_s, int o_m, int o_m_s) {
+                                                    CkArgs a, int o_inv, int o_inv_s, int o_m, int o_m_s,
+                                                    long long out_stride, long long in_stride) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.N) return;
+  outB += blockIdx.y * out_stride;
+  inQ += blockIdx.y * in_stride;
   const int l = a.level;
   uint64_t tr[kMaxCk], ti[kMaxCk];
   for (int i = 0; i <= l; ++i) {
@@ -58,11 +62,14 @@ __global__ void __launch_bounds__(128) k_ckks_raise(ulonglong2* __restrict__ out
 }
 
 // Q residues 0..level of the coefficient-domain QB polynomial; higher Q rows untouched.
+// Polynomial blockIdx.y at strides out_stride / in_stride (elements).
 __global__ void __launch_bounds__(128) k_ckks_reduce(ulonglong2* __restrict__ outQ, const ulonglong2* __restrict__ inQB,
                                                      CkArgs a, int o_bi, int o_bi_s, int o_bq, int o_bq_s, int o_ib,
-                                                     int o_ib_s) {
+                                                     int o_ib_s, long long out_stride, long long in_stride) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.N) return;
+  outQ += blockIdx.y * out_stride;
+  inQB += blockIdx.y * in_stride;
   uint64_t sr[kMaxCk], si[kMaxCk];
   for (int jb = 0; jb < a.kl; ++jb) {
     const uint64_t b = a.mc[a.k + jb].p;
@@ -139,63 +146,107 @@ using namespace cpoly;
 
 extern "C" {
 
-int cp_ckks_modulus_raising(const cp_engine* h, void* out_qb, const void* in_q, int level, void* ws, void* stream) {
+// Batched implementations: npolys polynomials back to back; the workspace holds
+// npolys QB polynomials.  The single-polynomial calls are npolys = 1.
+static int ckks_raise(const cp_engine* h, void* out_qb, const void* in_q, int level, int npolys, void* ws,
+                      void* stream, const char* name) {
   CK_ENGINE(h, "cp_ckks_modulus_raising");
-  CK_REQUIRE(out_qb && in_q && ws, "cp_ckks_modulus_raising: NULL argument");
+  CK_REQUIRE(out_qb && in_q && ws && npolys >= 0, "cp_ckks_modulus_raising: NULL argument or negative count");
   const Engine& e = h->e;
   CK_REQUIRE(level >= 0 && level < e.k, "cp_ckks_modulus_raising: level must be in [0, k)");
+  if (npolys == 0) return CP_OK;
+  CK_REQUIRE(npolys <= 65535, "cp_ckks_modulus_raising: at most 65535 polynomials per call");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   ulonglong2* out = reinterpret_cast<ulonglong2*>(out_qb);
   ulonglong2* w = reinterpret_cast<ulonglong2*>(ws);
-  const long long qsz = (long long)e.k * e.N;
-  cudaError_t err = cudaMemcpyAsync(out, in_q, qsz * 16, cudaMemcpyDeviceToDevice, st);
-  if (err != cudaSuccess) return cuda_fail("cp_ckks_modulus_raising", err);
-  if (int rc = launch_dgt_part(e, w, in_q, 0, level + 1, 1, qsz, true, st)) return rc;  // Q_l, coefficients
+  const long long qsz = (long long)e.k * e.N, qbsz = (long long)(e.k + e.kl) * e.N;
+  cudaError_t err = cudaMemcpy2DAsync(out, qbsz * 16, in_q, qsz * 16, qsz * 16, npolys, cudaMemcpyDeviceToDevice, st);
+  if (err != cudaSuccess) return cuda_fail(name, err);
+  if (int rc = launch_dgt_part(e, w, in_q, 0, level + 1, npolys, qsz, true, st)) return rc;  // Q_l, coefficients
   const auto& o = e.ho;
-  k_ckks_raise<<<(e.N + 127) / 128, 128, 0, st>>>(out + qsz, w, args(e, level), o.ck_qlqi_inv, o.ck_qlqi_inv_s,
-                                                   o.ck_qlqi_b, o.ck_qlqi_b_s);
-  if (int rc = check_launch("cp_ckks_modulus_raising")) return rc;
-  return launch_dgt_part(e, out + qsz, nullptr, e.k, e.kl, 1, (long long)e.kl * e.N, false, st);
+  k_ckks_raise<<<dim3((e.N + 127) / 128, npolys), 128, 0, st>>>(out + qsz, w, args(e, level), o.ck_qlqi_inv,
+                                                                 o.ck_qlqi_inv_s, o.ck_qlqi_b, o.ck_qlqi_b_s, qbsz, qsz);
+  if (int rc = check_launch(name)) return rc;
+  return launch_dgt_part(e, out + qsz, nullptr, e.k, e.kl, npolys, qbsz, false, st);
 }
 
-int cp_ckks_modulus_reduction(const cp_engine* h, void* out_q, const void* in_qb, int level, void* ws, void* stream) {
+static int ckks_reduce(const cp_engine* h, void* out_q, const void* in_qb, int level, int npolys, void* ws,
+                       void* stream, const char* name) {
   CK_ENGINE(h, "cp_ckks_modulus_reduction");
-  CK_REQUIRE(out_q && in_qb && ws, "cp_ckks_modulus_reduction: NULL argument");
+  CK_REQUIRE(out_q && in_qb && ws && npolys >= 0, "cp_ckks_modulus_reduction: NULL argument or negative count");
   const Engine& e = h->e;
   CK_REQUIRE(level >= 0 && level < e.k, "cp_ckks_modulus_reduction: level must be in [0, k)");
+  if (npolys == 0) return CP_OK;
+  CK_REQUIRE(npolys <= 65535, "cp_ckks_modulus_reduction: at most 65535 polynomials per call");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   ulonglong2* w = reinterpret_cast<ulonglong2*>(ws);
   const ulonglong2* in = reinterpret_cast<const ulonglong2*>(in_qb);
-  const long long qsz = (long long)e.k * e.N;
+  const long long qsz = (long long)e.k * e.N, qbsz = (long long)(e.k + e.kl) * e.N;
   // coefficients of Q_l and of B into the workspace (same QB layout)
-  if (int rc = launch_dgt_part(e, w, in, 0, level + 1, 1, qsz, true, st)) return rc;
-  if (int rc = launch_dgt_part(e, w + qsz, in + qsz, e.k, e.kl, 1, (long long)e.kl * e.N, true, st)) return rc;
+  if (int rc = launch_dgt_part(e, w, in, 0, level + 1, npolys, qbsz, true, st)) return rc;
+  if (int rc = launch_dgt_part(e, w + qsz, in + qsz, e.k, e.kl, npolys, qbsz, true, st)) return rc;
   const auto& o = e.ho;
   ulonglong2* out = reinterpret_cast<ulonglong2*>(out_q);
-  k_ckks_reduce<<<(e.N + 127) / 128, 128, 0, st>>>(out, w, args(e, level), o.ck_bbj_inv, o.ck_bbj_inv_s, o.ck_bbj_q,
-                                                    o.ck_bbj_q_s, o.ck_binv_q, o.ck_binv_q_s);
-  if (int rc = check_launch("cp_ckks_modulus_reduction")) return rc;
-  return launch_dgt_part(e, out, nullptr, 0, level + 1, 1, qsz, false, st);
+  k_ckks_reduce<<<dim3((e.N + 127) / 128, npolys), 128, 0, st>>>(out, w, args(e, level), o.ck_bbj_inv, o.ck_bbj_inv_s,
+                                                                  o.ck_bbj_q, o.ck_bbj_q_s, o.ck_binv_q, o.ck_binv_q_s,
+                                                                  qsz, qbsz);
+  if (int rc = check_launch(name)) return rc;
+  return launch_dgt_part(e, out, nullptr, 0, level + 1, npolys, qsz, false, st);
+}
+
+static int ckks_rescale(const cp_engine* h, void* x, int npolys, int level, void* stream) {
+  const Engine& e = h->e;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const long long qsz = (long long)e.k * e.N;
+  ulonglong2* p = reinterpret_cast<ulonglong2*>(x);
+  if (int rc = launch_dgt_part(e, p, nullptr, 0, level + 1, npolys, qsz, true, st)) return rc;
+  k_ckks_rescale<<<dim3((e.N + 255) / 256, npolys), 256, 0, st>>>(p, qsz, args(e, level), e.ho.ck_inv_ql,
+                                                                   e.ho.ck_inv_ql_s);
+  if (int rc = check_launch("cp_ckks_rescale")) return rc;
+  return launch_dgt_part(e, p, nullptr, 0, level + 1, npolys, qsz, false, st);
+}
+
+int cp_ckks_modulus_raising(const cp_engine* h, void* out_qb, const void* in_q, int level, void* ws, void* stream) {
+  return ckks_raise(h, out_qb, in_q, level, 1, ws, stream, "cp_ckks_modulus_raising");
+}
+
+int cp_ckks_modulus_reduction(const cp_engine* h, void* out_q, const void* in_qb, int level, void* ws, void* stream) {
+  return ckks_reduce(h, out_q, in_qb, level, 1, ws, stream, "cp_ckks_modulus_reduction");
 }
 
 int cp_ckks_rescale(const cp_engine* h, void* a, void* b, int level, void* stream) {
   CK_ENGINE(h, "cp_ckks_rescale");
   CK_REQUIRE(a, "cp_ckks_rescale: NULL argument");
-  const Engine& e = h->e;
-  CK_REQUIRE(level >= 1 && level < e.k, "cp_ckks_rescale: level must be in [1, k)");
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  const long long qsz = (long long)e.k * e.N;
+  CK_REQUIRE(level >= 1 && level < h->e.k, "cp_ckks_rescale: level must be in [1, k)");
   void* polys[2] = {a, b};
-  for (void* x : polys) {
-    if (!x) continue;
-    ulonglong2* p = reinterpret_cast<ulonglong2*>(x);
-    if (int rc = launch_dgt_part(e, p, nullptr, 0, level + 1, 1, qsz, true, st)) return rc;
-    dim3 grid((e.N + 255) / 256, 1);
-    k_ckks_rescale<<<grid, 256, 0, st>>>(p, qsz, args(e, level), e.ho.ck_inv_ql, e.ho.ck_inv_ql_s);
-    if (int rc = check_launch("cp_ckks_rescale")) return rc;
-    if (int rc = launch_dgt_part(e, p, nullptr, 0, level + 1, 1, qsz, false, st)) return rc;
-  }
+  for (void* x : polys)
+    if (x)
+      if (int rc = ckks_rescale(h, x, 1, level, stream)) return rc;
   return CP_OK;
+}
+
+size_t cp_ckks_batch_workspace_bytes(const cp_engine* h, int npolys) {
+  if (!h || npolys < 0) return 0;
+  return (size_t)npolys * (h->e.k + h->e.kl) * h->e.N * 16;
+}
+
+int cp_ckks_modulus_raising_batch(const cp_engine* h, void* out_qb, const void* in_q, int level, int npolys, void* ws,
+                                  void* stream) {
+  return ckks_raise(h, out_qb, in_q, level, npolys, ws, stream, "cp_ckks_modulus_raising_batch");
+}
+
+int cp_ckks_modulus_reduction_batch(const cp_engine* h, void* out_q, const void* in_qb, int level, int npolys,
+                                    void* ws, void* stream) {
+  return ckks_reduce(h, out_q, in_qb, level, npolys, ws, stream, "cp_ckks_modulus_reduction_batch");
+}
+
+int cp_ckks_rescale_batch(const cp_engine* h, void* x, int npolys, int level, void* stream) {
+  CK_ENGINE(h, "cp_ckks_rescale_batch");
+  CK_REQUIRE(x && npolys >= 0, "cp_ckks_rescale_batch: NULL argument or negative count");
+  CK_REQUIRE(level >= 1 && level < h->e.k, "cp_ckks_rescale_batch: level must be in [1, k)");
+  CK_REQUIRE(npolys <= 65535, "cp_ckks_rescale_batch: at most 65535 polynomials per call");
+  if (npolys == 0) return CP_OK;
+  return ckks_rescale(h, x, npolys, level, stream);
 }
 
 static int ckks_scale(const cp_engine* h, void* out, const void* in, bool xi, void* stream, const char* name) {

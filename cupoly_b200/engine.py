@@ -267,6 +267,24 @@ class Engine:
     def ckks_rescale(self, a, b, level: int, stream=None):
         call("cp_ckks_rescale", self._h, _ptr(a), _ptr(b), level, _stream(stream))
 
+    def ckks_batch_workspace(self, npolys: int) -> torch.Tensor:
+        n = int(_lib.lib().cp_ckks_batch_workspace_bytes(self._h, npolys))
+        return torch.empty(max(1, n // 8), dtype=torch.int64, device="cuda")
+
+    def ckks_modulus_raising_batch(self, out_qb, in_q, level: int, workspace, npolys=None, stream=None):
+        n = in_q.shape[0] if npolys is None else npolys
+        call("cp_ckks_modulus_raising_batch", self._h, _ptr(out_qb), _ptr(in_q), level, n, _ptr(workspace),
+             _stream(stream))
+
+    def ckks_modulus_reduction_batch(self, out_q, in_qb, level: int, workspace, npolys=None, stream=None):
+        n = in_qb.shape[0] if npolys is None else npolys
+        call("cp_ckks_modulus_reduction_batch", self._h, _ptr(out_q), _ptr(in_qb), level, n, _ptr(workspace),
+             _stream(stream))
+
+    def ckks_rescale_batch(self, x, level: int, npolys=None, stream=None):
+        n = x.shape[0] if npolys is None else npolys
+        call("cp_ckks_rescale_batch", self._h, _ptr(x), n, level, _stream(stream))
+
     def ckks_xi(self, out, a, stream=None):
         call("cp_ckks_xi", self._h, _ptr(out), _ptr(a), _stream(stream))
 

@@ -252,6 +252,16 @@ int cp_ckks_modulus_raising(const cp_engine* e, void* out_qb, const void* in_q, 
 int cp_ckks_modulus_reduction(const cp_engine* e, void* out_q, const void* in_qb, int level, void* workspace,
                               void* stream);
 int cp_ckks_rescale(const cp_engine* e, void* a, void* b, int level, void* stream);
+/* Batched forms of the three calls above (no counterpart in cuPoly, one polynomial per call
+ * there): npolys polynomials back to back (in_q / out_q over Q, in_qb / out_qb over QB, x over Q,
+ * rescaled in place), same definitions per polynomial; the workspace holds
+ * cp_ckks_batch_workspace_bytes(e, npolys) bytes; at most 65535 polynomials per call. */
+size_t cp_ckks_batch_workspace_bytes(const cp_engine* e, int npolys);
+int cp_ckks_modulus_raising_batch(const cp_engine* e, void* out_qb, const void* in_q, int level, int npolys,
+                                  void* workspace, void* stream);
+int cp_ckks_modulus_reduction_batch(const cp_engine* e, void* out_q, const void* in_qb, int level, int npolys,
+                                    void* workspace, void* stream);
+int cp_ckks_rescale_batch(const cp_engine* e, void* x, int npolys, int level, void* stream);
 int cp_ckks_xi(const cp_engine* e, void* out, const void* in, void* stream);
 int cp_ckks_rho(const cp_engine* e, void* out, const void* in, void* stream);
 

@@ -247,3 +247,36 @@ def test_ckks_uniform_sampler_over_narrow_primes(gpu, prec):
     for r, q in enumerate(e.Q):
         assert int(got[r].max()) < q
         assert abs(float(np.mean(got[r].astype(np.float64))) / q - 0.5) < 0.03
+
+
+@pytest.mark.parametrize("k,kl,nphi,prec,level", [(3, 4, 4096, 52, 2), (8, 9, 16384, 45, 5), (4, 5, 32768, 55, 3)])
+def test_ckks_batched_calls_equal_per_polynomial_calls(gpu, k, kl, nphi, prec, level):
+    """Batched modulus raising, reduction and rescale give, polynomial by polynomial, the
+    bytes of the one-polynomial calls (DGT domain in and out)."""
+    import torch
+
+    from cupoly_b200.engine import QBBase, QBase, UNIFORM
+    e = _eng(k, kl, nphi, prec)
+    P = 5
+    a = e.empty(QBase, P)
+    e.sample(a, QBase, UNIFORM, 21, 0, npolys=P, to_dgt=True)
+    qb = e.empty(QBBase, P)
+    e.sample(qb, QBBase, UNIFORM, 22, 0, npolys=P, to_dgt=True)
+    ws = e.ckks_batch_workspace(P)
+    raised = e.empty(QBBase, P)
+    e.ckks_modulus_raising_batch(raised, a, level, ws)
+    reduced = e.zeros(QBase, P)
+    e.ckks_modulus_reduction_batch(reduced, qb, level, ws)
+    resc = a.clone()
+    e.ckks_rescale_batch(resc, level)
+    for i in range(P):
+        r1 = e.empty(QBBase)
+        e.ckks_modulus_raising(r1, a[i:i + 1], level)
+        assert torch.equal(r1, raised[i:i + 1]), ("raising", i)
+        d1 = e.zeros(QBase)
+        e.ckks_modulus_reduction(d1, qb[i:i + 1], level)
+        assert torch.equal(d1[:, : level + 1], reduced[i:i + 1, : level + 1]), ("reduction", i)
+        s1 = a[i:i + 1].clone()
+        e.ckks_rescale(s1, None, level)
+        assert torch.equal(s1, resc[i:i + 1]), ("rescale", i)
+    e.check()
