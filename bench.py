@@ -253,9 +253,15 @@ def next_rows(seed: int, hbm_peak: float):
     xi = e.empty(QBase, k)
     ms_xi = _timed(lambda: e.xi(xi, x[0:1]), 50)
     ms_rho = _timed(lambda: e.rho(xi, x[0:1]), 50)
-    out["xi_rho"] = {"config": "nphi=%d, k=%d, one polynomial per call -> k polynomials" % (n, k),
+    XB = 64
+    xib = e.empty(QBase, XB * k)
+    ms_xib = _timed(lambda: e.xi_batch(xib, x[:XB]), 10)
+    out["xi_rho"] = {"config": "nphi=%d, k=%d, one polynomial -> k polynomials" % (n, k),
                      "xi_us_per_call": round(ms_xi * 1e3, 2), "rho_us_per_call": round(ms_rho * 1e3, 2),
-                     "GB_per_s": round((k * N * 16 * (1 + k)) / ms_xi / 1e6, 1)}
+                     "GB_per_s": round((k * N * 16 * (1 + k)) / ms_xi / 1e6, 1),
+                     "xi_batch_64_us_per_poly": round(ms_xib * 1e3 / XB, 3),
+                     "xi_batch_GB_per_s": round(XB * (k * N * 16 * (1 + k)) / ms_xib / 1e6, 1)}
+    del xib
     W = 128
     blob = torch.empty(e.wire_bytes(QBase, W), dtype=torch.uint8, pin_memory=True).numpy()
     z = e.empty(QBase, W)

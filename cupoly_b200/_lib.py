@@ -83,6 +83,8 @@ SIGNATURES = {
     "cp_simple_scaling": (_i, [_vp, _vp, _vp, _vp]),
     "cp_xi": (_i, [_vp, _vp, _vp, _vp]),
     "cp_rho": (_i, [_vp, _vp, _vp, _vp]),
+    "cp_xi_batch": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "cp_rho_batch": (_i, [_vp, _vp, _vp, _i, _vp]),
     "cp_poly_basis_extension_q_to_b": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cp_poly_basis_extension_q_to_qb": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "cp_poly_basis_extension_b_to_q": (_i, [_vp, _vp, _vp, _vp, _vp]),

@@ -446,6 +446,16 @@ int cp_rho(const cp_engine* h, void* out, const void* in, void* stream) {
   CP_REQUIRE(h && out && in, "cp_rho: bad argument");
   return rns_xi_rho(h->e, out, in, true, S(stream));
 }
+int cp_xi_batch(const cp_engine* h, void* out, const void* in, int npolys, void* stream) {
+  CP_BFV_ONLY(h, "cp_xi_batch");
+  CP_REQUIRE(h && out && in && npolys >= 0, "cp_xi_batch: bad argument");
+  return rns_xi_rho(h->e, out, in, false, S(stream), npolys);
+}
+int cp_rho_batch(const cp_engine* h, void* out, const void* in, int npolys, void* stream) {
+  CP_BFV_ONLY(h, "cp_rho_batch");
+  CP_REQUIRE(h && out && in && npolys >= 0, "cp_rho_batch: bad argument");
+  return rns_xi_rho(h->e, out, in, true, S(stream), npolys);
+}
 
 // ---------------- composite calls ----------------
 

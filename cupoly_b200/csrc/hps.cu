@@ -606,8 +606,11 @@ namespace {
 __global__ void __launch_bounds__(256) k_xi_rho(ulonglong2* __restrict__ out, const ulonglong2* __restrict__ in,
                                                 const ModConst* __restrict__ mc, const uint64_t* __restrict__ w,
                                                 const uint64_t* __restrict__ ws, int k, int N) {
-  const int i = blockIdx.y;  // output polynomial
-  const int r = blockIdx.z;  // residue
+  const int i = blockIdx.y;      // output polynomial of the decomposition
+  const int r = blockIdx.z % k;  // residue
+  const int pl = blockIdx.z / k;  // input polynomial of the batch
+  in += (size_t)pl * k * N;
+  out += (size_t)pl * k * k * N;
   ulonglong2* o = out + ((size_t)i * k + r) * N;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
     if (r != i) {
@@ -621,12 +624,17 @@ __global__ void __launch_bounds__(256) k_xi_rho(ulonglong2* __restrict__ out, co
 }
 }  // namespace
 
-int rns_xi_rho(const Engine& e, void* out, const void* in, bool rho, cudaStream_t st) {
+int rns_xi_rho(const Engine& e, void* out, const void* in, bool rho, cudaStream_t st, int npolys) {
   const uint64_t* w = e.d_hps + (rho ? e.ho.rho_q : e.ho.xi_q);
   const uint64_t* ws = e.d_hps + (rho ? e.ho.rho_q_s : e.ho.xi_q_s);
+  if (npolys <= 0) return 0;
+  if ((long long)npolys * e.k > 65535) {
+    set_error("xi_rho: at most 65535 / k polynomials per call");
+    return 1;
+  }
   int bx = (e.N + 255) / 256;
   if (bx > 1024) bx = 1024;
-  dim3 grid(bx, e.k, e.k);
+  dim3 grid(bx, e.k, e.k * npolys);
   k_xi_rho<<<grid, 256, 0, st>>>(reinterpret_cast<ulonglong2*>(out), reinterpret_cast<const ulonglong2*>(in), e.d_mc,
                                  w, ws, e.k, e.N);
   return check_launch("xi_rho");

@@ -29,7 +29,7 @@ int hps_complex_scaling(const Engine& e, void* out_b, const void* in_q, const vo
 int hps_scale_to_q(const Engine& e, void* out_q, const void* in_q, const void* in_b, void* scratch_b, int npolys,
                    cudaStream_t st);
 int hps_simple_scaling(const Engine& e, void* out_t, const void* in_q, cudaStream_t st);
-int rns_xi_rho(const Engine& e, void* out, const void* in, bool rho, cudaStream_t st);
+int rns_xi_rho(const Engine& e, void* out, const void* in, bool rho, cudaStream_t st, int npolys = 1);
 
 // Sampler
 int sample_poly(const Engine& e, void* out, int base, int kind, uint64_t seed, uint32_t stream_id, int npolys,

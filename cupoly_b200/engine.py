@@ -350,6 +350,15 @@ class Engine:
     def xi(self, out, a, stream=None):
         call("cp_xi", self._h, _ptr(out), _ptr(a), _stream(stream))
 
+    def xi_batch(self, out, a, npolys=None, stream=None):
+        """out (npolys * k, k, N, 2): the xi decomposition of each of the npolys polynomials of a."""
+        n = a.shape[0] if npolys is None else npolys
+        call("cp_xi_batch", self._h, _ptr(out), _ptr(a), n, _stream(stream))
+
+    def rho_batch(self, out, a, npolys=None, stream=None):
+        n = a.shape[0] if npolys is None else npolys
+        call("cp_rho_batch", self._h, _ptr(out), _ptr(a), n, _stream(stream))
+
     def rho(self, out, a, stream=None):
         call("cp_rho", self._h, _ptr(out), _ptr(a), _stream(stream))
 

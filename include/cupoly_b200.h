@@ -169,6 +169,11 @@ int cp_simple_scaling(const cp_engine* e, void* out_t, const void* in_q, void* s
  * out is k polynomials over Q; polynomial i has residue i set, the rest zero */
 int cp_xi(const cp_engine* e, void* out, const void* in, void* stream);
 int cp_rho(const cp_engine* e, void* out, const void* in, void* stream);
+/* batched forms (no counterpart in cuPoly): npolys input polynomials over Q back to back, out =
+ * npolys x k polynomials (input p's decomposition at polynomials p k .. p k + k - 1);
+ * npolys k <= 65535 */
+int cp_xi_batch(const cp_engine* e, void* out, const void* in, int npolys, void* stream);
+int cp_rho_batch(const cp_engine* e, void* out, const void* in, int npolys, void* stream);
 
 /* ---- composite polynomial calls, DGT domain in and out: replace
  *      poly_basis_extension_Q_to_B / _Q_to_QB / _B_to_Q, poly_complex_scaling_tDivQ,

@@ -309,3 +309,21 @@ def test_device_matches_cupolys_float_path_where_it_is_exact(gpu, k, t):
         assert [int(v) for v in oc[:, c]] == O.complex_scaling_exact([int(v) for v in zq[:, c]],
                                                                       [int(v) for v in zb[:, c]], Q, B, t)
     assert set(diff["simple"]) <= {0, 1}
+
+
+def test_xi_rho_batch_equals_per_polynomial_calls(gpu):
+    """cp_xi_batch / cp_rho_batch: polynomial p's decomposition equals the one-polynomial call."""
+    import torch
+
+    from cupoly_b200.engine import Engine, QBase, UNIFORM
+    e = Engine(4, 0, 4096, 256)
+    P, k = 6, 4
+    a = e.empty(QBase, P)
+    e.sample(a, QBase, UNIFORM, 31, 0, npolys=P, to_dgt=True)
+    for batch, single in ((e.xi_batch, e.xi), (e.rho_batch, e.rho)):
+        out = e.empty(QBase, P * k)
+        batch(out, a)
+        for p in range(P):
+            one = e.empty(QBase, k)
+            single(one, a[p:p + 1])
+            assert torch.equal(one, out[p * k:(p + 1) * k]), (batch.__name__, p)
