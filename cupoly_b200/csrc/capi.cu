@@ -111,8 +111,8 @@ int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int l
   CP_REQUIRE(k >= 1 && k <= 24, "cp_engine_create: k must be in [1, 24]");
   CP_REQUIRE(kl >= 1 && kl <= 24, "cp_engine_create: kl must be in [1, 24]");
   CP_REQUIRE(k + kl <= kNumPrimes, "cp_engine_create: k + kl exceeds the prime table");
-  CP_REQUIRE(nphi >= 2 && nphi <= 65536 && (nphi & (nphi - 1)) == 0,
-             "cp_engine_create: nphi must be a power of two in [2, 65536]");
+  CP_REQUIRE(nphi >= 4 && nphi <= 65536 && (nphi & (nphi - 1)) == 0,
+             "cp_engine_create: nphi must be a power of two in [4, 65536]");
   CP_REQUIRE(t >= 2 && t < kPrimes[kNumPrimes - 1], "cp_engine_create: t must be in [2, min prime)");
   CP_REQUIRE(log_radix == 0 || (log_radix >= 2 && log_radix <= 4), "cp_engine_create: log_radix must be 0, 2, 3 or 4");
   cp_engine* h = new_engine(k, kl, nphi, t);
@@ -140,8 +140,8 @@ int cp_ckks_engine_create(cp_engine** out, int k, int kl, int nphi, int prec, in
              "cp_ckks_engine_create: prec must be 45, 48, 52 or 55");
   CP_REQUIRE(k >= 1 && k <= 24, "cp_ckks_engine_create: k must be in [1, 24]");
   CP_REQUIRE(kl >= 1 && kl <= 24, "cp_ckks_engine_create: kl must be in [1, 24]");
-  CP_REQUIRE(nphi >= 2 && nphi <= 65536 && (nphi & (nphi - 1)) == 0,
-             "cp_ckks_engine_create: nphi must be a power of two in [2, 65536]");
+  CP_REQUIRE(nphi >= 4 && nphi <= 65536 && (nphi & (nphi - 1)) == 0,
+             "cp_ckks_engine_create: nphi must be a power of two in [4, 65536]");
   CP_REQUIRE(log_radix == 0 || (log_radix >= 2 && log_radix <= 4),
              "cp_ckks_engine_create: log_radix must be 0, 2, 3 or 4");
   // Q = the first 63-bit prime, then k - 1 primes of the precision bucket; B = kl primes of

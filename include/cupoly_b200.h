@@ -63,7 +63,7 @@ const char* cp_last_error(void);
 /* ---- engine: replaces CUDAEngine::init(k, kl, M, t) / destroy() / get_n_residues(base)
  *      (cuPoly include/cuPoly/cuda/cudaengine.h:65-123, src/cuda/cudaengine.cu:1691-1779)
  *      and DGTEngine::init (src/cuda/dgt.cu:1694-1982).  nphi is the ring degree
- *      (cuPoly's M), 2 <= nphi <= 65536 a power of two; kl <= 0 selects k + 1;
+ *      (cuPoly's M), 4 <= nphi <= 65536 a power of two; kl <= 0 selects k + 1;
  *      any t >= 2 coprime to Q (cuPoly requires a power of two).  The engine is
  *      created on the current CUDA device.  log_radix in {3, 4} picks the DGT
  *      register radix (0 = default). */

@@ -39,6 +39,9 @@ def test_no_torch_dependency_in_native_library():
     ((2, 3, 131072, 256, 0), "power of two"),
     ((2, 3, 4096, 1, 0), "t must be"),
     ((2, 3, 4096, 256, 5), "log_radix"),
+    ((2, 3, 2, 256, 0), "nphi must be a power of two in [4, 65536]"),
+    ((2, 3, 131072, 256, 0), "nphi must be a power of two"),
+    ((2, 3, 3000, 256, 0), "nphi must be a power of two"),
     ((2, 3, 4096, 256, 1), "log_radix"),
 ])
 def test_engine_create_rejects_bad_parameters(args, fragment):
