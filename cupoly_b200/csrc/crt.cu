@@ -272,9 +272,16 @@ int cp_import_residues(const cp_engine* h, void* poly, const void* host_in, size
   if (nthreads <= 1) {
     check_rows(0, rows);
   } else {
+    // no exception may cross the C ABI: if a thread cannot be started, the rows it would
+    // have checked are checked on this thread
     std::vector<std::thread> pool;
-    for (long long t = 0; t < nthreads; ++t)
-      pool.emplace_back(check_rows, rows * t / nthreads, rows * (t + 1) / nthreads);
+    long long started = 0;
+    try {
+      for (; started < nthreads; ++started)
+        pool.emplace_back(check_rows, rows * started / nthreads, rows * (started + 1) / nthreads);
+    } catch (...) {
+    }
+    if (started < nthreads) check_rows(rows * started / nthreads, rows);
     for (auto& th : pool) th.join();
   }
   if (bad.load()) {
