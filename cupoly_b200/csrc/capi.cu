@@ -59,6 +59,20 @@ const char* cp_last_error(void) { return last_error(); }
 
 namespace {
 
+// build_tables with host allocation failures turned into a status (no exception may cross
+// the C ABI).
+int build_tables_nothrow(Engine& e) {
+  try {
+    return build_tables(e);
+  } catch (const std::bad_alloc&) {
+    set_error("engine tables: host allocation failed");
+    return CP_ERR_OOM;
+  } catch (...) {
+    set_error("engine tables: unexpected host error");
+    return CP_ERR_INVALID;
+  }
+}
+
 // Shared tail of the two creation calls: tables for the given primes.
 int finish_engine(cp_engine** out, cp_engine* h, int log_radix) {
   Engine& e = h->e;
@@ -73,7 +87,7 @@ int finish_engine(cp_engine** out, cp_engine* h, int log_radix) {
     e.xi.push_back(canonical_xi(p, e.roots[i], (uint64_t)e.N));
   }
   e.plan = make_plan(e.logN, log_radix ? log_radix : 3);
-  int rc = build_tables(e);
+  int rc = build_tables_nothrow(e);
   if (rc) {
     delete h;
     return rc;
@@ -184,7 +198,7 @@ int cp_engine_set_plan(cp_engine* h, int log_radix, int log_cta) {
   const int cluster = e.plan.cluster;  // the split-stage form survives a plan change
   e.plan = make_plan(e.logN, log_radix ? log_radix : 3, lc);
   e.plan.cluster = cluster;
-  return build_tables(e);
+  return build_tables_nothrow(e);
 }
 
 int cp_engine_set_split_mode(cp_engine* h, int mode) {
@@ -261,7 +275,7 @@ int cp_engine_set_nthroot(cp_engine* h, const uint64_t* xi) {
   cudaDeviceSynchronize();
   free_tables(e);
   e.xi = nx;
-  return build_tables(e);
+  return build_tables_nothrow(e);
 }
 
 int cp_engine_get_nthroot(const cp_engine* h, uint64_t* xi_out) {
