@@ -327,3 +327,29 @@ def test_xi_rho_batch_equals_per_polynomial_calls(gpu):
             one = e.empty(QBase, k)
             single(one, a[p:p + 1])
             assert torch.equal(one, out[p * k:(p + 1) * k]), (batch.__name__, p)
+
+
+@pytest.mark.parametrize("k,nphi,t,npairs,seed", [(10, 16384, 256, 4, 1), (16, 32768, 65537, 2, 2),
+                                                  (8, 4096, 65537, 8, 3), (3, 16384, 256, 6, 4),
+                                                  (7, 8192, 3, 5, 5)])
+def test_bfv_mul_batch_at_the_large_configurations_vs_oracle(gpu, k, nphi, t, npairs, seed):
+    """The batched chain at nphi 2^14 with a 10-prime basis (the configuration the targets
+    are stated on), at nphi 32768 / k 16 / t 65537, and at other widths and plaintext moduli
+    (t = 3: not a power of two), bit-exact against the oracle pair by pair, in the tuned plans
+    (split stages included)."""
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine
+    e = Engine(k, 0, nphi, t)
+    rows = [np.stack([random_poly_residues(1000 * seed + 10 * i + j, e.Q, nphi) for i in range(npairs)])
+            for j in range(4)]
+    dev = []
+    for r in rows:
+        d = _dev(fold(r))
+        e.dgt(d, 0, FORWARD)
+        dev.append(d)
+    c = e.empty(0, 3 * npairs)
+    e.bfv_mul_batch(c, *dev, npairs, e.bfv_mul_batch_workspace(npairs))
+    e.dgt(c, 0, INVERSE)
+    got = unfold(_host(c))
+    ref = CO.bfv_mul(*rows, e.Q, e.B, t)
+    for j in range(3):
+        assert np.array_equal(got[j * npairs:(j + 1) * npairs], ref[j]), (j, k, nphi)
