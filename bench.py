@@ -219,11 +219,73 @@ def _timed(fn, reps: int) -> float:
     return a.elapsed_time(b) / reps
 
 
+def _dot_row(seed: int, hbm_peak: float):
+    """The key-switching inner product sum_i a_i b_i over k = 16 terms at nphi 32768 (one
+    relinearization component at the large configuration), fused (cp_dot, one pass) against
+    cuPoly's composition (one mul and k - 1 muladd calls), each as 10 calls in a CUDA graph.
+    Two operand sets alternate so the 132 MB working set of a call is not served from L2."""
+    import torch
+
+    from cupoly_b200.engine import QBase, UNIFORM, Engine
+
+    d = Engine(16, 0, 32768, 65537)
+    nt = d.k
+    sets = []
+    for s in range(2):
+        ops = d.empty(QBase, 2 * nt)
+        d.sample(ops, QBase, UNIFORM, seed, 60 + s, npolys=2 * nt, to_dgt=False)
+        sets.append(([ops[i] for i in range(nt)], [ops[nt + i] for i in range(nt)]))
+    acc = [d.empty(QBase), d.empty(QBase)]
+    it = [0]
+
+    def fused():
+        j = it[0] & 1
+        it[0] += 1
+        d.dot(acc[j], sets[j][0], sets[j][1], QBase)
+
+    def composed():
+        j = it[0] & 1
+        it[0] += 1
+        a, b = sets[j]
+        d.mul(acc[j], a[0], b[0], QBase)
+        for i in range(1, nt):
+            d.muladd(acc[j], a[i], b[i], acc[j], QBase)
+
+    def graph_of(fn, calls):
+        # captured, so the host's per-call cost (16-entry pointer arrays, 16 launches for the
+        # composition) does not hide the device time
+        fn()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s), torch.cuda.graph(g, stream=s):
+            for _ in range(calls):
+                fn()
+        torch.cuda.synchronize()
+        return g
+
+    calls = 10
+    gf, gc = graph_of(fused, calls), graph_of(composed, calls)
+    ms_f = _timed(gf.replay, 5) / calls
+    ref = [x.clone() for x in acc]
+    ms_c = _timed(gc.replay, 5) / calls
+    assert all(torch.equal(x, y) for x, y in zip(acc, ref)), "fused dot != composition"
+    del gf, gc
+    poly = d.k * d.N * 16
+    byt = (2 * nt + 1) * poly
+    d.check()
+    return {"config": "nphi=%d, k=%d, %d terms" % (d.nphi, d.k, nt), "fused_us": round(ms_f * 1e3, 2),
+            "composed_us": round(ms_c * 1e3, 2), "speedup": round(ms_c / ms_f, 2),
+            "GB_per_s": round(byt / ms_f / 1e6, 1), "frac_hbm": round(byt / ms_f / 1e6 / hbm_peak, 4),
+            "bytes_per_call": byt, "composed_bytes_per_call": (3 + 4 * (nt - 1)) * poly}
+
+
 def next_rows(seed: int, hbm_peak: float):
     """Throughput of the calls after the multiplication chain, each with its algorithmic bytes
     (what an ideal kernel reads and writes once) over the measured time:
     device CRT / ICRT (512 polynomials, nphi 8192, k 5: limbs and residues both above L2 size),
-    xi and rho (one polynomial per call, as cuPoly's API), the binary wire form (host side,
+    xi and rho (one polynomial per call, as cuPoly's API), the fused key-switching dot product
+    (nphi 32768, k 16), the binary wire form (host side,
     128 polynomials), and the CKKS calls (nphi 16384, k 8, kl 9, 52-bit primes, one polynomial
     per call, level k - 1)."""
     import time
@@ -262,6 +324,7 @@ def next_rows(seed: int, hbm_peak: float):
                      "xi_batch_64_us_per_poly": round(ms_xib * 1e3 / XB, 3),
                      "xi_batch_GB_per_s": round(XB * (k * N * 16 * (1 + k)) / ms_xib / 1e6, 1)}
     del xib
+    out["dot"] = _dot_row(seed, hbm_peak)
     W = 128
     blob = torch.empty(e.wire_bytes(QBase, W), dtype=torch.uint8, pin_memory=True).numpy()
     z = e.empty(QBase, W)

@@ -403,6 +403,14 @@ int cp_muladd(const cp_engine* h, void* d, const void* a, const void* b, const v
   CP_REQUIRE(d && a && b && c, "cp_muladd: NULL buffer");
   return pw_muladd(h->e, d, a, b, c, base, S(stream));
 }
+int cp_dot(const cp_engine* h, void* c, const void* const* a, const void* const* b, int n, int base,
+           void* stream) {
+  PW_CHECK("cp_dot");
+  CP_REQUIRE(c && a && b && n >= 1, "cp_dot: NULL buffer or n < 1");
+  for (int t = 0; t < n; ++t) CP_REQUIRE(a[t] && b[t], "cp_dot: NULL operand");
+  NvtxRange range("cp_dot");
+  return pw_dot(h->e, c, a, b, n, base, S(stream));
+}
 int cp_dr2(const cp_engine* h, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, void* stream) {
   PW_CHECK("cp_dr2");

@@ -157,6 +157,58 @@ struct DoubleOpIntF {
   }
 };
 
+// c = sum_t a_t b_t (+ c when `acc`) over up to kDotTerms pairs, one pass,
+// one thread per element.  The pseudo-Mersenne primes sum the Karatsuba
+// products P1 = a0 b0, P2 = a1 b1, P3 = (a0 + a1)(b0 + b1) (each below 2^128:
+// a0 + a1, b0 + b1 < 2^64) in three 192-bit accumulators and reduce once per
+// element: re = P1 - P2, im = P3 - P1 - P2.  64 terms stay below 2^134, inside
+// red192's t < 2^8 bound, and red192 needs 2^64 mod p < 2^32, which holds for
+// these primes.  Other primes reduce every product.  Each element is read
+// completely before its output is written, so c may alias any operand of the
+// launch.
+struct DotArgs {
+  const u2* a[kDotTerms];
+  const u2* b[kDotTerms];
+};
+
+__global__ void __launch_bounds__(256)
+    k_dot(DotArgs args, int n, u2* c, int acc, int N, int rid_off, const ModConst* __restrict__ mc) {
+  const ModConst m = mc[rid_off + blockIdx.y];
+  const size_t base = (size_t)blockIdx.y * N;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const size_t i = base + j;
+    uint64_t sr = 0, si = 0;
+    if (m.pm) {
+      uint64_t l1 = 0, h1 = 0, t1 = 0, l2 = 0, h2 = 0, t2 = 0, l3 = 0, h3 = 0, t3 = 0;
+#pragma unroll 4
+      for (int t = 0; t < n; ++t) {
+        const u2 x = args.a[t][i], y = args.b[t][i];
+        mac192(l1, h1, t1, x.x, y.x);
+        mac192(l2, h2, t2, x.y, y.y);
+        mac192(l3, h3, t3, x.x + x.y, y.x + y.y);
+      }
+      const uint64_t p1 = red192(l1, h1, t1, m.p, m.r1, m.r2), p2 = red192(l2, h2, t2, m.p, m.r1, m.r2),
+                     p3 = red192(l3, h3, t3, m.p, m.r1, m.r2);
+      sr = sub_mod(p1, p2, m.p);
+      si = sub_mod(sub_mod(p3, p1, m.p), p2, m.p);
+    } else {
+      for (int t = 0; t < n; ++t) {
+        const u2 x = args.a[t][i], y = args.b[t][i];
+        uint64_t r, im;
+        gi_mul(r, im, x.x, x.y, y.x, y.y, m);
+        sr = add_mod(sr, r, m.p);
+        si = add_mod(si, im, m.p);
+      }
+    }
+    if (acc) {
+      const u2 z = c[i];
+      sr = add_mod(sr, z.x, m.p);
+      si = add_mod(si, z.y, m.p);
+    }
+    c[i] = make_ulonglong2(sr, si);
+  }
+}
+
 }  // namespace
 
 #define U2(p) reinterpret_cast<u2*>(p)
@@ -184,6 +236,36 @@ int pw_mul_u64(const Engine& e, void* c, const void* a, const uint64_t* b, int b
 }
 int pw_muladd(const Engine& e, void* d, const void* a, const void* b, const void* c, int base, cudaStream_t st) {
   return launch_ew(e, MulAddF{U2(d), CU2(a), CU2(b), CU2(c)}, base, st);
+}
+int pw_dot(const Engine& e, void* c, const void* const* a, const void* const* b, int n, int base,
+           cudaStream_t st) {
+  const int nres = e.n_residues(base);
+  if (nres <= 0) {
+    set_error("dot: unknown base");
+    return CP_ERR_INVALID_;
+  }
+  // Launches after the first accumulate into c: c must not be an operand of
+  // a later launch, whose input the first launch would already have overwritten.
+  for (int t = kDotTerms; t < n; ++t)
+    if (a[t] == c || b[t] == c) {
+      set_error("dot: the output aliases an operand beyond the first 64 terms");
+      return CP_ERR_INVALID_;
+    }
+  const int threads = 256;
+  for (int t0 = 0; t0 < n; t0 += kDotTerms) {
+    const int m = n - t0 < kDotTerms ? n - t0 : kDotTerms;
+    DotArgs args{};
+    for (int t = 0; t < m; ++t) {
+      args.a[t] = CU2(a[t0 + t]);
+      args.b[t] = CU2(b[t0 + t]);
+    }
+    int bx = (e.N + threads - 1) / threads;
+    if (bx > 4096) bx = 4096;
+    k_dot<<<dim3(bx, nres), threads, 0, st>>>(args, m, U2(c), t0 > 0, e.N, e.rid_offset(base), e.d_mc);
+    const int rc = check_launch("dot");
+    if (rc != CP_OK_) return rc;
+  }
+  return CP_OK_;
 }
 int pw_dr2(const Engine& e, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, cudaStream_t st, int npolys) {

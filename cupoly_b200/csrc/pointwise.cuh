@@ -15,6 +15,10 @@ int pw_mul_u64(const Engine& e, void* c, const void* a, const uint64_t* b, int b
 int pw_mul_list(const Engine& e, void* c, const void* a, const void* b, const int* rid_list, int nlist,
                 cudaStream_t st);
 int pw_muladd(const Engine& e, void* d, const void* a, const void* b, const void* c, int base, cudaStream_t st);
+// Operand pairs per dot-product launch; longer sums take several launches.
+constexpr int kDotTerms = 64;
+int pw_dot(const Engine& e, void* c, const void* const* a, const void* const* b, int n, int base,
+           cudaStream_t st);
 int pw_dr2(const Engine& e, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, cudaStream_t st, int npolys = 1);
 int pw_negate(const Engine& e, void* b, const void* a, int base, cudaStream_t st);

@@ -448,6 +448,28 @@ def poly_mul_add(ctx, d, a, b, c):
     _done(d, a.base)
 
 
+def poly_dot(ctx, c, a, b, k):
+    """c = sum_{i<k} a[i] b[i] (cuPoly src/arithmetic/polynomial.cu:1439-1451), one fused pass.
+
+    cuPoly composes one poly_mul and k - 1 poly_mul_add calls, so when c is also an
+    operand of a later term those calls read the partial sum; that case keeps the
+    composition and gives the same bytes.
+    """
+    if k < 1:
+        raise ValueError("poly_dot: k must be at least 1")
+    if any(a[i] is c or b[i] is c for i in range(1, k)):
+        poly_mul(ctx, c, a[0], b[0])
+        for i in range(1, k):
+            poly_mul_add(ctx, c, a[i], b[i], c)
+        return
+    base = a[0].base
+    ops = list(a[:k]) + list(b[:k])
+    assert all(x.base == base for x in ops)
+    _prep(ctx, c, base, *ops)
+    _E().dot(c.d_coefs, [x.d_coefs for x in a[:k]], [x.d_coefs for x in b[:k]], base, ctx.stream)
+    _done(c, base)
+
+
 def poly_dr2(ctx, ct21, ct22, ct23, ct01, ct02, ct11, ct12):
     assert ct01.base == ct02.base == ct11.base == ct12.base
     base = ct01.base

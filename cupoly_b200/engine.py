@@ -237,6 +237,18 @@ class Engine:
     def muladd(self, d, a, b, c, base, stream=None):
         call("cp_muladd", self._h, _ptr(d), _ptr(a), _ptr(b), _ptr(c), base, _stream(stream))
 
+    def dot(self, c, a, b, base, stream=None):
+        """c = sum_i a[i] b[i] in the DGT domain, one pass (cuPoly's poly_dot).
+
+        ``a`` and ``b`` are equal-length sequences of residue tensors over ``base``.
+        """
+        if len(a) != len(b) or not a:
+            raise ValueError("dot: a and b must be non-empty and of equal length")
+        n = len(a)
+        pa = (C.c_void_p * n)(*[_ptr(x) for x in a])
+        pb = (C.c_void_p * n)(*[_ptr(x) for x in b])
+        call("cp_dot", self._h, _ptr(c), pa, pb, n, base, _stream(stream))
+
     def dr2(self, c21, c22, c23, c01, c02, c11, c12, base, stream=None):
         call("cp_dr2", self._h, _ptr(c21), _ptr(c22), _ptr(c23), _ptr(c01), _ptr(c02), _ptr(c11), _ptr(c12),
              base, _stream(stream))

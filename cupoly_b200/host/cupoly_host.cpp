@@ -550,9 +550,33 @@ void poly_right_shift(Context* ctx, poly_t* b, poly_t* a, int bits) {
   for (int i = 0; i <= deg; ++i) poly_set_coeff(ctx, b, i, poly_get_coeff(ctx, a, i) >> bits);
 }
 
+// cuPoly composes one poly_mul and k - 1 poly_mul_add calls (polynomial.cu:1439-1451),
+// so when c is also an operand of a later term those calls read the partial sum; that
+// case keeps the composition and gives the same bytes.  Otherwise one fused pass.
 void poly_dot(Context* ctx, poly_t* c, poly_t* a, poly_t* b, const int k) {
-  poly_mul(ctx, c, &a[0], &b[0]);
-  for (int i = 1; i < k; ++i) poly_mul_add(ctx, c, &a[i], &b[i], c);
+  require(k >= 1, "poly_dot: k must be at least 1");
+  bool later_alias = false;
+  for (int i = 1; i < k; ++i) later_alias = later_alias || &a[i] == c || &b[i] == c;
+  if (later_alias) {
+    poly_mul(ctx, c, &a[0], &b[0]);
+    for (int i = 1; i < k; ++i) poly_mul_add(ctx, c, &a[i], &b[i], c);
+    return;
+  }
+  const int base = a[0].base;
+  std::vector<const void*> pa(k), pb(k);
+  for (int i = 0; i < k; ++i) {
+    same_base(&a[0], &a[i]);
+    same_base(&a[0], &b[i]);
+    poly_copy_to_device(ctx, &a[i]);
+    poly_copy_to_device(ctx, &b[i]);
+  }
+  prep_out(ctx, c, base);
+  for (int i = 0; i < k; ++i) {
+    pa[i] = a[i].d_coefs;
+    pb[i] = b[i].d_coefs;
+  }
+  check(cp_dot(E(), c->d_coefs, pa.data(), pb.data(), k, base, S(ctx)), "poly_dot");
+  done(c, base);
 }
 
 // ---------------------------------------------------------------------------

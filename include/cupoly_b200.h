@@ -148,6 +148,14 @@ int cp_mul_u64(const cp_engine* e, void* c, const void* a, const uint64_t* b, in
 /* cp_mul over npolys densely packed polynomials (no counterpart in cuPoly) */
 int cp_mul_batch(const cp_engine* e, void* c, const void* a, const void* b, int base, int npolys, void* stream);
 int cp_muladd(const cp_engine* e, void* d, const void* a, const void* b, const void* c, int base, void* stream);
+/* replaces poly_dot (src/arithmetic/polynomial.cu:1439-1451), which composes one
+ * poly_mul and n-1 poly_mul_add calls: c = sum_i a[i] b[i] over `base` in the DGT domain
+ * in one pass, each operand read once and each sum reduced once per element.  a and b are
+ * HOST arrays of n >= 1 device pointers.  c may alias any operand among the first 64 pairs
+ * (the result is the sum over the inputs as they were before the call); aliasing a later
+ * operand returns CP_ERR_INVALID. */
+int cp_dot(const cp_engine* e, void* c, const void* const* a, const void* const* b, int n, int base,
+           void* stream);
 int cp_dr2(const cp_engine* e, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, void* stream);
 /* replace CUDAEngine::execute_polynomial_negate / _op_by_int / _double_op_by_int

@@ -411,9 +411,22 @@ TEST_F(TestArithmetic, Dot) {
     for (int i = 0; i < 3; ++i) s += F.negacyclic(va[i], vb[i], j, F.q);
     CHECK(vc[j] == s % F.q, "index " << j);
   }
+  // c is also a later operand: the result must be the bytes of cuPoly's
+  // poly_mul + poly_mul_add composition, which reads the partial sum
+  poly_t x[3], y[3];
+  for (int i = 0; i < 3; ++i) {
+    poly_copy(F.ctx, &x[i], &a[i]);
+    poly_copy(F.ctx, &y[i], &a[i]);
+  }
+  poly_dot(F.ctx, &x[2], x, b, 3);
+  poly_mul(F.ctx, &y[2], &y[0], &b[0]);
+  for (int i = 1; i < 3; ++i) poly_mul_add(F.ctx, &y[2], &y[i], &b[i], &y[2]);
+  CHECK(F.coeffs(&x[2]) == F.coeffs(&y[2]), "aliased output");
   for (int i = 0; i < 3; ++i) {
     poly_free(F.ctx, &a[i]);
     poly_free(F.ctx, &b[i]);
+    poly_free(F.ctx, &x[i]);
+    poly_free(F.ctx, &y[i]);
   }
   poly_free(F.ctx, &c);
 }

@@ -210,3 +210,100 @@ def test_fused_polymul_vs_oracle(gpu, k, nphi, npolys):
     assert np.array_equal(unfold(to_u64(c)), ref)
     e.polymul(da, da, db, QBase, ws)                    # in place over a
     assert np.array_equal(unfold(to_u64(da)), ref)
+
+
+def _dot_exact(xs, ys, primes):
+    """sum_t xs[t] ys[t] per residue, exact (numpy object ints)."""
+    acc = None
+    for x, y in zip(xs, ys):
+        term = np.stack([_gi_mul(x[r], y[r], p) for r, p in enumerate(primes)]).astype(object)
+        acc = term if acc is None else acc + term
+    return np.stack([acc[r] % p for r, p in enumerate(primes)]).astype(np.uint64)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 64, 65, 130])
+def test_dot_vs_exact(gpu, n):
+    """cp_dot (cuPoly poly_dot, polynomial.cu:1439-1451) == exact sum of Gaussian products,
+    across the 64-term launch boundary; every base of a BFV engine and a CKKS engine."""
+    from cupoly_b200.engine import Engine, from_u64, to_u64
+    for e, bases in ((Engine(3, 4, 2048, 256), (0, 1, 2)), (Engine.ckks(3, 0, 2048, 52), (0,))):
+        for base in bases if n <= 5 else bases[:1]:
+            primes = e.base_primes(base)
+            xs = [fold(random_poly_residues(1000 + 7 * t + base, primes, 2048)) for t in range(n)]
+            ys = [fold(random_poly_residues(5000 + 7 * t + base, primes, 2048)) for t in range(n)]
+            out = e.empty(base)
+            e.dot(out, [from_u64(x[None]) for x in xs], [from_u64(y[None]) for y in ys], base)
+            assert np.array_equal(to_u64(out)[0], _dot_exact(xs, ys, primes))
+
+
+def test_dot_extreme_operands_and_aliasing(gpu):
+    """Every operand at p - 1 + (p - 1) i, so each Karatsuba product (a0 + a1)(b0 + b1) is at
+    its maximum (2p - 2)^2, over 64 terms (the widest lazy sum of a launch); an output that
+    aliases an operand of the launch; an output that aliases an operand of a later launch is
+    refused."""
+    from cupoly_b200._lib import CupolyError
+    from cupoly_b200.engine import Engine, from_u64, to_u64
+    e = Engine(2, 3, 64, 256)
+    primes = e.base_primes(0)
+    P = np.array(primes, dtype=np.uint64)[:, None]
+    x = np.stack([np.full((32, 2), p - 1, dtype=np.uint64) for p in primes])  # (p-1) + (p-1) i
+    xs, ys = [x] * 64, [x] * 64
+    out = e.empty(0)
+    e.dot(out, [from_u64(v[None]) for v in xs], [from_u64(v[None]) for v in ys], 0)
+    assert np.array_equal(to_u64(out)[0], _dot_exact(xs, ys, primes))
+    assert (to_u64(out)[0] < P[..., None]).all()
+
+    xs = [fold(random_poly_residues(70 + t, primes, 64)) for t in range(70)]
+    ys = [fold(random_poly_residues(170 + t, primes, 64)) for t in range(70)]
+    exp = _dot_exact(xs[:5], ys[:5], primes)
+    da = [from_u64(v[None]) for v in xs]
+    db = [from_u64(v[None]) for v in ys]
+    e.dot(da[3], da[:5], db[:5], 0)  # c is a[3]: read before written, element by element
+    assert np.array_equal(to_u64(da[3])[0], exp)
+    da[3] = from_u64(xs[3][None])
+    with pytest.raises(CupolyError):
+        e.dot(da[66], da, db, 0)
+    exp = _dot_exact(xs, ys, primes)
+    e.dot(da[2], da, db, 0)  # aliasing the first launch's operands is fine
+    assert np.array_equal(to_u64(da[2])[0], exp)
+
+
+def test_poly_dot_mirror_matches_composition(gpu):
+    """poly_dot through the cuPoly mirror equals cuPoly's poly_mul + poly_mul_add composition,
+    including an output that is also a later operand (the composition reads the partial sum)."""
+    import torch
+    from cupoly_b200.engine import to_u64
+    cp, ctx = _ref_engine(120, 2048)
+    k = 4
+    A = [cp.poly_t() for _ in range(k)]
+    B = [cp.poly_t() for _ in range(k)]
+    for x in A + B:
+        cp.poly_init(ctx, x)
+        cp.Sampler.sample(ctx, x, cp.UNIFORM)
+
+    def composed(a, b, c=None):
+        c = cp.poly_t() if c is None else c
+        cp.poly_mul(ctx, c, a[0], b[0])
+        for i in range(1, k):
+            cp.poly_mul_add(ctx, c, a[i], b[i], c)
+        return c
+
+    def coeffs(x):
+        torch.cuda.synchronize()
+        return to_u64(x.d_coefs)
+
+    ref = coeffs(composed(A, B))
+    got = cp.poly_t()
+    cp.poly_dot(ctx, got, A, B, k)
+    assert np.array_equal(coeffs(got), ref)
+    # c is A[2]: both forms must give cuPoly's bytes
+    A2 = [cp.poly_t() for _ in range(k)]
+    for i in range(k):
+        cp.poly_copy(ctx, A2[i], A[i])
+    cp.poly_dot(ctx, A2[2], A2, B, k)
+    A3 = [cp.poly_t() for _ in range(k)]
+    for i in range(k):
+        cp.poly_copy(ctx, A3[i], A[i])
+    composed(A3, B, A3[2])
+    assert np.array_equal(coeffs(A2[2]), coeffs(A3[2]))
+    cp.CUDAEngine.destroy()

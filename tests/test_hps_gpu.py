@@ -173,6 +173,10 @@ def test_reference_rns_tests(gpu, logq2, nphi):
     cp.poly_mul(ctx, prod_, x, y)
     assert [cp.poly_get_coeff(ctx, acc, i) for i in range(nphi)] == \
         [cp.poly_get_coeff(ctx, prod_, i) for i in range(nphi)]
+    dot = cp.poly_t()
+    cp.poly_dot(ctx, dot, R, X, k)  # the fused form of the loop above
+    assert [cp.poly_get_coeff(ctx, dot, i) for i in range(nphi)] == \
+        [cp.poly_get_coeff(ctx, prod_, i) for i in range(nphi)]
     cp.CUDAEngine.destroy()
 
 
