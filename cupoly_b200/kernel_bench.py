@@ -19,6 +19,8 @@ Workloads (names for --only):
   crt, icrt          coefficient limbs <-> residues, nphi 8192, k 5, 512 polynomials
   sample_ternary, sample_gaussian, sample_uniform
                      2^24 coefficients x 16 residues (nphi 32768, k 16, 512 polynomials)
+  dot                key-switching dot product (cp_dot), 16 terms, nphi 32768, k 16; bytes = 32
+                     operands read + 1 written
   bfv_chain, bfv_chain_target, bfv_chain_large
                      the batched BFV multiplication chain (cp_bfv_mul_batch) at nphi 8192 / k 5 /
                      128 pairs, nphi 16384 / k 10 / 32 pairs and nphi 32768 / k 16 / t 65537 / 64
@@ -166,6 +168,26 @@ def workloads():
                     "batched BFV multiplication, nphi %d, k %d, kl %d, t %d, %d pairs per call" % (nphi, k, k + 1, t, P), e)
         return build
 
+    def dot():
+        e = _engine(16, 17, 32768, 65537)
+        nt = 16
+        sets = []
+        for s in range(2):  # two operand sets alternate: 2 x 138 MB
+            ops = e.empty(QBase, 2 * nt)
+            e.sample(ops, QBase, UNIFORM, 9, 2 * nt * s, npolys=2 * nt, to_dgt=False)
+            sets.append(([ops[i] for i in range(nt)], [ops[nt + i] for i in range(nt)]))
+        c = e.empty(QBase)
+        it = [0]
+
+        def fn():
+            a, b = sets[it[0] & 1]
+            it[0] += 1
+            e.dot(c, a, b, QBase)
+
+        return (fn, (2 * nt + 1) * 16 * e.N * 16,
+                "key-switching dot product (cp_dot), %d terms, nphi 32768, k 16" % nt, e)
+
+    W["dot"] = dot
     W["bfv_chain"] = chain(8192, 5, 256, 128)
     W["bfv_chain_target"] = chain(16384, 10, 256, 32)
     W["bfv_chain_large"] = chain(32768, 16, 65537, 64)
