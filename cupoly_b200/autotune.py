@@ -11,9 +11,12 @@ file keyed by GPU name and nphi (the RNS width only scales the batch, so it
 does not change the choice).  Plans with a split stage are timed in both of its
 forms (a separate element-wise kernel, or inside a thread-block cluster through
 distributed shared memory; cp_engine_set_split_mode); the cluster form is cached
-with the plan only when it is more than 2 % faster.  Engines created with log_radix = 0 from Python use the
-cached plan when one exists and the library default (radix 8, c = 13, split
-kernel) otherwise.
+with the plan only when it is more than 2 % faster.  `best_narrow_plan(nphi, wide)`
+then picks a second plan for small launches (cp_engine_set_narrow_plan): the
+candidate fastest at 16 residue transforms per launch, and the largest launch
+size at which it still beats the main plan.  Engines created with log_radix = 0
+from Python use the cached plans when they exist and the library default
+(radix 8, c = 13, split kernel, no small-launch plan) otherwise.
 """
 from __future__ import annotations
 
@@ -63,6 +66,16 @@ def cached_split_mode(nphi: int) -> int:
         return 0
 
 
+def cached_narrow_plan(nphi: int) -> Tuple[int, int, int]:
+    """Cached small-launch plan (log_radix, log_cta, max_units) for this GPU and nphi;
+    (0, 0, 0) when none is cached."""
+    try:
+        ent = _load().get(_key(nphi), {}).get("narrow", {})
+        return int(ent.get("log_radix", 0)), int(ent.get("log_cta", 0)), int(ent.get("max_units", 0))
+    except Exception:
+        return 0, 0, 0
+
+
 def cached_log_radix(nphi: int) -> int:
     return cached_plan(nphi)[0]
 
@@ -71,7 +84,7 @@ def candidates(nphi: int) -> List[Tuple[int, int]]:
     """(log_radix, log_cta) pairs the library compiles for this size."""
     logn = max(1, (nphi // 2).bit_length() - 1)
     out = []
-    for c in (13, 12, 11):
+    for c in (13, 12, 11, 10, 9):
         if c >= logn and c != 13:
             continue  # a cap at or above the size changes nothing: only the default is timed
         lognc = min(logn, c)
@@ -128,6 +141,76 @@ def best_plan(nphi: int, residues: int = 2048, reps: int = 5, save: bool = True)
     return best[:2]
 
 
+# Launch sizes (residue transforms per launch) at which the small-launch plan is compared
+# with the main plan.
+NARROW_UNITS = (16, 96, 384, 768, 1536)
+
+
+def _graph_ms(fn, calls: int = 10, reps: int = 5) -> float:
+    """Device milliseconds per fn() call, fn captured `calls` times in a CUDA graph so the
+    host's per-launch cost does not hide small launches."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s), torch.cuda.graph(g, stream=s):
+        for _ in range(calls):
+            fn()
+    g.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        g.replay()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / (reps * calls)
+    del g
+    return ms
+
+
+def best_narrow_plan(nphi: int, wide: Tuple[int, int], save: bool = True) -> Tuple[int, int, int]:
+    """Small-launch plan for this nphi: the candidate fastest at the smallest launch size
+    (forward + inverse DGT, CUDA-graph timed), used up to the largest size of NARROW_UNITS,
+    counted up from the smallest, at which it beats the main plan `wide` by more than 2 %.
+    Returns (log_radix, log_cta, max_units); max_units = 0 when the main plan is as fast."""
+    from .engine import FORWARD, INVERSE, UNIFORM, Engine
+
+    cands = candidates(nphi)
+    if tuple(wide) not in cands:
+        cands.append(tuple(wide))
+    e = Engine(1, 1, nphi, 256, wide[0] or 3)
+    times = {}
+    for U in NARROW_UNITS:
+        x = e.empty(0, U)
+        e.sample(x, 0, UNIFORM, 1, 0, npolys=U, to_dgt=False)
+        for r, c in cands:
+            e.set_plan(r, c)
+            times[(r, c, U)] = _graph_ms(lambda: (e.dgt(x, 0, FORWARD), e.dgt(x, 0, INVERSE)))
+        del x
+    del e
+    u0 = NARROW_UNITS[0]
+    narrow = min(cands, key=lambda rc: times[(rc[0], rc[1], u0)])
+    max_units = 0
+    if narrow != tuple(wide):
+        for U in NARROW_UNITS:
+            if times[narrow + (U,)] * 1.02 < times[tuple(wide) + (U,)]:
+                max_units = U
+            else:
+                break
+    if save:
+        data = _load()
+        ent = data.setdefault(_key(nphi), {})
+        ent["narrow"] = {"log_radix": narrow[0], "log_cta": narrow[1], "max_units": max_units,
+                         "ms_fwd_inv": {"r%d_c%d_u%d" % k: round(v, 4) for k, v in times.items()}}
+        os.makedirs(os.path.dirname(cache_path()), exist_ok=True)
+        with open(cache_path(), "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+    return narrow[0], narrow[1], max_units
+
+
 def best_log_radix(nphi: int, **kw) -> int:
     return best_plan(nphi, **kw)[0]
 
@@ -139,5 +222,6 @@ if __name__ == "__main__":
     ap.add_argument("--nphi", default="2048,4096,8192,16384,32768,65536")
     a = ap.parse_args()
     for n in [int(x) for x in a.nphi.split(",")]:
-        print(json.dumps({"nphi": n, "plan": best_plan(n)}), flush=True)
+        wide = best_plan(n)
+        print(json.dumps({"nphi": n, "plan": wide, "narrow": best_narrow_plan(n, wide)}), flush=True)
     print(json.dumps(_load(), indent=1))

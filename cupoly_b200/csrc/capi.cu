@@ -201,6 +201,39 @@ int cp_engine_set_plan(cp_engine* h, int log_radix, int log_cta) {
   return build_tables_nothrow(e);
 }
 
+int cp_engine_set_narrow_plan(cp_engine* h, int log_radix, int log_cta, long long max_units) {
+  CP_REQUIRE(h, "cp_engine_set_narrow_plan: NULL engine");
+  CP_REQUIRE(max_units >= 0, "cp_engine_set_narrow_plan: max_units must be >= 0");
+  Engine& e = h->e;
+  if (max_units > 0) {
+    CP_REQUIRE(log_radix == 0 || (log_radix >= 2 && log_radix <= 4),
+               "cp_engine_set_narrow_plan: log_radix must be 0, 2, 3 or 4");
+    const int lc = log_cta ? log_cta : kMaxLogNc;
+    CP_REQUIRE(lc >= 8 && lc <= kMaxLogNc, "cp_engine_set_narrow_plan: log_cta must be 0 or in [8, 13]");
+    CP_REQUIRE(e.logN - (e.logN < lc ? e.logN : lc) <= 2,
+               "cp_engine_set_narrow_plan: at most 2 split bits (log N - log_cta)");
+  }
+  cudaDeviceSynchronize();
+  free_tables(e);
+  if (max_units > 0) {
+    e.plan_narrow = make_plan(e.logN, log_radix ? log_radix : 3, log_cta ? log_cta : kMaxLogNc);
+    e.plan_narrow.cluster = 0;
+  } else {
+    e.plan_narrow = DgtPlan{};
+  }
+  e.narrow_units = max_units;
+  return build_tables_nothrow(e);
+}
+
+int cp_engine_get_narrow_plan(const cp_engine* h, int* log_radix, int* log_cta, long long* max_units) {
+  CP_REQUIRE(h, "cp_engine_get_narrow_plan: NULL engine");
+  const Engine& e = h->e;
+  if (log_radix) *log_radix = e.narrow_units > 0 ? e.plan_narrow.logR : 0;
+  if (log_cta) *log_cta = e.narrow_units > 0 ? e.plan_narrow.logNc : 0;
+  if (max_units) *max_units = e.narrow_units;
+  return CP_OK;
+}
+
 int cp_engine_set_split_mode(cp_engine* h, int mode) {
   CP_REQUIRE(h, "cp_engine_set_split_mode: NULL engine");
   CP_REQUIRE(mode == 0 || mode == 1, "cp_engine_set_split_mode: mode must be 0 (split kernel) or 1 (cluster)");

@@ -29,12 +29,13 @@ unsigned persistent_grid(K kernel, int threads, int smem, std::atomic<int>& resi
 }
 
 template <int LOGNC, int LOGR>
-int run_cta(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres, int rid_off,
-            int npolys, long long poly_stride, bool inverse, bool twist, cudaStream_t st, const int* rid_list) {
+int run_cta(const Engine& e, const DgtPlan& P, const DgtTableLayout& L, ulonglong2* data, const ulonglong2* fsrc,
+            const InvSrc& isrc, int nres, int rid_off, int npolys, long long poly_stride, bool inverse, bool twist,
+            cudaStream_t st, const int* rid_list) {
   constexpr int T = (1 << LOGNC) >> LOGR;
   constexpr int smem = dgt_smem_bytes<LOGNC, LOGR>();
-  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc, rid_list};
-  const int S = e.plan.S;
+  DgtArgs A{e.d_tab, L.stride, L, e.d_mc, rid_list};
+  const int S = P.S;
   const long long blocks = (long long)npolys * nres << S;
   if (blocks <= 0) return 0;
   if (blocks > 0x7fffffffLL) {
@@ -59,8 +60,8 @@ int run_cta(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const Inv
   return check_launch("dgt");
 }
 
-using RunFn = int (*)(const Engine&, ulonglong2*, const ulonglong2*, const InvSrc&, int, int, int, long long, bool,
-                      bool, cudaStream_t, const int*);
+using RunFn = int (*)(const Engine&, const DgtPlan&, const DgtTableLayout&, ulonglong2*, const ulonglong2*,
+                      const InvSrc&, int, int, int, long long, bool, bool, cudaStream_t, const int*);
 
 constexpr int kNoCluster = -1;  // the cluster form cannot be scheduled on this device: use the split kernel
 
@@ -68,12 +69,12 @@ constexpr int kNoCluster = -1;  // the cluster form cannot be scheduled on this 
 // per unit: the cluster's CTAs are the chunks of one residue).  Returns kNoCluster,
 // having launched nothing, when the device cannot co-schedule such a cluster.
 template <int LOGNC, int LOGR, int CL>
-int run_cluster(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres,
-                int rid_off, int npolys, long long poly_stride, bool inverse, bool, cudaStream_t st,
-                const int* rid_list) {
+int run_cluster(const Engine& e, const DgtPlan&, const DgtTableLayout& L, ulonglong2* data, const ulonglong2* fsrc,
+                const InvSrc& isrc, int nres, int rid_off, int npolys, long long poly_stride, bool inverse, bool,
+                cudaStream_t st, const int* rid_list) {
   constexpr int T = (1 << LOGNC) >> LOGR;
   constexpr int smem = dgt_smem_bytes<LOGNC, LOGR>();
-  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc, rid_list};
+  DgtArgs A{e.d_tab, L.stride, L, e.d_mc, rid_list};
   const long long blocks = (long long)npolys * nres << CL;
   if (blocks <= 0) return 0;
   if (blocks > 0x7fffffffLL) {
@@ -132,12 +133,13 @@ RunFn pick_cluster(int logNc, int logR, int S) {
 
 // The plan's split stage inside a cluster, when the plan asks for it and a kernel exists;
 // returns kNoCluster otherwise (nothing launched).
-int try_cluster(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres, int rid_off,
-                int npolys, long long poly_stride, bool inverse, cudaStream_t st, const int* rid_list) {
-  if (!e.plan.cluster || e.plan.S == 0) return kNoCluster;
-  RunFn fc = pick_cluster(e.plan.logNc, e.plan.logR, e.plan.S);
+int try_cluster(const Engine& e, const DgtPlan& P, const DgtTableLayout& L, ulonglong2* data, const ulonglong2* fsrc,
+                const InvSrc& isrc, int nres, int rid_off, int npolys, long long poly_stride, bool inverse,
+                cudaStream_t st, const int* rid_list) {
+  if (!P.cluster || P.S == 0) return kNoCluster;
+  RunFn fc = pick_cluster(P.logNc, P.logR, P.S);
   if (!fc) return kNoCluster;
-  return fc(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, inverse, false, st, rid_list);
+  return fc(e, P, L, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, inverse, false, st, rid_list);
 }
 
 // (logNc, effective logR) -> instantiation.
@@ -154,16 +156,17 @@ RunFn pick(int logNc, int logR) {
   return nullptr;
 }
 
-int launch_split(const Engine& e, ulonglong2* data, const ulonglong2* src, int nres, int rid_off, int npolys,
-                 long long poly_stride, bool inverse, cudaStream_t st, const int* rid_list = nullptr) {
-  DgtArgs A{e.d_tab, e.layout.stride, e.layout, e.d_mc, rid_list};
-  const int Nc = 1 << e.plan.logNc;
+int launch_split(const Engine& e, const DgtPlan& P, const DgtTableLayout& L, ulonglong2* data, const ulonglong2* src,
+                 int nres, int rid_off, int npolys, long long poly_stride, bool inverse, cudaStream_t st,
+                 const int* rid_list = nullptr) {
+  DgtArgs A{e.d_tab, L.stride, L, e.d_mc, rid_list};
+  const int Nc = 1 << P.logNc;
   const long long blocks = (long long)npolys * nres * (Nc / 256);
   if (blocks > 0x7fffffffLL) {
     set_error("dgt: grid too large");
     return 1;
   }
-  const int S = e.plan.S, lc = e.plan.logNc, lr = e.plan.logR;
+  const int S = P.S, lc = P.logNc, lr = P.logR;
   if (!inverse) {
     if (S == 1)
       k_dgt_split<1, false><<<(unsigned)blocks, 256, 0, st>>>(data, src, A, nres, rid_off, poly_stride, lc, lr);
@@ -176,6 +179,53 @@ int launch_split(const Engine& e, ulonglong2* data, const ulonglong2* src, int n
       k_dgt_split<2, true><<<(unsigned)blocks, 256, 0, st>>>(data, nullptr, A, nres, rid_off, poly_stride, lc, lr);
   }
   return check_launch("dgt split");
+}
+
+// The plan of a launch of `units` residue transforms: the small-launch plan when the
+// engine has one and the launch is at most its size, else the main plan.
+struct PlanSel {
+  const DgtPlan& P;
+  const DgtTableLayout& L;
+};
+PlanSel select_plan(const Engine& e, long long units) {
+  if (e.narrow_units > 0 && units <= e.narrow_units) return {e.plan_narrow, e.layout_narrow};
+  return {e.plan, e.layout};
+}
+
+}  // namespace
+
+namespace {
+
+// One transform of npolys x nres residues with the plan selected for that many units:
+// forward = split stage (when any) then the in-CTA kernel, which also twists when there is
+// no split stage; inverse = the in-CTA kernel (untwisting when there is no split stage)
+// then the split stage.  With the cluster form the split stage runs inside the kernel.
+int run_transform(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, const InvSrc& isrc, int nres,
+                  int rid_off, int npolys, long long poly_stride, bool inverse, cudaStream_t st, const int* rid_list) {
+  const PlanSel ps = select_plan(e, (long long)npolys * nres);
+  const DgtPlan& P = ps.P;
+  const DgtTableLayout& L = ps.L;
+  RunFn fn = pick(P.logNc, P.logR);
+  if (!fn) {
+    set_error("dgt: no kernel for this size");
+    return 3;
+  }
+  {
+    const int rc = try_cluster(e, P, L, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, inverse, st, rid_list);
+    if (rc != kNoCluster) return rc;
+  }
+  const int S = P.S;
+  if (!inverse) {
+    if (S > 0) {
+      int rc = launch_split(e, P, L, data, fsrc, nres, rid_off, npolys, poly_stride, false, st, rid_list);
+      if (rc) return rc;
+      return fn(e, P, L, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, false, false, st, rid_list);
+    }
+    return fn(e, P, L, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, false, true, st, rid_list);
+  }
+  int rc = fn(e, P, L, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, true, S == 0, st, rid_list);
+  if (rc || S == 0) return rc;
+  return launch_split(e, P, L, data, nullptr, nres, rid_off, npolys, poly_stride, true, st, rid_list);
 }
 
 }  // namespace
@@ -192,11 +242,6 @@ int launch_dgt_ex(const Engine& e, void* dst_v, const void* fsrc_v, const InvSrc
   ulonglong2* data = reinterpret_cast<ulonglong2*>(dst_v);
   const ulonglong2* fsrc = reinterpret_cast<const ulonglong2*>(fsrc_v);
   if (poly_stride == 0) poly_stride = (long long)nres * e.N;
-  RunFn fn = pick(e.plan.logNc, e.plan.logR);
-  if (!fn) {
-    set_error("dgt: no kernel for this size");
-    return 3;
-  }
   InvSrc isrc{};
   if (isrc_p) {
     isrc = *isrc_p;
@@ -205,22 +250,7 @@ int launch_dgt_ex(const Engine& e, void* dst_v, const void* fsrc_v, const InvSrc
     isrc.mode = 0;
     isrc.npairs = 1;
   }
-  const int S = e.plan.S;
-  {
-    const int rc = try_cluster(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, inverse, st, nullptr);
-    if (rc != kNoCluster) return rc;
-  }
-  if (!inverse) {
-    if (S > 0) {
-      int rc = launch_split(e, data, fsrc, nres, rid_off, npolys, poly_stride, false, st);
-      if (rc) return rc;
-      return fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, false, false, st, nullptr);
-    }
-    return fn(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, false, true, st, nullptr);
-  }
-  int rc = fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, true, S == 0, st, nullptr);
-  if (rc || S == 0) return rc;
-  return launch_split(e, data, nullptr, nres, rid_off, npolys, poly_stride, true, st);
+  return run_transform(e, data, fsrc, isrc, nres, rid_off, npolys, poly_stride, inverse, st, nullptr);
 }
 
 // Residues rid_off .. rid_off + nres - 1 of npolys polynomials (stride poly_stride
@@ -228,33 +258,13 @@ int launch_dgt_ex(const Engine& e, void* dst_v, const void* fsrc_v, const InvSrc
 int launch_dgt_part(const Engine& e, void* dst_v, const void* src_v, int rid_off, int nres, int npolys,
                     long long poly_stride, bool inverse, cudaStream_t st) {
   if (nres <= 0 || npolys <= 0) return 0;
-  RunFn fn = pick(e.plan.logNc, e.plan.logR);
-  if (!fn) {
-    set_error("dgt: no kernel for this size");
-    return 3;
-  }
   ulonglong2* data = reinterpret_cast<ulonglong2*>(dst_v);
   const ulonglong2* src = reinterpret_cast<const ulonglong2*>(src_v);
   InvSrc isrc{};
   isrc.p[0] = src ? src : data;
   isrc.mode = 0;
   isrc.npairs = 1;
-  const int S = e.plan.S;
-  {
-    const int rc = try_cluster(e, data, src, isrc, nres, rid_off, npolys, poly_stride, inverse, st, nullptr);
-    if (rc != kNoCluster) return rc;
-  }
-  if (!inverse) {
-    if (S > 0) {
-      int rc = launch_split(e, data, src, nres, rid_off, npolys, poly_stride, false, st);
-      if (rc) return rc;
-      return fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, false, false, st, nullptr);
-    }
-    return fn(e, data, src, isrc, nres, rid_off, npolys, poly_stride, false, true, st, nullptr);
-  }
-  int rc = fn(e, data, nullptr, isrc, nres, rid_off, npolys, poly_stride, true, S == 0, st, nullptr);
-  if (rc || S == 0) return rc;
-  return launch_split(e, data, nullptr, nres, rid_off, npolys, poly_stride, true, st);
+  return run_transform(e, data, src, isrc, nres, rid_off, npolys, poly_stride, inverse, st, nullptr);
 }
 
 int launch_dgt(const Engine& e, void* data, int base, int npolys, long long poly_stride, bool inverse,
@@ -274,11 +284,6 @@ int launch_dgt_list(const Engine& e, void* data_v, const int* rid_list, int nlis
 int launch_dgt_list_ex(const Engine& e, void* data_v, const void* fsrc_v, const InvSrc* isrc_p, const int* rid_list,
                        int nlist, bool inverse, cudaStream_t st) {
   if (nlist <= 0) return 0;
-  RunFn fn = pick(e.plan.logNc, e.plan.logR);
-  if (!fn) {
-    set_error("dgt: no kernel for this size");
-    return 3;
-  }
   ulonglong2* data = reinterpret_cast<ulonglong2*>(data_v);
   const ulonglong2* fsrc = reinterpret_cast<const ulonglong2*>(fsrc_v);
   InvSrc isrc{};
@@ -289,23 +294,7 @@ int launch_dgt_list_ex(const Engine& e, void* data_v, const void* fsrc_v, const 
     isrc.mode = 0;
     isrc.npairs = 1;
   }
-  const long long stride = e.N;
-  const int S = e.plan.S;
-  {
-    const int rc = try_cluster(e, data, fsrc, isrc, 1, 0, nlist, stride, inverse, st, rid_list);
-    if (rc != kNoCluster) return rc;
-  }
-  if (!inverse) {
-    if (S > 0) {
-      int rc = launch_split(e, data, fsrc, 1, 0, nlist, stride, false, st, rid_list);
-      if (rc) return rc;
-      return fn(e, data, nullptr, isrc, 1, 0, nlist, stride, false, false, st, rid_list);
-    }
-    return fn(e, data, fsrc, isrc, 1, 0, nlist, stride, false, true, st, rid_list);
-  }
-  int rc = fn(e, data, nullptr, isrc, 1, 0, nlist, stride, true, S == 0, st, rid_list);
-  if (rc || S == 0) return rc;
-  return launch_split(e, data, nullptr, 1, 0, nlist, stride, true, st, rid_list);
+  return run_transform(e, data, fsrc, isrc, 1, 0, nlist, (long long)e.N, inverse, st, rid_list);
 }
 
 }  // namespace cpoly

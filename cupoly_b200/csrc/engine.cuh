@@ -102,6 +102,14 @@ struct Engine {
   std::vector<std::pair<uint64_t, uint64_t>> xi;  // Gaussian root of i used for the twist, per residue
   DgtPlan plan;
   DgtTableLayout layout;
+  // Small-launch plan: a launch of at most narrow_units residue transforms (polynomials x
+  // residues) uses plan_narrow / layout_narrow instead (0: no such plan).  With few residues
+  // per launch, one CTA per residue leaves most SMs idle; a plan whose split stage spreads
+  // each residue over 2-4 CTAs finishes sooner.  Its radix, pass and split tables follow the
+  // main plan's in each residue block; the twist tables are shared.
+  DgtPlan plan_narrow;
+  DgtTableLayout layout_narrow;
+  long long narrow_units = 0;
 
   // device allocations
   ModConst* d_mc = nullptr;

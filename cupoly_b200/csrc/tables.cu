@@ -143,16 +143,11 @@ DgtPlan make_plan(int logN, int logR, int logCta) {
   return P;
 }
 
-int build_tables(Engine& e) {
-  const int nres = e.k + e.kl;
-  const int N = e.N;
-  const int Nc = 1 << e.plan.logNc;
-  const int R = 1 << e.plan.logR;
-  const DgtPlan& P = e.plan;
-  DgtTableLayout& L = e.layout;
-  int off = 0;
+// Place a plan's radix, pass and split tables from entry `off` of a residue block;
+// returns the next free entry.
+static int place_plan(const DgtPlan& P, int N, DgtTableLayout& L, int off) {
   L.off_rad = off;
-  off += R;
+  off += 1 << P.logR;
   for (int i = 0; i < P.npass; ++i) {
     if (P.p[i] > 0) {
       L.off_fwd[i] = off;
@@ -167,11 +162,27 @@ int build_tables(Engine& e) {
     L.off_split_inv = off;
     off += N;
   }
+  return off;
+}
+
+int build_tables(Engine& e) {
+  const int nres = e.k + e.kl;
+  const int N = e.N;
+  const bool narrow = e.narrow_units > 0;
+  DgtTableLayout& L = e.layout;
+  DgtTableLayout& L2 = e.layout_narrow;
+  L = DgtTableLayout{};
+  L2 = DgtTableLayout{};
+  int off = place_plan(e.plan, N, L, 0);
+  if (narrow) off = place_plan(e.plan_narrow, N, L2, off);
   L.off_twist = off;
   off += 3 * N;
   L.off_untwist = off;
   off += 3 * N;
   L.stride = (off + 1) & ~1;
+  L2.off_twist = L.off_twist;
+  L2.off_untwist = L.off_untwist;
+  L2.stride = L.stride;
 
   std::vector<ulonglong2> tab((size_t)L.stride * nres);
   parallel_for(nres, [&](int r) {
@@ -188,31 +199,37 @@ int build_tables(Engine& e) {
       pwi[i] = h_mulmod(pwi[i - 1], wNi, p);
     }
     auto put = [&](int idx, uint64_t w) { T[idx] = make_ulonglong2(w, h_shoup(w, p)); };
-    for (int j = 0; j < R; ++j) put(L.off_rad + j, pw[(size_t)j * (N / R)]);
-    for (int i = 0; i < P.npass; ++i) {
-      if (P.p[i] == 0) continue;
-      const int pp = P.p[i], ww = P.w[i];
-      const int M = 1 << (pp + ww);
-      const int step = N / M;  // w_M = w_N^step
-      for (int pos = 0; pos < (1 << ww); ++pos) {
-        const int kk = brev(pos, ww);
-        for (int Lw = 0; Lw < (1 << pp); ++Lw) {
-          const size_t e_ = (size_t)Lw * kk % M * step;
-          put(L.off_fwd[i] + pos * (1 << pp) + Lw, pw[e_]);
-          put(L.off_inv[i] + pos * (1 << pp) + Lw, pwi[e_]);
+    auto fill_plan = [&](const DgtPlan& P, const DgtTableLayout& Lp) {
+      const int R = 1 << P.logR;
+      const int Nc = 1 << P.logNc;
+      for (int j = 0; j < R; ++j) put(Lp.off_rad + j, pw[(size_t)j * (N / R)]);
+      for (int i = 0; i < P.npass; ++i) {
+        if (P.p[i] == 0) continue;
+        const int pp = P.p[i], ww = P.w[i];
+        const int M = 1 << (pp + ww);
+        const int step = N / M;  // w_M = w_N^step
+        for (int pos = 0; pos < (1 << ww); ++pos) {
+          const int kk = brev(pos, ww);
+          for (int Lw = 0; Lw < (1 << pp); ++Lw) {
+            const size_t e_ = (size_t)Lw * kk % M * step;
+            put(Lp.off_fwd[i] + pos * (1 << pp) + Lw, pw[e_]);
+            put(Lp.off_inv[i] + pos * (1 << pp) + Lw, pwi[e_]);
+          }
         }
       }
-    }
-    if (P.S > 0) {
-      for (int pos = 0; pos < (1 << P.S); ++pos) {
-        const int kk = brev(pos, P.S);
-        for (int Lw = 0; Lw < Nc; ++Lw) {
-          const size_t e_ = (size_t)Lw * kk % N;
-          put(L.off_split_fwd + pos * Nc + Lw, pw[e_]);
-          put(L.off_split_inv + pos * Nc + Lw, pwi[e_]);
+      if (P.S > 0) {
+        for (int pos = 0; pos < (1 << P.S); ++pos) {
+          const int kk = brev(pos, P.S);
+          for (int Lw = 0; Lw < Nc; ++Lw) {
+            const size_t e_ = (size_t)Lw * kk % N;
+            put(Lp.off_split_fwd + pos * Nc + Lw, pw[e_]);
+            put(Lp.off_split_inv + pos * Nc + Lw, pwi[e_]);
+          }
         }
       }
-    }
+    };
+    fill_plan(e.plan, L);
+    if (narrow) fill_plan(e.plan_narrow, L2);
     // twist by xi^n and untwist by xi^-n * N^-1
     G xi{e.xi[r].first, e.xi[r].second};
     G xii = gpow(xi, 4 * (uint64_t)N - 1, p);

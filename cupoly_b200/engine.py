@@ -100,12 +100,13 @@ class Engine:
         if not torch.cuda.is_available():
             raise RuntimeError("cupoly_b200 needs a CUDA device")
         _lib.lib()
-        log_cta, split_mode = 0, 0
-        if log_radix == 0:  # use the autotuner's plan for this GPU and size when one is cached
-            from .autotune import cached_plan, cached_split_mode
+        log_cta, split_mode, narrow = 0, 0, (0, 0, 0)
+        if log_radix == 0:  # use the autotuner's plans for this GPU and size when cached
+            from .autotune import cached_narrow_plan, cached_plan, cached_split_mode
 
             log_radix, log_cta = cached_plan(nphi)
             split_mode = cached_split_mode(nphi)
+            narrow = cached_narrow_plan(nphi)
         h = C.c_void_p()
         if ckks_prec:
             call("cp_ckks_engine_create", C.byref(h), k, kl, nphi, ckks_prec, log_radix)
@@ -117,6 +118,8 @@ class Engine:
             call("cp_engine_set_plan", h, log_radix, log_cta)
         if split_mode:
             call("cp_engine_set_split_mode", h, split_mode)
+        if narrow[2] > 0:
+            call("cp_engine_set_narrow_plan", h, narrow[0], narrow[1], narrow[2])
         self.log_radix = log_radix
         self._h = h
         self.k = k
@@ -143,6 +146,15 @@ class Engine:
 
     def get_split_mode(self) -> int:
         return int(_lib.lib().cp_engine_get_split_mode(self._h))
+
+    def set_narrow_plan(self, log_radix: int, log_cta: int, max_units: int):
+        """Plan for launches of at most max_units residue transforms (0 removes it); rebuilds the tables."""
+        call("cp_engine_set_narrow_plan", self._h, log_radix, log_cta, int(max_units))
+
+    def get_narrow_plan(self):
+        r, c, u = C.c_int(), C.c_int(), C.c_longlong()
+        call("cp_engine_get_narrow_plan", self._h, C.byref(r), C.byref(c), C.byref(u))
+        return {"log_radix": r.value, "log_cta": c.value, "max_units": u.value}
 
     def get_plan(self):
         r, c, s = C.c_int(), C.c_int(), C.c_int()

@@ -86,6 +86,16 @@ int cp_engine_ckks_prec(const cp_engine* e);
  * (cupoly_b200/autotune.py) measures the candidates and caches the fastest. */
 int cp_engine_set_plan(cp_engine* e, int log_radix, int log_cta);
 int cp_engine_get_plan(const cp_engine* e, int* log_radix, int* log_cta, int* split_bits);
+/* Second DGT plan for small launches (no counterpart in cuPoly): a transform launch of at
+ * most max_units residue transforms (polynomials x residues) uses (log_radix, log_cta)
+ * instead of the main plan; max_units = 0 removes it.  With few residues per launch, one
+ * CTA per residue leaves most SMs idle, and a plan whose split stage spreads each residue
+ * over 2-4 CTAs finishes sooner.  Results are identical.  Same limits as cp_engine_set_plan;
+ * the split stage of this plan is always the separate kernel.  Rebuilds the engine's
+ * tables (synchronises the device).  The autotuner picks the plan and the crossover.
+ * get: zeros when there is no such plan. */
+int cp_engine_set_narrow_plan(cp_engine* e, int log_radix, int log_cta, long long max_units);
+int cp_engine_get_narrow_plan(const cp_engine* e, int* log_radix, int* log_cta, long long* max_units);
 /* Form of the split stage of transforms larger than one CTA (plans with split bits > 0; no
  * counterpart in cuPoly, whose two-pass split always goes through HBM):
  * 0 = a separate element-wise kernel with its own HBM pass (default);

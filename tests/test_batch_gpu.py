@@ -196,3 +196,62 @@ def test_cluster_split_stage_in_the_fused_calls(gpu):
             out[mode] = (c3.clone(), pm.clone())
         assert torch.equal(out[0][0], out[1][0]), nphi
         assert torch.equal(out[0][1], out[1][1]), nphi
+
+
+@pytest.mark.parametrize("nphi,k,t,narrow,main", [(8192, 3, 256, 10, 13), (4096, 2, 256, 9, 13),
+                                                  (32768, 2, 65537, 12, 13)])
+def test_small_launch_plan_gives_the_same_bytes(gpu, nphi, k, t, narrow, main):
+    """With a small-launch plan set, launches at or below its size run with it and larger ones
+    with the main plan; the DGT (oracle-checked), the work-list DGT, the fused polymul and the
+    batched BFV chain give the bytes of the single-plan engine either way."""
+    import ctypes as C
+
+    import torch
+
+    from cupoly_b200._lib import call
+    from cupoly_b200.engine import FORWARD, INVERSE, QBase, UNIFORM, Engine, from_u64, to_u64
+    from oracle import coracle
+    e = Engine(k, 0, nphi, t)
+    e.set_plan(3, main)
+    e.set_narrow_plan(0, 0, 0)
+    assert e.get_narrow_plan()["max_units"] == 0
+    x = random_poly_residues(nphi + 5, e.Q, nphi)
+    ref = coracle.dgt(fold(x)[None], e.Q)
+    P = 3
+    ins = []
+    for j in range(4):
+        v = e.empty(QBase, P)
+        e.sample(v, QBase, UNIFORM, 7, 16 * j, npolys=P, to_dgt=True)
+        ins.append(v)
+    ws, pws = e.bfv_mul_batch_workspace(P), e.polymul_workspace(QBase, P)
+    rid = torch.tensor([i % k for i in range(P * k)], dtype=torch.int32, device="cuda")
+
+    def run():
+        d = from_u64(fold(x)[None])
+        e.dgt(d, 0, FORWARD)
+        fwd = to_u64(d).copy()
+        e.dgt(d, 0, INVERSE)
+        back = to_u64(d)[0].copy()
+        c3 = e.empty(QBase, 3 * P)
+        e.bfv_mul_batch(c3, *ins, P, ws)
+        pm = e.empty(QBase, P)
+        e.polymul(pm, ins[0], ins[1], QBase, pws, P)
+        lst = ins[2].clone()
+        call("cp_dgt_list", e.handle, C.c_void_p(lst.data_ptr()), C.c_void_p(rid.data_ptr()), P * k, INVERSE,
+             C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        return fwd, back, c3.clone(), pm.clone(), lst
+
+    base = run()
+    assert np.array_equal(base[0], ref) and np.array_equal(base[1], fold(x))
+    # every launch of run() has at most 4 P k residue transforms: all of them take the
+    # small-launch plan with a large limit, none with limit 1 (single-residue launches aside)
+    for units in (4 * P * (k + 1), 1):
+        e.set_narrow_plan(3, narrow, units)
+        got = e.get_narrow_plan()
+        assert got["max_units"] == units and got["log_cta"] == min(narrow, (nphi // 2).bit_length() - 1)
+        out = run()
+        assert np.array_equal(out[0], ref) and np.array_equal(out[1], fold(x)), units
+        for a, b in zip(base[2:], out[2:]):
+            assert torch.equal(a, b), units
+    e.set_narrow_plan(0, 0, 0)
