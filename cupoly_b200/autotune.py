@@ -110,6 +110,7 @@ def best_plan(nphi: int, residues: int = 2048, reps: int = 5, save: bool = True)
     npolys = max(1, residues // 2)
     for r, c in candidates(nphi):
         e = Engine(2, 1, nphi, 256, r)
+        e.set_narrow_plan(0, 0, 0)  # every launch timed with the candidate
         e.set_plan(r, c)
         x = e.empty(0, npolys)
         e.sample(x, 0, UNIFORM, 1, 0, npolys=npolys, to_dgt=False)
@@ -182,6 +183,7 @@ def best_narrow_plan(nphi: int, wide: Tuple[int, int], save: bool = True) -> Tup
     if tuple(wide) not in cands:
         cands.append(tuple(wide))
     e = Engine(1, 1, nphi, 256, wide[0] or 3)
+    e.set_narrow_plan(0, 0, 0)  # every launch timed with the candidate
     times = {}
     for U in NARROW_UNITS:
         x = e.empty(0, U)

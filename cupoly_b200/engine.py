@@ -100,13 +100,14 @@ class Engine:
         if not torch.cuda.is_available():
             raise RuntimeError("cupoly_b200 needs a CUDA device")
         _lib.lib()
-        log_cta, split_mode, narrow = 0, 0, (0, 0, 0)
+        log_cta, split_mode, narrow = 0, 0, None
         if log_radix == 0:  # use the autotuner's plans for this GPU and size when cached
             from .autotune import cached_narrow_plan, cached_plan, cached_split_mode
 
             log_radix, log_cta = cached_plan(nphi)
             split_mode = cached_split_mode(nphi)
-            narrow = cached_narrow_plan(nphi)
+            if log_radix:  # a tuned entry replaces the library's default small-launch plan
+                narrow = cached_narrow_plan(nphi)
         h = C.c_void_p()
         if ckks_prec:
             call("cp_ckks_engine_create", C.byref(h), k, kl, nphi, ckks_prec, log_radix)
@@ -118,7 +119,7 @@ class Engine:
             call("cp_engine_set_plan", h, log_radix, log_cta)
         if split_mode:
             call("cp_engine_set_split_mode", h, split_mode)
-        if narrow[2] > 0:
+        if narrow is not None:
             call("cp_engine_set_narrow_plan", h, narrow[0], narrow[1], narrow[2])
         self.log_radix = log_radix
         self._h = h

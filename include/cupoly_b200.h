@@ -93,7 +93,8 @@ int cp_engine_get_plan(const cp_engine* e, int* log_radix, int* log_cta, int* sp
  * over 2-4 CTAs finishes sooner.  Results are identical.  Same limits as cp_engine_set_plan;
  * the split stage of this plan is always the separate kernel.  Rebuilds the engine's
  * tables (synchronises the device).  The autotuner picks the plan and the crossover.
- * get: zeros when there is no such plan. */
+ * Default for nphi >= 4096: radix 4 (log_radix 2), log_cta = log2(nphi / 2) - 2, up to 96
+ * units, when that differs from the main plan.  get: zeros when there is no such plan. */
 int cp_engine_set_narrow_plan(cp_engine* e, int log_radix, int log_cta, long long max_units);
 int cp_engine_get_narrow_plan(const cp_engine* e, int* log_radix, int* log_cta, long long* max_units);
 /* Form of the split stage of transforms larger than one CTA (plans with split bits > 0; no

@@ -255,3 +255,32 @@ def test_small_launch_plan_gives_the_same_bytes(gpu, nphi, k, t, narrow, main):
         for a, b in zip(base[2:], out[2:]):
             assert torch.equal(a, b), units
     e.set_narrow_plan(0, 0, 0)
+
+
+def test_default_and_cached_small_launch_plans(gpu, tmp_path, monkeypatch):
+    """Engines start with the library's small-launch plan (radix 4, 2 split bits, up to 96
+    residue transforms) from nphi 4096 up while the main plan has fewer split bits; a tuned
+    cache entry replaces it, including by none."""
+    import json
+    monkeypatch.setenv("CUPOLY_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    from cupoly_b200 import autotune
+    from cupoly_b200.engine import Engine
+    for nphi, exp in ((2048, 0), (4096, 9), (8192, 10), (16384, 11), (32768, 12), (65536, 0)):
+        got = Engine(1, 1, nphi, 65537 if nphi >= 32768 else 256).get_narrow_plan()
+        if exp:
+            assert got == {"log_radix": 2, "log_cta": exp, "max_units": 96}, nphi
+        else:
+            assert got["max_units"] == 0, nphi
+    wide = autotune.best_plan(8192, residues=128, reps=2)
+    narrow = autotune.best_narrow_plan(8192, wide)
+    assert narrow[:2] in autotune.candidates(8192) + [tuple(wide)]
+    assert narrow[2] in (0,) + autotune.NARROW_UNITS
+    assert autotune.cached_narrow_plan(8192) == narrow
+    ent = next(iter(json.load(open(tmp_path / "tune.json")).values()))
+    assert len(ent["narrow"]["ms_fwd_inv"]) == len(autotune.NARROW_UNITS) * len(
+        set(autotune.candidates(8192)) | {tuple(wide)})
+    got = Engine(2, 0, 8192, 256).get_narrow_plan()
+    if narrow[2]:
+        assert (got["log_radix"], got["log_cta"], got["max_units"]) == narrow
+    else:
+        assert got["max_units"] == 0
