@@ -274,10 +274,30 @@ def _dot_row(seed: int, hbm_peak: float):
     poly = d.k * d.N * 16
     byt = (2 * nt + 1) * poly
     d.check()
-    return {"config": "nphi=%d, k=%d, %d terms" % (d.nphi, d.k, nt), "fused_us": round(ms_f * 1e3, 2),
-            "composed_us": round(ms_c * 1e3, 2), "speedup": round(ms_c / ms_f, 2),
-            "GB_per_s": round(byt / ms_f / 1e6, 1), "frac_hbm": round(byt / ms_f / 1e6 / hbm_peak, 4),
-            "bytes_per_call": byt, "composed_bytes_per_call": (3 + 4 * (nt - 1)) * poly}
+    row = {"config": "nphi=%d, k=%d, %d terms" % (d.nphi, d.k, nt), "fused_us": round(ms_f * 1e3, 2),
+           "composed_us": round(ms_c * 1e3, 2), "speedup": round(ms_c / ms_f, 2),
+           "GB_per_s": round(byt / ms_f / 1e6, 1), "frac_hbm": round(byt / ms_f / 1e6 / hbm_peak, 4),
+           "bytes_per_call": byt, "composed_bytes_per_call": (3 + 4 * (nt - 1)) * poly}
+    del sets, acc, d
+    # batched relinearization inner product: the xi decomposition of 128 polynomials (nphi 8192,
+    # k 5) against one shared set of k key polynomials, one cp_dot_batch launch
+    e = Engine(K_Q, K_B, NPHI, T_PLAIN)
+    P, k = 128, e.k
+    dec = e.empty(QBase, P * k)
+    e.sample(dec, QBase, UNIFORM, seed, 70, npolys=P * k, to_dgt=False)
+    keys = e.empty(QBase, k)
+    e.sample(keys, QBase, UNIFORM, seed, 71, npolys=k, to_dgt=False)
+    out = e.empty(QBase, P)
+    gb = graph_of(lambda: e.dot_batch(out, dec, keys, k, P, QBase, b_shared=True), 1)
+    ms_b = _timed(gb.replay, 10)
+    del gb
+    pq = k * e.N * 16
+    byt_b = (P * k + k + P) * pq
+    e.check()
+    row["batch"] = {"config": "nphi=%d, k=%d: %d decompositions x %d shared keys" % (e.nphi, k, P, k),
+                    "us_per_call": round(ms_b * 1e3, 2), "us_per_polynomial": round(ms_b * 1e3 / P, 3),
+                    "GB_per_s": round(byt_b / ms_b / 1e6, 1), "frac_hbm": round(byt_b / ms_b / 1e6 / hbm_peak, 4)}
+    return row
 
 
 def next_rows(seed: int, hbm_peak: float):

@@ -76,6 +76,7 @@ SIGNATURES = {
     "cp_mul_batch": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "cp_muladd": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "cp_dot": (_i, [_vp, _vp, C.POINTER(_vp), C.POINTER(_vp), _i, _i, _vp]),
+    "cp_dot_batch": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _vp]),
     "cp_dr2": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "cp_negate": (_i, [_vp, _vp, _vp, _i, _vp]),
     "cp_op_by_int": (_i, [_vp, _vp, _vp, _i, _u64, _i, _vp]),

@@ -452,6 +452,13 @@ int cp_dot(const cp_engine* h, void* c, const void* const* a, const void* const*
   NvtxRange range("cp_dot");
   return pw_dot(h->e, c, a, b, n, base, S(stream));
 }
+int cp_dot_batch(const cp_engine* h, void* c, const void* a, const void* b, int n, int npolys, int b_shared, int base,
+                 void* stream) {
+  PW_CHECK("cp_dot_batch");
+  CP_REQUIRE(c && a && b && n >= 1 && npolys >= 0, "cp_dot_batch: NULL buffer, n < 1 or npolys < 0");
+  NvtxRange range("cp_dot_batch");
+  return pw_dot_batch(h->e, c, a, b, n, npolys, b_shared != 0, base, S(stream));
+}
 int cp_dr2(const cp_engine* h, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, void* stream) {
   PW_CHECK("cp_dr2");

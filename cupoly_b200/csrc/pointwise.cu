@@ -171,42 +171,72 @@ struct DotArgs {
   const u2* b[kDotTerms];
 };
 
+// sum_{t < n} x_t y_t mod p for one element, (x_t, y_t) = load(t).
+template <class Load>
+__device__ __forceinline__ u2 dot_elem(int n, const ModConst& m, Load load) {
+  uint64_t sr = 0, si = 0;
+  if (m.pm) {
+    uint64_t l1 = 0, h1 = 0, t1 = 0, l2 = 0, h2 = 0, t2 = 0, l3 = 0, h3 = 0, t3 = 0;
+#pragma unroll 4
+    for (int t = 0; t < n; ++t) {
+      u2 x, y;
+      load(t, x, y);
+      mac192(l1, h1, t1, x.x, y.x);
+      mac192(l2, h2, t2, x.y, y.y);
+      mac192(l3, h3, t3, x.x + x.y, y.x + y.y);
+    }
+    const uint64_t p1 = red192(l1, h1, t1, m.p, m.r1, m.r2), p2 = red192(l2, h2, t2, m.p, m.r1, m.r2),
+                   p3 = red192(l3, h3, t3, m.p, m.r1, m.r2);
+    sr = sub_mod(p1, p2, m.p);
+    si = sub_mod(sub_mod(p3, p1, m.p), p2, m.p);
+  } else {
+    for (int t = 0; t < n; ++t) {
+      u2 x, y;
+      load(t, x, y);
+      uint64_t r, im;
+      gi_mul(r, im, x.x, x.y, y.x, y.y, m);
+      sr = add_mod(sr, r, m.p);
+      si = add_mod(si, im, m.p);
+    }
+  }
+  return make_ulonglong2(sr, si);
+}
+
 __global__ void __launch_bounds__(256)
     k_dot(DotArgs args, int n, u2* c, int acc, int N, int rid_off, const ModConst* __restrict__ mc) {
   const ModConst m = mc[rid_off + blockIdx.y];
   const size_t base = (size_t)blockIdx.y * N;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
     const size_t i = base + j;
-    uint64_t sr = 0, si = 0;
-    if (m.pm) {
-      uint64_t l1 = 0, h1 = 0, t1 = 0, l2 = 0, h2 = 0, t2 = 0, l3 = 0, h3 = 0, t3 = 0;
-#pragma unroll 4
-      for (int t = 0; t < n; ++t) {
-        const u2 x = args.a[t][i], y = args.b[t][i];
-        mac192(l1, h1, t1, x.x, y.x);
-        mac192(l2, h2, t2, x.y, y.y);
-        mac192(l3, h3, t3, x.x + x.y, y.x + y.y);
-      }
-      const uint64_t p1 = red192(l1, h1, t1, m.p, m.r1, m.r2), p2 = red192(l2, h2, t2, m.p, m.r1, m.r2),
-                     p3 = red192(l3, h3, t3, m.p, m.r1, m.r2);
-      sr = sub_mod(p1, p2, m.p);
-      si = sub_mod(sub_mod(p3, p1, m.p), p2, m.p);
-    } else {
-      for (int t = 0; t < n; ++t) {
-        const u2 x = args.a[t][i], y = args.b[t][i];
-        uint64_t r, im;
-        gi_mul(r, im, x.x, x.y, y.x, y.y, m);
-        sr = add_mod(sr, r, m.p);
-        si = add_mod(si, im, m.p);
-      }
-    }
+    u2 r = dot_elem(n, m, [&](int t, u2& x, u2& y) {
+      x = args.a[t][i];
+      y = args.b[t][i];
+    });
     if (acc) {
       const u2 z = c[i];
-      sr = add_mod(sr, z.x, m.p);
-      si = add_mod(si, z.y, m.p);
+      r = make_ulonglong2(add_mod(r.x, z.x, m.p), add_mod(r.y, z.y, m.p));
     }
-    c[i] = make_ulonglong2(sr, si);
+    c[i] = r;
   }
+}
+
+// Batched form: polynomial q of c = sum_t a[q n + t] b[q n + t] (b[t] when b is shared);
+// every operand a polynomial of `poly` elements, residue r at offset r N.
+__global__ void __launch_bounds__(256)
+    k_dot_batch(const u2* __restrict__ a, const u2* __restrict__ b, u2* __restrict__ c, int n, int b_shared, int N,
+                int nres, int rid_off, const ModConst* __restrict__ mc) {
+  const int r = blockIdx.y % nres;
+  const size_t q = blockIdx.y / nres + (size_t)blockIdx.z * (gridDim.y / nres);
+  const ModConst m = mc[rid_off + r];
+  const size_t poly = (size_t)nres * N;
+  const u2* ap = a + q * n * poly + (size_t)r * N;
+  const u2* bp = b + (b_shared ? 0 : q * n * poly) + (size_t)r * N;
+  u2* cp = c + q * poly + (size_t)r * N;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x)
+    cp[j] = dot_elem(n, m, [&](int t, u2& x, u2& y) {
+      x = ap[t * poly + j];
+      y = bp[t * poly + j];
+    });
 }
 
 }  // namespace
@@ -266,6 +296,33 @@ int pw_dot(const Engine& e, void* c, const void* const* a, const void* const* b,
     if (rc != CP_OK_) return rc;
   }
   return CP_OK_;
+}
+int pw_dot_batch(const Engine& e, void* c, const void* a, const void* b, int n, int npolys, bool b_shared, int base,
+                 cudaStream_t st) {
+  const int nres = e.n_residues(base);
+  if (nres <= 0) {
+    set_error("dot_batch: unknown base");
+    return CP_ERR_INVALID_;
+  }
+  if (n < 1 || n > kDotTerms) {
+    set_error("dot_batch: n must be in [1, 64]");
+    return CP_ERR_INVALID_;
+  }
+  if (npolys <= 0) return CP_OK_;
+  const int threads = 256;
+  int bx = (e.N + threads - 1) / threads;
+  if (bx > 4096) bx = 4096;
+  // (polynomial, residue) rows over y, split over z in whole polynomials when needed
+  long long gz = 1;
+  while ((long long)npolys * nres / gz > 65535 || npolys % gz) ++gz;
+  if (gz > 65535) {
+    set_error("dot_batch: batch too large");
+    return CP_ERR_INVALID_;
+  }
+  const dim3 grid(bx, (unsigned)((long long)npolys / gz * nres), (unsigned)gz);
+  k_dot_batch<<<grid, threads, 0, st>>>(CU2(a), CU2(b), U2(c), n, b_shared ? 1 : 0, e.N, nres, e.rid_offset(base),
+                                        e.d_mc);
+  return check_launch("dot_batch");
 }
 int pw_dr2(const Engine& e, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, cudaStream_t st, int npolys) {

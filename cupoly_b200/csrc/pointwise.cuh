@@ -19,6 +19,8 @@ int pw_muladd(const Engine& e, void* d, const void* a, const void* b, const void
 constexpr int kDotTerms = 64;
 int pw_dot(const Engine& e, void* c, const void* const* a, const void* const* b, int n, int base,
            cudaStream_t st);
+int pw_dot_batch(const Engine& e, void* c, const void* a, const void* b, int n, int npolys, bool b_shared, int base,
+                 cudaStream_t st);
 int pw_dr2(const Engine& e, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, cudaStream_t st, int npolys = 1);
 int pw_negate(const Engine& e, void* b, const void* a, int base, cudaStream_t st);

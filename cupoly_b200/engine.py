@@ -262,6 +262,11 @@ class Engine:
         pb = (C.c_void_p * n)(*[_ptr(x) for x in b])
         call("cp_dot", self._h, _ptr(c), pa, pb, n, base, _stream(stream))
 
+    def dot_batch(self, c, a, b, n, npolys, base, b_shared=False, stream=None):
+        """Polynomial q of c = sum_{t<n} a[q n + t] b[q n + t] (b[t] when b_shared), one launch."""
+        call("cp_dot_batch", self._h, _ptr(c), _ptr(a), _ptr(b), n, npolys, 1 if b_shared else 0, base,
+             _stream(stream))
+
     def dr2(self, c21, c22, c23, c01, c02, c11, c12, base, stream=None):
         call("cp_dr2", self._h, _ptr(c21), _ptr(c22), _ptr(c23), _ptr(c01), _ptr(c02), _ptr(c11), _ptr(c12),
              base, _stream(stream))

@@ -167,6 +167,12 @@ int cp_muladd(const cp_engine* e, void* d, const void* a, const void* b, const v
  * operand returns CP_ERR_INVALID. */
 int cp_dot(const cp_engine* e, void* c, const void* const* a, const void* const* b, int n, int base,
            void* stream);
+/* batched cp_dot (no counterpart in cuPoly): for q < npolys, polynomial q of c = sum_{t<n}
+ * a[q n + t] b[q n + t], or b[t] when b_shared (one key set for every q, as in
+ * relinearization); a, b, c are densely packed polynomials over `base`, 1 <= n <= 64.  The
+ * layout of a is cp_xi_batch's output (n = k).  c must not overlap a or b. */
+int cp_dot_batch(const cp_engine* e, void* c, const void* a, const void* b, int n, int npolys, int b_shared,
+                 int base, void* stream);
 int cp_dr2(const cp_engine* e, void* c21, void* c22, void* c23, const void* c01, const void* c02, const void* c11,
            const void* c12, int base, void* stream);
 /* replace CUDAEngine::execute_polynomial_negate / _op_by_int / _double_op_by_int

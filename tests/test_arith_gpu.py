@@ -307,3 +307,36 @@ def test_poly_dot_mirror_matches_composition(gpu):
     composed(A3, B, A3[2])
     assert np.array_equal(coeffs(A2[2]), coeffs(A3[2]))
     cp.CUDAEngine.destroy()
+
+
+def test_dot_batch_vs_dot_and_exact(gpu):
+    """cp_dot_batch: per-polynomial operands and shared keys (the relinearization layout: the
+    xi_batch decomposition of P polynomials against one set of k key polynomials) equal cp_dot
+    per polynomial and the exact sums."""
+    import torch
+
+    from cupoly_b200.engine import QBase, UNIFORM, Engine, from_u64, to_u64
+    e = Engine(3, 0, 2048, 256)
+    k, P = e.k, 5
+    x = e.empty(QBase, P)
+    e.sample(x, QBase, UNIFORM, 3, 0, npolys=P, to_dgt=True)
+    dec = e.empty(QBase, P * k)
+    e.xi_batch(dec, x)
+    keys = e.empty(QBase, k)
+    e.sample(keys, QBase, UNIFORM, 3, 100, npolys=k, to_dgt=False)
+    out = e.empty(QBase, P)
+    e.dot_batch(out, dec, keys, k, P, QBase, b_shared=True)
+    for q in range(P):
+        ref = e.empty(QBase)
+        e.dot(ref, [dec[q * k + t] for t in range(k)], [keys[t] for t in range(k)], QBase)
+        assert torch.equal(out[q], ref[0]), q
+    # per-polynomial second operands, against the exact sums; n = 7 terms
+    n = 7
+    A = [fold(random_poly_residues(900 + i, e.Q, 2048)) for i in range(P * n)]
+    B = [fold(random_poly_residues(1900 + i, e.Q, 2048)) for i in range(P * n)]
+    da, db = from_u64(np.stack(A)), from_u64(np.stack(B))
+    out = e.empty(QBase, P)
+    e.dot_batch(out, da, db, n, P, QBase)
+    got = to_u64(out)
+    for q in range(P):
+        assert np.array_equal(got[q], _dot_exact(A[q * n:(q + 1) * n], B[q * n:(q + 1) * n], e.Q)), q
