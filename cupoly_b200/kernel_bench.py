@@ -21,6 +21,8 @@ Workloads (names for --only):
                      2^24 coefficients x 16 residues (nphi 32768, k 16, 512 polynomials)
   dot                key-switching dot product (cp_dot), 16 terms, nphi 32768, k 16; bytes = 32
                      operands read + 1 written
+  dot_batch          cp_dot_batch: the xi decomposition of 128 polynomials against 5 shared key
+                     polynomials, nphi 8192, k 5; bytes = decompositions + keys read + results written
   bfv_chain, bfv_chain_target, bfv_chain_large
                      the batched BFV multiplication chain (cp_bfv_mul_batch) at nphi 8192 / k 5 /
                      128 pairs, nphi 16384 / k 10 / 32 pairs and nphi 32768 / k 16 / t 65537 / 64
@@ -188,6 +190,18 @@ def workloads():
                 "key-switching dot product (cp_dot), %d terms, nphi 32768, k 16" % nt, e)
 
     W["dot"] = dot
+
+    def dot_batch():
+        e = _engine(5, 6, 8192, 256)
+        P, k = 128, 5
+        dec, keys, out = e.empty(QBase, P * k), e.empty(QBase, k), e.empty(QBase, P)
+        e.sample(dec, QBase, UNIFORM, 10, 0, npolys=P * k, to_dgt=False)
+        e.sample(keys, QBase, UNIFORM, 10, P * k, npolys=k, to_dgt=False)
+        return (lambda: e.dot_batch(out, dec, keys, k, P, QBase, b_shared=True), (P * k + k + P) * k * e.N * 16,
+                "batched key-switching dot (cp_dot_batch), %d decompositions x %d shared keys, nphi 8192, k 5"
+                % (P, k), e)
+
+    W["dot_batch"] = dot_batch
     W["bfv_chain"] = chain(8192, 5, 256, 128)
     W["bfv_chain_target"] = chain(16384, 10, 256, 32)
     W["bfv_chain_large"] = chain(32768, 16, 65537, 64)
