@@ -57,6 +57,10 @@ def test_null_engine_calls_fail_cleanly():
     assert L.cp_dgt(None, None, 0, 0, 1, 0, None) == 1
     assert L.cp_add(None, None, None, None, 0, None) == 1
     assert L.cp_bfv_mul(None, None, None, None, None, None, None, None, None, None) == 1
+    assert L.cp_dot(None, None, None, None, 1, 0, None) == 1
+    assert L.cp_dot_batch(None, None, None, None, 1, 1, 0, 0, None) == 1
+    assert L.cp_engine_set_narrow_plan(None, 2, 10, 96) == 1
+    assert L.cp_engine_get_narrow_plan(None, None, None, None) == 1
     assert L.cp_engine_n_residues(None, 0) == -1
     assert L.cp_workspace_bytes(None) == 0
     assert L.cp_engine_destroy(None) == 0
