@@ -82,3 +82,19 @@ def test_modarith_eval_checks_arguments_before_any_cuda_call():
     assert L.cp_modarith_eval(4, buf, buf, None, buf, 4, p, None) == 1           # SHOUP without companions
     assert "missing operand" in L.cp_last_error().decode()
     assert L.cp_modarith_eval(0, buf, buf, None, buf, 0, p, None) == 0           # nothing to do
+
+
+def test_engine_create_reports_a_failed_device_allocation():
+    """With no usable CUDA device every cudaMalloc fails: engine creation builds its tables on
+    the host, reaches the device allocation, frees what it built and returns CP_ERR_OOM with
+    the CUDA message and no handle, as often as it is called (the out-of-memory path, driven
+    by a real failing allocation rather than a GPU fault)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present: allocations succeed")
+    L = _lib.lib()
+    for _ in range(3):
+        h = C.c_void_p()
+        rc = L.cp_engine_create(C.byref(h), 2, 3, 4096, 256, 0)
+        assert rc == 4 and not h.value
+        assert "cudaMalloc failed for engine tables" in L.cp_last_error().decode()
