@@ -328,8 +328,8 @@ class GpuExecutor:
         for c, e in enumerate(self.engines):
             for b in self.pool_bufs[c]:
                 s = b["stream"]
-                b["ids_d"][:4].zero_()
                 with torch.cuda.stream(s):
+                    b["ids_d"][:4].zero_()
                     self._enqueue(e, b, 1, s)  # warm-up outside the capture
                 s.synchronize()
                 g = torch.cuda.CUDAGraph()
