@@ -41,6 +41,7 @@ SIGNATURES = {
     "cp_engine_ckks_prec": (_i, [_vp]),
     "cp_engine_set_plan": (_i, [_vp, _i, _i]),
     "cp_engine_get_plan": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "cp_engine_check_async": (_i, [_vp, _vp, _vp]),
     "cp_engine_set_narrow_plan": (_i, [_vp, _i, _i, C.c_longlong]),
     "cp_engine_get_narrow_plan": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_longlong)]),
     "cp_engine_set_split_mode": (_i, [_vp, _i]),

@@ -345,6 +345,13 @@ int cp_engine_check(const cp_engine* h, void* stream) {
   return CP_OK;
 }
 
+int cp_engine_check_async(const cp_engine* h, int* flag_host, void* stream) {
+  CP_REQUIRE(h && flag_host, "cp_engine_check_async: NULL engine or flag");
+  const cudaError_t err = cudaMemcpyAsync(flag_host, h->e.d_err, sizeof(int), cudaMemcpyDeviceToHost, S(stream));
+  if (err != cudaSuccess) return cuda_fail("cp_engine_check_async", err);
+  return CP_OK;
+}
+
 int cp_dgt(const cp_engine* h, void* data, int base, int direction, int npolys, int64_t poly_stride, void* stream) {
   CP_REQUIRE(valid_base(h, base) && data, "cp_dgt: bad engine, base or data");
   CP_REQUIRE(direction == CP_FORWARD || direction == CP_INVERSE, "cp_dgt: bad direction");

@@ -211,6 +211,10 @@ class Engine:
     def check(self, stream=None):
         call("cp_engine_check", self._h, _stream(stream))
 
+    def check_async(self, flag_host: torch.Tensor, stream=None):
+        """Queue a copy of the engine's error flag into flag_host (a pinned int32 tensor) on the stream."""
+        call("cp_engine_check_async", self._h, _ptr(flag_host), _stream(stream))
+
     # ---- DGT ----
     def dgt(self, x: torch.Tensor, base: int, direction: int, npolys: Optional[int] = None, stream=None):
         n = x.shape[0] if npolys is None else npolys

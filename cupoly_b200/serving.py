@@ -320,6 +320,7 @@ class GpuExecutor:
                     "ids_d": torch.empty(4 * cl.max_batch, dtype=torch.int32, device="cuda"),
                     "ids_h": torch.empty(4 * cl.max_batch, dtype=torch.int32).pin_memory(),
                     "stream": torch.cuda.Stream(),
+                    "flag_h": torch.zeros(1, dtype=torch.int32).pin_memory(),
                 })
             self.pool_bufs.append(bufs)
         torch.cuda.synchronize()
@@ -358,6 +359,7 @@ class GpuExecutor:
                 b["graph1"].replay()
             else:
                 self._enqueue(e, b, B, s)
+            e.check_async(b["flag_h"], stream=s)  # the error flag follows the batch to the host
             ev = torch.cuda.Event()
             ev.record(s)
         return ev
@@ -366,8 +368,11 @@ class GpuExecutor:
         return ev.query()
 
     def finish(self, pool):
-        # a kernel's error flag (e.g. a sampler rejection limit) fails the batch
-        self.engines[pool.cls].check(self.pool_bufs[pool.cls][pool.index]["stream"])
+        # a kernel's error flag (e.g. a sampler rejection limit) fails the batch; the flag was
+        # copied behind the batch, so a clear flag needs no device round trip
+        b = self.pool_bufs[pool.cls][pool.index]
+        if int(b["flag_h"][0]) != 0:
+            self.engines[pool.cls].check(b["stream"])  # raises with the message, resets the flag
         if not self.keep:
             return
         b = self.pool_bufs[pool.cls][pool.index]

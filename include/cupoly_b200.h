@@ -120,6 +120,10 @@ int cp_engine_get_nthroot(const cp_engine* e, uint64_t* xi_out);
 size_t cp_workspace_bytes(const cp_engine* e);
 /* read and clear the engine's device error flag (synchronises `stream`) */
 int cp_engine_check(const cp_engine* e, void* stream);
+/* the engine's error flag, copied into flag_host (page-locked host memory) on `stream` behind
+ * the work already queued there, without waiting: nonzero once the copy has completed means
+ * that cp_engine_check will report the error (and reset the flag). */
+int cp_engine_check_async(const cp_engine* e, int* flag_host, void* stream);
 
 /* ---- DGT: replaces DGTEngine::execute_dgt(data, base, direction, ctx)
  *      (src/cuda/dgt.cu:1069-1094).  In place on npolys consecutive polynomials

@@ -60,6 +60,7 @@ def test_null_engine_calls_fail_cleanly():
     assert L.cp_dot(None, None, None, None, 1, 0, None) == 1
     assert L.cp_dot_batch(None, None, None, None, 1, 1, 0, 0, None) == 1
     assert L.cp_engine_set_narrow_plan(None, 2, 10, 96) == 1
+    assert L.cp_engine_check_async(None, None, None) == 1
     assert L.cp_engine_get_narrow_plan(None, None, None, None) == 1
     assert L.cp_engine_n_residues(None, 0) == -1
     assert L.cp_workspace_bytes(None) == 0

@@ -185,3 +185,28 @@ def test_queue_timeout_rejects_requests_that_wait_too_long():
     assert st["rejected"] > 0 and st["completed"] >= 2
     assert all(r.error == "queue timeout" for r in reqs if r.status == "rejected")
     assert sch.peak_used <= budget and sch.used == 0
+
+
+@pytest.mark.gpu
+def test_error_flag_copy_follows_the_batch(gpu):
+    """cp_engine_check_async copies the engine's (clear) error flag behind queued work into
+    pinned memory; the executor's batches carry it, and a clear flag passes finish()."""
+    import torch
+
+    from cupoly_b200.engine import QBase, UNIFORM, Engine
+    from cupoly_b200.serving import GpuExecutor
+
+    e = Engine(2, 0, 4096, 256)
+    flag = torch.full((1,), 7, dtype=torch.int32).pin_memory()
+    x = e.empty(QBase, 4)
+    s = torch.cuda.Stream()
+    e.sample(x, QBase, UNIFORM, 1, 0, npolys=4, to_dgt=True, stream=s)
+    e.check_async(flag, stream=s)
+    s.synchronize()
+    assert int(flag[0]) == 0
+    cls = _classes()
+    ex = GpuExecutor(cls)
+    sch = Scheduler(cls, ex, budget_bytes=1 << 30)
+    reqs = sch.run([Request(i, i % len(cls), 0.0) for i in range(6)])
+    assert all(r.status == "done" for r in reqs)
+    assert all(int(b["flag_h"][0]) == 0 for bs in ex.pool_bufs for b in bs)
