@@ -166,9 +166,10 @@ int cp_muladd(const cp_engine* e, void* d, const void* a, const void* b, const v
 /* replaces poly_dot (src/arithmetic/polynomial.cu:1439-1451), which composes one
  * poly_mul and n-1 poly_mul_add calls: c = sum_i a[i] b[i] over `base` in the DGT domain
  * in one pass, each operand read once and each sum reduced once per element.  a and b are
- * HOST arrays of n >= 1 device pointers.  c may alias any operand among the first 64 pairs
- * (the result is the sum over the inputs as they were before the call); aliasing a later
- * operand returns CP_ERR_INVALID. */
+ * HOST arrays of n >= 1 device pointers.  c may be the same buffer as any operand among the
+ * first 64 pairs (the result is the sum over the inputs as they were before the call); c equal
+ * to a later operand returns CP_ERR_INVALID; any other overlap of c with an operand is not
+ * allowed. */
 int cp_dot(const cp_engine* e, void* c, const void* const* a, const void* const* b, int n, int base,
            void* stream);
 /* batched cp_dot (no counterpart in cuPoly): for q < npolys, polynomial q of c = sum_{t<n}
