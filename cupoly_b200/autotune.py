@@ -144,7 +144,7 @@ def best_plan(nphi: int, residues: int = 2048, reps: int = 5, save: bool = True)
 
 # Launch sizes (residue transforms per launch) at which the small-launch plan is compared
 # with the main plan.
-NARROW_UNITS = (16, 96, 384, 768, 1536)
+NARROW_UNITS = (16, 96, 192, 288, 384, 768, 1536)
 
 
 def _graph_ms(fn, calls: int = 10, reps: int = 5) -> float:
