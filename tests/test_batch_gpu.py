@@ -284,3 +284,32 @@ def test_default_and_cached_small_launch_plans(gpu, tmp_path, monkeypatch):
         assert (got["log_radix"], got["log_cta"], got["max_units"]) == narrow
     else:
         assert got["max_units"] == 0
+
+
+def test_pipelined_batches_equal_single_calls(gpu):
+    """PipelinedBFV (two batches in flight on two streams) gives each batch the bytes of one
+    cp_bfv_mul_batch call on the default stream."""
+    import torch
+
+    from cupoly_b200.batch import PipelinedBFV
+    from cupoly_b200.engine import QBase, UNIFORM, Engine
+    e = Engine(3, 0, 4096, 256)
+    P, nb = 8, 5
+    batches = []
+    for i in range(nb):
+        ins = []
+        for v in range(4):
+            x = e.empty(QBase, P)
+            e.sample(x, QBase, UNIFORM, 21 + i, 16 * v, npolys=P, to_dgt=True)
+            ins.append(x)
+        batches.append(ins)
+    outs = [e.empty(QBase, 3 * P) for _ in range(nb)]
+    pl = PipelinedBFV(e, P)
+    pl.run(batches, outs)
+    pl.join()
+    ws = e.bfv_mul_batch_workspace(P)
+    for ins, out in zip(batches, outs):
+        ref = e.empty(QBase, 3 * P)
+        e.bfv_mul_batch(ref, *ins, P, ws)
+        torch.cuda.synchronize()
+        assert torch.equal(ref, out)
