@@ -12,8 +12,9 @@ groups' launches are captured once in a CUDA graph and replayed.
 `BFVBatch`: the fused BFV multiplication chain over a fixed batch of pairs,
 captured in a CUDA graph.
 
-`PipelinedBFV`: consecutive device-resident batches with two in flight on two
-streams; `StreamedBFV`: batches in host memory, copies overlapped with the chain.
+`PipelinedBFV`, `PipelinedPolymul`: consecutive device-resident batches with two
+in flight on two streams; `StreamedBFV`: batches in host memory, copies
+overlapped with the chain.
 """
 from __future__ import annotations
 
@@ -180,6 +181,37 @@ class PipelinedBFV:
 
     def join(self, stream=None):
         """Make `stream` (default: the current stream) wait for every batch issued so far."""
+        cur = stream if stream is not None else torch.cuda.current_stream()
+        for s in self.streams:
+            cur.wait_stream(s)
+
+
+class PipelinedPolymul:
+    """Fused negacyclic products (cp_polymul, coefficient domain in and out) of
+    consecutive device-resident batches, `lanes` of them in flight on as many
+    streams, each lane with its own workspace (on B200, nphi 4096, k 2, 1024
+    products: 305 instead of 339 us per batch).  Results are those of one
+    cp_polymul call per batch.  The outputs of batches in flight at the same
+    time must be distinct tensors."""
+
+    def __init__(self, engine: Engine, base: int, npolys: int, lanes: int = 2):
+        self.e = engine
+        self.base = base
+        self.P = npolys
+        self.lanes = lanes
+        self.ws = [engine.polymul_workspace(base, npolys) for _ in range(lanes)]
+        self.streams = [torch.cuda.Stream() for _ in range(lanes)]
+
+    def run(self, batches, outputs, stream=None):
+        """batches[i] = (a, b), npolys polynomials each; outputs[i] receives a b."""
+        cur = stream if stream is not None else torch.cuda.current_stream()
+        for s in self.streams:
+            s.wait_stream(cur)
+        for i, ((a, b), out) in enumerate(zip(batches, outputs)):
+            j = i % self.lanes
+            self.e.polymul(out, a, b, self.base, self.ws[j], self.P, stream=self.streams[j])
+
+    def join(self, stream=None):
         cur = stream if stream is not None else torch.cuda.current_stream()
         for s in self.streams:
             cur.wait_stream(s)

@@ -313,3 +313,29 @@ def test_pipelined_batches_equal_single_calls(gpu):
         e.bfv_mul_batch(ref, *ins, P, ws)
         torch.cuda.synchronize()
         assert torch.equal(ref, out)
+
+
+def test_pipelined_polymul_equals_single_calls(gpu):
+    """PipelinedPolymul gives each batch the bytes of one cp_polymul call."""
+    import torch
+
+    from cupoly_b200.batch import PipelinedPolymul
+    from cupoly_b200.engine import QBase, UNIFORM, Engine
+    e = Engine(2, 0, 4096, 256)
+    P, nb = 16, 4
+    batches = []
+    for i in range(nb):
+        a, b = e.empty(QBase, P), e.empty(QBase, P)
+        e.sample(a, QBase, UNIFORM, 41 + i, 0, npolys=P, to_dgt=False)
+        e.sample(b, QBase, UNIFORM, 41 + i, P, npolys=P, to_dgt=False)
+        batches.append((a, b))
+    outs = [e.empty(QBase, P) for _ in range(nb)]
+    pp = PipelinedPolymul(e, QBase, P)
+    pp.run(batches, outs)
+    pp.join()
+    ws = e.polymul_workspace(QBase, P)
+    for (a, b), out in zip(batches, outs):
+        ref = e.empty(QBase, P)
+        e.polymul(ref, a, b, QBase, ws, P)
+        torch.cuda.synchronize()
+        assert torch.equal(ref, out)
