@@ -21,7 +21,14 @@
 #include <string>
 #include <vector>
 
-namespace cupoly {
+// The class lives in namespace cupoly unless the includer defines
+// CUPOLY_ZZ_NAMESPACE first (the build of cuPoly's own sources under oracle/
+// places it in namespace NTL, beside its RR).
+#ifndef CUPOLY_ZZ_NAMESPACE
+#define CUPOLY_ZZ_NAMESPACE cupoly
+#endif
+
+namespace CUPOLY_ZZ_NAMESPACE {
 
 class ZZ {
  public:
@@ -392,7 +399,16 @@ inline void conv(ZZ& x, const char* s) { x = ZZ::from_string(s); }
 inline void conv(ZZ& x, const std::string& s) { x = ZZ::from_string(s); }
 inline void conv(ZZ& x, const ZZ& a) { x = a; }
 inline void conv(long& x, const ZZ& a) { x = to_long(a); }
+#ifdef CUPOLY_ZZ_LOW_WORD_CONV
+// NTL's rule for a machine-word conversion: the low-order 64 bits of a (two's
+// complement for a negative a), whatever a's size.
+inline void conv(unsigned long& x, const ZZ& a) {
+  const unsigned long w = a.limbs().empty() ? 0ul : (unsigned long)a.limbs()[0];
+  x = a.is_negative() ? 0ul - w : w;
+}
+#else
 inline void conv(unsigned long& x, const ZZ& a) { x = to_ulong(a); }
+#endif
 template <class T, class S>
 inline T conv(const S& a) {
   T x;
@@ -400,4 +416,4 @@ inline T conv(const S& a) {
   return x;
 }
 
-}  // namespace cupoly
+}  // namespace CUPOLY_ZZ_NAMESPACE

@@ -500,23 +500,60 @@ def cupoly_float_ext_b_to_q(ys, Q, B):
     return out
 
 
+def _rr_round(m: int, e: int, prec: int, sticky: bool = False):
+    """NTL RR rounding: m 2^e (m >= 0) to ``prec`` mantissa bits, to nearest, ties to
+    even; ``sticky`` marks nonzero bits already dropped below m."""
+    nb = m.bit_length()
+    if nb > prec:
+        drop = nb - prec
+        kept, rest, half = m >> drop, m & ((1 << drop) - 1), 1 << (drop - 1)
+        if rest > half or (rest == half and (sticky or kept & 1)):
+            kept += 1
+        m, e = kept, e + drop
+    return m, e
+
+
+def _rr_quotient_frac(aux: int, q: int, prec: int = 512):
+    """cuPoly's split of aux / q into an integer part and a 128-bit fraction
+    (``cudaengine.cu:1479-1486``, ``:1498-1506``): RR::SetPrecision(512); tmp = to_RR(aux)
+    / to_RR(q) -- each step rounded to 512 bits as NTL's RR does -- then
+    FloorToZZ(tmp) and floor((tmp - floor(tmp)) 2^128).  When aux / q has more than
+    384 integer bits, the fraction keeps only the rounded quotient's low bits."""
+    ma, ea = _rr_round(aux, 0, prec)
+    s = max(prec + 2 + q.bit_length() - ma.bit_length(), 0)
+    quo, rem = divmod(ma << s, q)
+    m, e = _rr_round(quo, ea - s, prec, rem != 0)
+    if e >= 0:
+        return m << e, 0
+    ip = m >> -e
+    frac = m - (ip << -e)  # fractional part = frac 2^e, exact
+    return ip, (frac << 128) >> -e
+
+
 @lru_cache(maxsize=None)
 def _cupoly_omega(Q, B, t):
-    """omega_int, the 128-bit omega_frac and lambda of ``cudaengine.cu:1466-1492``:
-    omega_{l,j} = t [(QB/q_l)^-1]_{q_l} B / q_l split into floor mod b_j and a 128-bit
-    fraction (floor of frac * 2^128; cuPoly rounds a 512-bit RR, which differs from
-    the floor by at most one unit of 2^-128); lambda_j = t [(QB/b_j)^-1]_{b_j} (B/b_j)
-    mod b_j."""
+    """omega_int, the 128-bit omega_frac and lambda of ``cudaengine.cu:1463-1492``:
+    omega_{l,j} = t [(QB/q_l)^-1]_{q_l} B / q_l split into its integer part mod b_j and
+    a 128-bit fraction, both from the 512-bit RR quotient (``_rr_quotient_frac``);
+    lambda_j = t [(QB/b_j)^-1]_{b_j} (B/b_j) mod b_j."""
     Qp, Bp = prod(Q), prod(B)
     lam = tuple(t * pow(Bp * Qp // b % b, -1, b) * (Bp // b) % b for b in B)
     om_int, om_frac = {}, {}
     for j, b in enumerate(B):
         for l, q in enumerate(Q):
             aux = t * pow(Qp * Bp // q % q, -1, q) * Bp
-            ti = aux // q
+            ti, fr = _rr_quotient_frac(aux, q)
             om_int[l, j] = ti % b
-            om_frac[l, j] = ((aux - ti * q) << 128) // q
+            om_frac[l, j] = fr
     return om_int, om_frac, lam
+
+
+@lru_cache(maxsize=None)
+def _cupoly_tomega(Q, t):
+    """tomega_int and the 128-bit tomega_frac of ``cudaengine.cu:1494-1509``:
+    t [(Q/q_i)^-1]_{q_i} / q_i from the 512-bit RR quotient."""
+    Qp = prod(Q)
+    return tuple(_rr_quotient_frac(t * pow(Qp // q % q, -1, q), q) for q in Q)
 
 
 def cupoly_float_complex_scaling(xq, yb, Q, B, t):
@@ -552,12 +589,8 @@ def cupoly_float_simple_scaling(xq, Q, t):
     """cuPoly's simple_scaling for one coefficient, t a power of two (``cudaengine.cu:323-362``,
     tomega from ``:1494-1509``): integer parts masked mod t, fraction parts summed in double."""
     assert t > 0 and t & (t - 1) == 0
-    Qp = prod(Q)
     result, acc = 0, 0.0
-    for x, q in zip(xq, Q):
-        aux = t * pow(Qp // q % q, -1, q)
-        ti = aux // q
-        frac = ((aux - ti * q) << 128) // q
+    for x, (ti, frac) in zip(xq, _cupoly_tomega(tuple(Q), t)):
         vint = (x * ti) & _U64 & (t - 1)
         c = (frac * x) >> 64
         hi, lo = c >> 64, c & _U64
@@ -598,6 +631,29 @@ def load_cdt(name):
 # Distribution kinds of the device sampler (values of enum cp_distribution).
 DISCRETE_GAUSSIAN, HAMMINGWEIGHT, NARROW, ZO, BINARY, UNIFORM, TERNARY, GAUSSIAN = range(8)
 SIGNED_DG = 8  # CKKS engines: DISCRETE_GAUSSIAN without the absolute value (device-internal kind)
+UNIFORM_U32 = 9  # cuPoly's BFV UNIFORM (src/cuda/sampler.cu:295-341): one value below 2^32 for all residues
+ZO_HALF = 10  # cuPoly's BFV ZO (src/cuda/sampler.cu:236-283): exactly nphi/2 nonzero, each +-1
+
+
+def zo_half_position(c, nphi, sid, seed):
+    """Image of coefficient c under the device's keyed bijection of [0, nphi): a 4-round
+    Feistel network with Philox4x32-10 rounds over counters (half, 0x5A000000 + round,
+    stream id, ZO_HALF); for odd log2(nphi) it runs on one more bit and walks the cycle
+    back into range."""
+    k0, k1 = seed & _M, (seed >> 32) & _M
+    b = nphi.bit_length() - 1
+    hb = (b + 1) >> 1
+    m = (1 << hb) - 1
+    x = c
+    for _ in range(64):
+        L, R = x >> hb, x & m
+        for r in range(4):
+            f = philox4x32_10((R, 0x5A000000 + r, sid, ZO_HALF), (k0, k1))[0] & m
+            L, R = R, L ^ f
+        x = (L << hb) | R
+        if x < nphi:
+            return x
+    raise RuntimeError("cycle walk limit")
 
 
 def _cdt_lookup(u63, cdt):
@@ -613,6 +669,8 @@ def sample_small(kind, c, sid, seed):
     ZO is i.i.d. (cuPoly fixes exactly half the coefficients nonzero).
     """
     k0, k1 = seed & _M, (seed >> 32) & _M
+    if kind == ZO_HALF:
+        raise ValueError("ZO_HALF depends on nphi: use sample_zo_half")
     if kind in (NARROW, TERNARY):
         for d in range(8):
             for w in philox4x32_10((c, d, sid, kind), (k0, k1)):
@@ -671,6 +729,20 @@ def sample_hamming(nphi, sid, seed, h=64):
     return out
 
 
+def sample_zo_half(nphi, sid, seed):
+    """cuPoly's ZO with exactly nphi/2 nonzero coefficients: coefficient c is nonzero iff
+    its image under the keyed bijection is below nphi/2; its sign is bit 0 of the
+    Philox block (c, 1, stream id, ZO_HALF)."""
+    k0, k1 = seed & _M, (seed >> 32) & _M
+    out = []
+    for c in range(nphi):
+        if zo_half_position(c, nphi, sid, seed) >= nphi // 2:
+            out.append(0)
+        else:
+            out.append(-1 if philox4x32_10((c, 1, sid, ZO_HALF), (k0, k1))[0] & 1 else 1)
+    return out
+
+
 def sample_poly(kind, primes, nphi, sid, seed, ckks=False):
     """(nres, nphi) coefficient rows the device sampler produces.  On a CKKS engine the
     small kinds are signed, as in cuPoly's CKKS build (``src/cuda/sampler.cu:73-106,
@@ -678,6 +750,15 @@ def sample_poly(kind, primes, nphi, sid, seed, ckks=False):
     if ckks:
         kind = {NARROW: TERNARY, DISCRETE_GAUSSIAN: SIGNED_DG}.get(kind, kind)
     rows = []
+    if kind == UNIFORM_U32:
+        N = nphi // 2
+        k0, k1 = seed & _M, (seed >> 32) & _M
+        w = [philox4x32_10((j, 0, sid, UNIFORM_U32), (k0, k1)) for j in range(N)]
+        row = [q[0] for q in w] + [q[1] for q in w]
+        return [list(row) for _ in primes]
+    if kind == ZO_HALF:
+        vals = sample_zo_half(nphi, sid, seed)
+        return [[v % p for v in vals] for p in primes]
     if kind == UNIFORM:
         N = nphi // 2
         rows = []

@@ -8,8 +8,9 @@ read only here, never at test time):
 
 Writes:
   ref_nthroot.json -- cuPoly's tabulated Gaussian roots of i, NTHROOT[p][N]
-                      (src/arithmetic/coprimes/qis_63.json), for the first 12
-                      primes and the transform sizes the tests use.  With them
+                      (src/arithmetic/coprimes/qis_63.json), for the first 33
+                      primes (Q u B of nphi 32768, k 16, kl 17) and every
+                      tabulated size N = 16 ... 32768.  With them
                       the DGT-domain bytes can be compared with cuPoly's.
   dgt_golden.json  -- seeded inputs (by seed) and SHA-256 of the forward DGT
                       computed by the Python restatement of cuPoly's
@@ -30,7 +31,7 @@ import numpy as np  # noqa: E402
 from oracle import pyoracle as O  # noqa: E402
 from tests.common import fold, gi_rows_to_list, random_poly_residues, sha  # noqa: E402
 
-SIZES = [16, 64, 128, 1024, 2048, 4096, 8192]
+SIZES = [16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192, 16384, 32768]
 DGT_CASES = [  # (nphi, nres, seed)
     (32, 3, 11), (128, 2, 12), (256, 2, 13), (2048, 2, 14), (4096, 3, 15), (8192, 2, 16),
 ]
@@ -42,7 +43,7 @@ HPS_CASES = [  # (nphi, k, kl, t, seed)
 def main(ref_root):
     qis = json.load(open(os.path.join(ref_root, "src", "arithmetic", "coprimes", "qis_63.json")))
     roots = {}
-    for p in O.PRIMES[:12]:
+    for p in O.PRIMES[:33]:
         tab = qis[str(p)][0]
         roots[str(p)] = {str(N): [tab[str(N)]["re"], tab[str(N)]["imag"]] for N in SIZES}
         for N in SIZES:  # sanity: xi^N == i

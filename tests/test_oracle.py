@@ -29,6 +29,17 @@ def test_prime_table():
         assert g == sympy.ntheory.primitive_root(p)  # smallest primitive root
 
 
+def test_prime_table_is_cupolys_bucket():
+    """The 100 primes, in order, are cuPoly's COPRIMES_63_BUCKET and the primitive
+    roots its PROOTS (src/arithmetic/coprimes.cu:763-866, :26976): SHA-256 of the
+    comma-joined decimal lists, taken from that file."""
+    import hashlib
+    digest = lambda xs: hashlib.sha256(",".join(map(str, xs)).encode()).hexdigest()  # noqa: E731
+    assert digest(O.PRIMES) == "ee159669b078b2215faef040edc778ae39fc2f40c4089db139fa03fa251daf36"
+    assert digest([O.PROOT[p] for p in O.PRIMES]) == \
+        "224baee04d60cb7a9bb6f09cd87d3db8c851c7f025fe42902402b7437d96a926"
+
+
 @pytest.mark.parametrize("N", [2, 4, 16, 32, 64])
 def test_dgt_is_bitreversed_twisted_dft(N):
     p = O.PRIMES[3]
@@ -181,10 +192,11 @@ def test_fold_unfold():
     assert (unfold(fold(x)) == x).all()
 
 
-@pytest.mark.parametrize("k", [1, 2, 5, 10])
+@pytest.mark.parametrize("k", [1, 2, 4, 5])
 def test_cupoly_float_path_equals_exact_on_random_inputs(k):
     """The restatement of cuPoly's double-precision HPS path (overflow count with FPERROR,
-    128-bit fractions summed in double) gives the exact values on random inputs."""
+    128-bit fractions summed in double, constants from 512-bit RR quotients) gives the
+    exact values on random inputs up to k = 5 (the benchmark's BFV size)."""
     import random
     rng = random.Random(k)
     Q, B = O.bases(k, k + 1)
@@ -199,6 +211,53 @@ def test_cupoly_float_path_equals_exact_on_random_inputs(k):
         assert O.cupoly_float_complex_scaling_tdivq(zq, zb, Q, B, 256) == \
             O.complex_scaling_tdivq_exact(zq, zb, Q, B, 256)
         assert O.cupoly_float_simple_scaling(xs, Q, 256) == O.simple_scaling_exact(xs, Q, 256)
+
+
+def test_cupoly_complex_scaling_is_off_by_one_often_at_k6():
+    """At k = 6, kl = 7 (the largest base of cuPoly's own test grid) the 512-bit RR
+    quotient behind omega keeps only about 63 fraction bits, so the fraction sum of
+    cuPoly's complex scaling lands on the wrong side of the rounding boundary for a
+    sizeable share of ordinary coefficients -- always by exactly one (cuPoly's own test
+    allows |error| < 2, test_bfv_mode.cu:1092-1095).  Simple scaling and the base
+    conversions stay exact there."""
+    import random
+    rng = random.Random(6)
+    Q, B = O.bases(6, 7)
+    Qp, Bp = O.prod(Q), O.prod(B)
+    wrong = 0
+    for _ in range(200):
+        Z = rng.randrange(Qp * Bp)
+        zq, zb = [Z % q for q in Q], [Z % b for b in B]
+        f = O.cupoly_float_complex_scaling(zq, zb, Q, B, 256)
+        e = O.complex_scaling_exact(zq, zb, Q, B, 256)
+        if f != e:
+            wrong += 1
+            assert (O.crt(f, B) - O.crt(e, B)) % Bp in (1, Bp - 1)
+        xs = [Z % q for q in Q]
+        assert O.cupoly_float_ext_q_to_b(xs, Q, B) == O.basis_extension_exact(xs, Q, B)
+        assert O.cupoly_float_simple_scaling(xs, Q, 256) == O.simple_scaling_exact(xs, Q, 256)
+    assert 10 < wrong < 100
+
+
+def test_cupoly_complex_scaling_constants_break_beyond_512_bits():
+    """cuPoly computes omega = t [(QB/q_l)^-1] B / q_l as a 512-bit RR quotient
+    (src/cuda/cudaengine.cu:1463-1490).  Once that quotient needs more than 512 bits
+    (k = 10, kl = 11: about 700), its integer part is rounded by about 2^189, so
+    omega_int mod b_j is unrelated to the true value and cuPoly's complex scaling is
+    wrong on ordinary inputs, not only at edges.  The exact definitions (and the
+    device) do not depend on those constants."""
+    import random
+    rng = random.Random(10)
+    Q, B = O.bases(10, 11)
+    Qp, Bp = O.prod(Q), O.prod(B)
+    wrong = 0
+    for _ in range(20):
+        Z = rng.randrange(Qp * Bp)
+        zq, zb = [Z % q for q in Q], [Z % b for b in B]
+        exact = O.complex_scaling_exact(zq, zb, Q, B, 256)
+        assert exact == [((2 * 256 * Z + Qp) // (2 * Qp)) % b for b in B]
+        wrong += O.cupoly_float_complex_scaling(zq, zb, Q, B, 256) != exact
+    assert wrong == 20
 
 
 def test_cupoly_float_path_is_off_at_its_edges():
@@ -225,3 +284,20 @@ def test_cupoly_float_path_is_off_at_its_edges():
                     wrong += 1
                     assert all((a - e) % b in (1, b - 1) for a, e, b in zip(f, ex, B))
         assert wrong > 0
+
+
+@pytest.mark.parametrize("nphi", [4, 8, 32, 64, 128, 2048])
+def test_zo_half_restatement_has_exactly_half_nonzero(nphi):
+    """cuPoly's ZO (src/cuda/sampler.cu:236-283): exactly nphi/2 coefficients in
+    {-1, +1}; the keyed bijection behind it is a permutation of [0, nphi)."""
+    for sid in range(3):
+        assert sorted(O.zo_half_position(c, nphi, sid, 99) for c in range(nphi)) == list(range(nphi))
+        v = O.sample_zo_half(nphi, sid, 99)
+        assert set(v) <= {-1, 0, 1} and sum(1 for x in v if x) == nphi // 2
+
+
+def test_uniform_u32_restatement_is_one_word_on_every_residue():
+    """cuPoly's BFV UNIFORM (src/cuda/sampler.cu:295-341): one value below 2^32 per
+    coefficient, written to every residue."""
+    rows = O.sample_poly(O.UNIFORM_U32, O.PRIMES[:3], 64, 4, 11)
+    assert rows[0] == rows[1] == rows[2] and max(rows[0]) < 1 << 32 and len(set(rows[0])) == 64
