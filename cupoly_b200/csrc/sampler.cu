@@ -57,7 +57,37 @@ enum Kind : int {
   TERNARY = 6,            // uniform {-1, 0, +1}
   GAUSSIAN = 7,           // discrete Gaussian sigma = 3.19, |x| <= 19, signed
   SIGNED_DG = 8,          // CKKS engines' DISCRETE_GAUSSIAN: nearbyint(3.2 Z), signed (internal)
+  UNIFORM_U32 = 9,        // cuPoly BFV UNIFORM: one value uniform in [0, 2^32), the same on every residue
+  ZO_HALF = 10,           // cuPoly BFV ZO: exactly nphi/2 coefficients nonzero, each +-1 with probability 1/2
 };
+
+// A keyed bijection of [0, 2^b) (b = log2 nphi): a 4-round Feistel network whose
+// round function is Philox4x32-10 (Luby-Rackoff: a pseudo-random permutation).
+// For odd b it runs on b + 1 bits and walks the cycle until the value is back in
+// range (at most 64 steps; the chance of more is below 2^-64).  Counter words
+// (half, 0x5A000000 + round, stream id, kind) never meet the sign draw's (c, 1, ...).
+__device__ __forceinline__ bool zo_half_position(uint32_t c, int b, uint32_t sid, uint32_t k0, uint32_t k1,
+                                                 uint32_t& out) {
+  const int hb = (b + 1) >> 1;  // half width of the even-width network
+  const uint32_t m = (1u << hb) - 1, lim = 1u << b;
+  uint32_t x = c;
+  for (int walk = 0; walk < 64; ++walk) {
+    uint32_t L = x >> hb, R = x & m;
+#pragma unroll
+    for (uint32_t r = 0; r < 4; ++r) {
+      const uint32_t f = philox4x32_10(R, 0x5A000000u + r, sid, (uint32_t)ZO_HALF, k0, k1).v[0] & m;
+      const uint32_t nl = R;
+      R = L ^ f;
+      L = nl;
+    }
+    x = (L << hb) | R;
+    if (x < lim) {
+      out = x;
+      return true;
+    }
+  }
+  return false;
+}
 
 __device__ __forceinline__ uint64_t cdt_lookup(uint64_t u63, const uint64_t* cdt) {
   uint64_t m = 0;
@@ -69,7 +99,7 @@ __device__ __forceinline__ uint64_t cdt_lookup(uint64_t u63, const uint64_t* cdt
 // Small signed value of coefficient c for the residue-independent kinds.
 // Returns false if all draws were rejected (probability < 2^-250).
 __device__ __forceinline__ bool small_value(int kind, uint32_t c, uint32_t sid, uint32_t k0, uint32_t k1,
-                                            int64_t& v) {
+                                            int nphi_log, int64_t& v) {
   if (kind == NARROW || kind == TERNARY) {
     for (uint32_t d = 0; d < 8; ++d) {
       const Philox r = philox4x32_10(c, d, sid, (uint32_t)kind, k0, k1);
@@ -82,6 +112,13 @@ __device__ __forceinline__ bool small_value(int kind, uint32_t c, uint32_t sid, 
         }
     }
     return false;
+  }
+  if (kind == ZO_HALF) {  // nonzero iff the coefficient's image lies in the first half
+    uint32_t pos;
+    if (!zo_half_position(c, nphi_log, sid, k0, k1, pos)) return false;
+    const Philox sg = philox4x32_10(c, 1, sid, (uint32_t)kind, k0, k1);
+    v = (pos >> (nphi_log - 1)) ? 0 : ((sg.v[0] & 1u) ? -1 : 1);
+    return true;
   }
   const Philox r = philox4x32_10(c, 0, sid, (uint32_t)kind, k0, k1);
   const uint64_t u63 = ((uint64_t)(r.v[1] & 0x7FFFFFFFu) << 32) | r.v[0];
@@ -146,9 +183,17 @@ __global__ void __launch_bounds__(256) k_sample(ulonglong2* __restrict__ out, co
     }
     return;
   }
+  if (kind == UNIFORM_U32) {
+    // one Philox block per Gaussian element: word 0 for coefficient j, word 1 for
+    // j + N; every prime exceeds 2^32, so the value itself is its residue everywhere
+    const Philox q = philox4x32_10((uint32_t)j, 0, sid, (uint32_t)kind, k0, k1);
+    for (int r = 0; r < nres; ++r) out[(size_t)r * N + j] = make_ulonglong2(q.v[0], q.v[1]);
+    return;
+  }
   int64_t v0 = 0, v1 = 0;
-  const bool ok0 = small_value(kind, (uint32_t)j, sid, k0, k1, v0);
-  const bool ok1 = small_value(kind, (uint32_t)(j + N), sid, k0, k1, v1);
+  const int nphi_log = 31 - __clz(2 * N);
+  const bool ok0 = small_value(kind, (uint32_t)j, sid, k0, k1, nphi_log, v0);
+  const bool ok1 = small_value(kind, (uint32_t)(j + N), sid, k0, k1, nphi_log, v1);
   if (!(ok0 && ok1)) atomicExch(err, 1);
   for (int r = 0; r < nres; ++r) {
     const uint64_t p = mc[rid_off + r].p;
@@ -223,7 +268,7 @@ int upload_cdt() {
 
 int sample_poly(const Engine& e, void* out_v, int base, int kind, uint64_t seed, uint32_t stream_id, int npolys,
                 cudaStream_t st, const uint32_t* ids) {
-  if (kind < 0 || kind > GAUSSIAN) {
+  if (kind < 0 || kind > ZO_HALF || kind == SIGNED_DG) {
     set_error("sample: unknown distribution");
     return CP_ERR_INVALID_;
   }

@@ -26,9 +26,12 @@ import torch
 
 from .engine import (ADD, ADDADD, BBase, BINARY, DESTROY_INPUTS, DISCRETE_GAUSSIAN, FORWARD, GAUSSIAN,
                      HAMMINGWEIGHT, INVERSE, MUL, MULMUL, NARROW, QBBase, QBase, SUB, TBase, TERNARY, UNIFORM, ZO,
-                     Engine, from_u64, ints_to_limbs, limbs_to_ints, to_u64)
+                     UNIFORM_U32, ZO_HALF, Engine, from_u64, ints_to_limbs, limbs_to_ints, to_u64)
 
 HOSTSTATE, RNSSTATE, BOTHSTATE = 0, 1, 2
+# Sampler kinds of this layer beyond cuPoly's: the library's independent forms of
+# UNIFORM (uniform mod each q_i) and ZO (i.i.d. -1/0/+1 with 1/4, 1/2, 1/4).
+UNIFORM_MOD_Q, ZO_IID = 105, 103
 HAMMINGWEIGHT_H = 64
 GAUSSIAN_STD_DEVIATION = 3.2
 SEED = 42
@@ -36,7 +39,7 @@ SEED = 42
 __all__ = [
     "CUDAEngine", "DGTEngine", "Context", "Sampler", "poly_t", "QBase", "BBase", "QBBase", "TBase", "FORWARD",
     "INVERSE", "ADD", "SUB", "MUL", "MULMUL", "ADDADD", "DISCRETE_GAUSSIAN", "HAMMINGWEIGHT", "NARROW", "ZO",
-    "BINARY", "UNIFORM", "TERNARY", "GAUSSIAN", "HOSTSTATE", "RNSSTATE", "BOTHSTATE",
+    "BINARY", "UNIFORM", "TERNARY", "GAUSSIAN", "HOSTSTATE", "RNSSTATE", "BOTHSTATE", "UNIFORM_MOD_Q", "ZO_IID",
 ]
 
 
@@ -664,6 +667,18 @@ class Sampler:
     def destroy(cls):
         pass
 
+    @staticmethod
+    def device_kind(e: Engine, kind: int) -> int:
+        """cuPoly's names keep cuPoly's meanings (src/cuda/sampler.cu:236-341): on a BFV
+        engine UNIFORM is one value below 2^32 written to every residue and ZO has
+        exactly nphi/2 nonzero coefficients.  UNIFORM_MOD_Q and ZO_IID select the
+        library's independent forms; cuPoly's CKKS UNIFORM is already per residue."""
+        if kind == UNIFORM:
+            return UNIFORM if e.ckks_prec else UNIFORM_U32
+        if kind == ZO:
+            return ZO_HALF
+        return {UNIFORM_MOD_Q: UNIFORM, ZO_IID: ZO}.get(kind, kind)
+
     @classmethod
     def sample(cls, ctx: Context, p: Optional[poly_t] = None, kind: int = UNIFORM):
         """sample(ctx, p, kind) fills p; sample(ctx, kind) returns a new poly_t."""
@@ -676,6 +691,7 @@ class Sampler:
         e = _E()
         sid = cls._counter
         cls._counter += 1
-        e.sample(p.d_coefs, p.base, kind, cls.seed, sid, npolys=1, to_dgt=True, stream=ctx.stream)
+        e.sample(p.d_coefs, p.base, cls.device_kind(e, kind), cls.seed, sid, npolys=1, to_dgt=True,
+                 stream=ctx.stream)
         p.status = RNSSTATE
         return p if ret else None

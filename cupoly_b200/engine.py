@@ -22,6 +22,7 @@ QBase, BBase, QBBase, TBase = 0, 1, 2, 3
 FORWARD, INVERSE = 0, 1
 ADD, SUB, MUL, MULMUL, ADDADD = 0, 1, 2, 3, 4
 (DISCRETE_GAUSSIAN, HAMMINGWEIGHT, NARROW, ZO, BINARY, UNIFORM, TERNARY, GAUSSIAN) = range(8)
+UNIFORM_U32, ZO_HALF = 9, 10  # cuPoly's BFV UNIFORM and ZO (enum cp_distribution)
 DESTROY_INPUTS = 1
 
 

@@ -13,8 +13,12 @@
 #include <cuPoly/cuda/sampler.h>
 
 #include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <sstream>
 
 // ---------------------------------------------------------------------------
@@ -98,6 +102,168 @@ NTL::ZZ zz_from_decimal(const std::string& s) { return NTL::conv<NTL::ZZ>(s.c_st
 // x mod m in [0, m) for m > 0 (NTL's % takes the sign of the divisor).
 NTL::ZZ floor_mod(const NTL::ZZ& x, const NTL::ZZ& m) { return x % m; }
 
+// ---- cuPoly's tabulated roots of i, read from its own data files ----
+//
+// cuPoly's NTHROOT[p][N] (src/arithmetic/coprimes.cu:868, used by
+// src/cuda/dgt.cu:1610-1692) is generated from the JSON files of
+// src/arithmetic/coprimes/: qis_<bits>.json maps each prime p of that bit
+// length to [ {N: {"re": ..., "imag": ...}, ...}, ... ], the first element
+// holding xi with xi^N = i.  A minimal reader of that format follows: objects,
+// arrays, strings and unsigned integers (the only value types those files use).
+struct RootFileReader {
+  const std::string& s;
+  size_t i = 0;
+  explicit RootFileReader(const std::string& text) : s(text) {}
+  void ws() {
+    while (i < s.size() && std::isspace((unsigned char)s[i])) ++i;
+  }
+  bool eat(char c) {
+    ws();
+    if (i < s.size() && s[i] == c) {
+      ++i;
+      return true;
+    }
+    return false;
+  }
+  void expect(char c) {
+    if (!eat(c)) throw std::runtime_error(std::string("cuPoly root table: expected '") + c + "'");
+  }
+  std::string str() {
+    expect('"');
+    const size_t b = i;
+    while (i < s.size() && s[i] != '"') ++i;
+    require(i < s.size(), "cuPoly root table: unterminated string");
+    return s.substr(b, i++ - b);
+  }
+  uint64_t num() {
+    ws();
+    const size_t b = i;
+    while (i < s.size() && std::isdigit((unsigned char)s[i])) ++i;
+    require(i > b && i - b <= 20, "cuPoly root table: expected an unsigned integer");
+    errno = 0;
+    const unsigned long long v = std::strtoull(s.c_str() + b, nullptr, 10);
+    require(errno == 0, "cuPoly root table: integer out of range");
+    return (uint64_t)v;
+  }
+  void skip() {  // any value
+    ws();
+    require(i < s.size(), "cuPoly root table: truncated");
+    if (s[i] == '{') {
+      ++i;
+      if (eat('}')) return;
+      do {
+        str();
+        expect(':');
+        skip();
+      } while (eat(','));
+      expect('}');
+    } else if (s[i] == '[') {
+      ++i;
+      if (eat(']')) return;
+      do skip();
+      while (eat(','));
+      expect(']');
+    } else if (s[i] == '"') {
+      str();
+    } else {
+      num();
+    }
+  }
+  // {"re": a, "imag": b}
+  std::pair<uint64_t, uint64_t> gauss() {
+    uint64_t re = 0, im = 0;
+    int seen = 0;
+    expect('{');
+    do {
+      const std::string k = str();
+      expect(':');
+      if (k == "re") re = num(), seen |= 1;
+      else if (k == "imag") im = num(), seen |= 2;
+      else skip();
+    } while (eat(','));
+    expect('}');
+    require(seen == 3, "cuPoly root table: a root lacks re or imag");
+    return {re, im};
+  }
+  // Whole file: p -> (N -> xi) from the first element of each prime's array.
+  void read(std::map<uint64_t, std::map<int, std::pair<uint64_t, uint64_t>>>& out) {
+    expect('{');
+    if (eat('}')) return;
+    do {
+      const uint64_t p = std::strtoull(str().c_str(), nullptr, 10);
+      expect(':');
+      expect('[');
+      auto& roots = out[p];
+      if (!eat(']')) {
+        expect('{');
+        if (!eat('}')) {
+          do {
+            const int n = std::atoi(str().c_str());
+            expect(':');
+            roots[n] = gauss();
+          } while (eat(','));
+          expect('}');
+        }
+        while (eat(',')) skip();
+        expect(']');
+      }
+    } while (eat(','));
+    expect('}');
+  }
+};
+
+// Load xi = NTHROOT[p][N] for every prime of the engine from cuPoly's
+// coprimes directory and install it (cp_engine_set_nthroot).
+void load_cupoly_roots(cp_engine* e, const std::string& dir, int N) {
+  const int n = cp_engine_n_residues(e, CP_QBBASE);
+  std::vector<uint64_t> ps(n), xi(2 * (size_t)n);
+  require(cp_engine_primes(e, ps.data(), n) == n, "cp_engine_primes failed");
+  std::map<int, std::map<uint64_t, std::map<int, std::pair<uint64_t, uint64_t>>>> files;  // by bit length
+  for (int r = 0; r < n; ++r) {
+    const int bits = 64 - __builtin_clzll(ps[r]);
+    if (!files.count(bits)) {
+      const std::string path = dir + "/qis_" + std::to_string(bits) + ".json";
+      std::FILE* f = std::fopen(path.c_str(), "rb");
+      if (!f) throw std::runtime_error("cuPoly root table: cannot open " + path);
+      std::string text;
+      char buf[1 << 16];
+      size_t got;
+      while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
+      std::fclose(f);
+      RootFileReader(text).read(files[bits]);
+    }
+    const auto& tab = files[bits];
+    const auto pi = tab.find(ps[r]);
+    const bool found = pi != tab.end() && pi->second.count(N);
+    if (!found)
+      throw std::runtime_error("cuPoly root table in " + dir + " has no root for prime " + std::to_string(ps[r]) +
+                               " and N = " + std::to_string(N));
+    const auto x = pi->second.at(N);
+    xi[2 * (size_t)r] = x.first;
+    xi[2 * (size_t)r + 1] = x.second;
+  }
+  check(cp_engine_set_nthroot(e, xi.data()), "cp_engine_set_nthroot (cuPoly's root table)");
+}
+
+// With CUPOLY_COPRIMES_DIR set, engines take cuPoly's roots; otherwise the
+// library's canonical root, said once on stderr (coefficient-domain results
+// are the same either way; only the DGT-domain bytes of poly_t::d_coefs differ).
+void apply_root_table(cp_engine* e, int N) {
+  const char* dir = std::getenv("CUPOLY_COPRIMES_DIR");
+  if (dir && *dir) {
+    load_cupoly_roots(e, dir, N);
+    return;
+  }
+  static bool said = false;
+  if (!said) {
+    said = true;
+    std::fprintf(stderr,
+                 "cupoly_b200: DGT-domain bytes use the library's canonical root of i; set CUPOLY_COPRIMES_DIR to "
+                 "cuPoly's src/arithmetic/coprimes directory for cuPoly's own (coefficient-domain results do not "
+                 "depend on it)\n");
+  }
+}
+
 void d2d(void* dst, const void* src, size_t bytes, Context* ctx) {
   if (dst == src || bytes == 0) return;
   cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->get_stream()), "cudaMemcpyAsync");
@@ -163,8 +329,13 @@ static void fill_statics(int M) {
     const uint64_t r = (uint64_t)NTL::conv<unsigned long>(m % zz_u64(q));
     CUDAEngine::RNSInvMpi.push_back(inv_mod(r, q));
   }
+  apply_root_table(e, M / 2);
   DGTEngine::init();
   CUDAEngine::is_init = 1;
+}
+
+void CUDAEngine::load_nthroot_table(const std::string& coprimes_dir) {
+  load_cupoly_roots(handle(), coprimes_dir, N);
 }
 
 void CUDAEngine::init_bfv(int k, int kl, int M, uint64_t t_) {
@@ -902,9 +1073,21 @@ uint32_t Sampler::counter = 0;
 void Sampler::init(Context*) { counter = 0; }
 void Sampler::reset(Context*) { counter = 0; }
 
+// cuPoly's names keep cuPoly's meanings; the layer-only kinds select the
+// library's independent forms.  cuPoly's CKKS UNIFORM is per residue already.
+static int device_kind(int kind) {
+  switch (kind) {
+    case UNIFORM: return CUDAEngine::scalingfactor ? CP_UNIFORM : CP_UNIFORM_U32;
+    case ZO: return CP_ZO_HALF;
+    case UNIFORM_MOD_Q: return CP_UNIFORM;
+    case ZO_IID: return CP_ZO;
+    default: return kind;
+  }
+}
+
 void Sampler::sample(Context* ctx, poly_t* p, int kind) {
   poly_init(ctx, p);
-  check(cp_sample(E(), p->d_coefs, p->base, kind, seed, counter++, 1, 1, S(ctx)), "Sampler::sample");
+  check(cp_sample(E(), p->d_coefs, p->base, device_kind(kind), seed, counter++, 1, 1, S(ctx)), "Sampler::sample");
   p->status = RNSSTATE;
 }
 

@@ -50,6 +50,13 @@ class CUDAEngine {
   static void destroy();
   static int get_n_residues(int base);
   static cp_engine* handle();  // the engine; throws when not initialised
+  // DGT-domain roots: engines use the library's canonical root of i unless the
+  // environment variable CUPOLY_COPRIMES_DIR names cuPoly's
+  // src/arithmetic/coprimes directory at init, in which case they take
+  // cuPoly's NTHROOT (coprimes.cu:868) from its qis_<bits>.json files and
+  // poly_t::d_coefs holds cuPoly's own DGT-domain bytes.  This loads the same
+  // table into the current engine explicitly (throws when a root is missing).
+  static void load_nthroot_table(const std::string& coprimes_dir);
 
   // cudaengine.h:140-185 (elementwise, any domain)
   static void execute_polynomial_negate(GaussianInteger* b, const GaussianInteger* a, const int base, Context* ctx);

@@ -49,7 +49,12 @@ enum cp_distribution {                                                  /* pdist
   CP_BINARY = 4,            /* uniform {0, 1} */
   CP_UNIFORM = 5,           /* uniform mod q_i, independent per residue */
   CP_TERNARY = 6,           /* uniform {-1, 0, +1} (secrets) */
-  CP_GAUSSIAN = 7           /* discrete Gaussian, sigma = 3.19, |x| <= 19, signed (errors) */
+  CP_GAUSSIAN = 7,          /* discrete Gaussian, sigma = 3.19, |x| <= 19, signed (errors) */
+  /* cuPoly's BFV meanings of UNIFORM and ZO, under their own values:           */
+  CP_UNIFORM_U32 = 9,       /* one value uniform in [0, 2^32) per coefficient, the same on every
+                               residue (sampler.cu:295-341: floor(u (2^32 - 1)) for all residues) */
+  CP_ZO_HALF = 10           /* exactly nphi/2 coefficients nonzero, each +-1 with probability 1/2
+                               (sampler.cu:236-283: N values in {1, 2} shuffled among 2N) */
 };
 /* flags of the composite scaling calls */
 #define CP_DESTROY_INPUTS 1u /* inverse-transform the inputs in place, as cuPoly does (polynomial.h:346-347) */

@@ -361,7 +361,7 @@ TEST_F(TestArithmetic, MulBaseB) {
 
 TEST_F(TestArithmetic, DR2) {
   poly_t a0, a1, b0, b1, c0, c1, c2;
-  for (poly_t* x : {&a0, &a1, &b0, &b1}) Sampler::sample(F.ctx, x, UNIFORM);
+  for (poly_t* x : {&a0, &a1, &b0, &b1}) Sampler::sample(F.ctx, x, UNIFORM_MOD_Q);
   poly_dr2(F.ctx, &c0, &c1, &c2, &a0, &a1, &b0, &b1);
   const auto A0 = F.coeffs(&a0), A1 = F.coeffs(&a1), B0 = F.coeffs(&b0), B1 = F.coeffs(&b1);
   const auto C0 = F.coeffs(&c0), C1 = F.coeffs(&c1), C2 = F.coeffs(&c2);
@@ -396,8 +396,8 @@ TEST_F(TestArithmetic, MulByInt) {
 TEST_F(TestArithmetic, Dot) {
   poly_t a[3], b[3], c;
   for (int i = 0; i < 3; ++i) {
-    Sampler::sample(F.ctx, &a[i], UNIFORM);
-    Sampler::sample(F.ctx, &b[i], UNIFORM);
+    Sampler::sample(F.ctx, &a[i], UNIFORM_MOD_Q);
+    Sampler::sample(F.ctx, &b[i], UNIFORM_MOD_Q);
   }
   poly_dot(F.ctx, &c, a, b, 3);
   std::vector<std::vector<ZZ>> va, vb;
@@ -440,6 +440,43 @@ TEST_F(TestSampler, Uniform) {
   CHECK(poly_get_deg(F.ctx, a) > 0, "degree");
   poly_free(F.ctx, a);
   delete a;
+}
+
+// cuPoly's BFV UNIFORM (sampler.cu:295-341): one value below 2^32 on every residue.
+TEST_F(TestSampler, UniformBelow2To32) {
+  poly_t a;
+  Sampler::sample(F.ctx, &a, UNIFORM);
+  const ZZ lim = ZZ(1) << 32;
+  for (int i = 0; i < F.nphi; ++i) CHECK(poly_get_coeff(F.ctx, &a, i) < lim, "index " << i);
+  poly_free(F.ctx, &a);
+}
+
+// The library's independent form: uniform mod Q, so values far above 2^32 appear.
+TEST_F(TestSampler, UniformModQ) {
+  poly_t a;
+  Sampler::sample(F.ctx, &a, UNIFORM_MOD_Q);
+  ZZ mx(0);
+  for (int i = 0; i < F.nphi; ++i) {
+    const ZZ c = poly_get_coeff(F.ctx, &a, i);
+    CHECK(c < F.q, "index " << i);
+    if (c > mx) mx = c;
+  }
+  if (F.nphi >= 128) CHECK(mx > (ZZ(1) << 40), "largest coefficient " << mx);
+  poly_free(F.ctx, &a);
+}
+
+// cuPoly's ZO (sampler.cu:236-283): exactly nphi/2 coefficients in {-1, +1}.
+TEST_F(TestSampler, ZOHalf) {
+  poly_t a;
+  Sampler::sample(F.ctx, &a, ZO);
+  int nz = 0;
+  for (int i = 0; i < F.nphi; ++i) {
+    const ZZ c = poly_get_coeff(F.ctx, &a, i);
+    CHECK(c == ZZ(0) || c == ZZ(1) || c == F.q - 1, "index " << i);
+    nz += c != ZZ(0);
+  }
+  CHECK(nz == F.nphi / 2, "nonzero " << nz);
+  poly_free(F.ctx, &a);
 }
 
 TEST_F(TestSampler, Narrow) {

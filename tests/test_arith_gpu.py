@@ -162,7 +162,7 @@ def test_reference_mul_base_b(gpu, logq2, nphi):
     aq, bq, ab, bb, cb = (cp.poly_t() for _ in range(5))
     for x in (aq, bq):
         cp.poly_init(ctx, x)
-        cp.Sampler.sample(ctx, x, cp.UNIFORM)
+        cp.Sampler.sample(ctx, x, cp.UNIFORM_MOD_Q)
     A = [cp.poly_get_coeff(ctx, aq, i) for i in range(nphi)]
     Bc = [cp.poly_get_coeff(ctx, bq, i) for i in range(nphi)]
     cp.poly_basis_extension_Q_to_B(ctx, ab, aq)
@@ -279,7 +279,7 @@ def test_poly_dot_mirror_matches_composition(gpu):
     B = [cp.poly_t() for _ in range(k)]
     for x in A + B:
         cp.poly_init(ctx, x)
-        cp.Sampler.sample(ctx, x, cp.UNIFORM)
+        cp.Sampler.sample(ctx, x, cp.UNIFORM_MOD_Q)
 
     def composed(a, b, c=None):
         c = cp.poly_t() if c is None else c

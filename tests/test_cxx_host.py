@@ -17,7 +17,10 @@ from cupoly_b200 import build as B
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CXX_DIR = os.path.join(ROOT, "tests", "cxx")
-REF_DEMO = "/root/reference/demos/src/simple_polyop.cpp"
+# cuPoly's own demo, compiled unmodified against the layer when a cuPoly source
+# tree is named by CUPOLY_REF_DIR (the test is skipped otherwise).
+REF_DIR = os.environ.get("CUPOLY_REF_DIR", "")
+REF_DEMO = os.path.join(REF_DIR, "demos", "src", "simple_polyop.cpp") if REF_DIR else ""
 
 # C++ names (demangled) the layer must export: cuPoly's public API surface.
 API = [
@@ -113,3 +116,66 @@ def test_cxx_host_layer_suite_on_gpu(gpu, host_lib, tmp_path):
     tail = (r.stdout + r.stderr)[-4000:]
     assert r.returncode == 0, tail
     assert " 0 failed" in r.stdout, tail
+
+
+def _write_cupoly_root_dir(d):
+    """A directory laid out like cuPoly's src/arithmetic/coprimes: qis_63.json in its
+    format ({p: [{N: {"re", "imag"}}, ...]}) with cuPoly's NTHROOT values from
+    tests/golden/ref_nthroot.json."""
+    import json
+    roots = json.load(open(os.path.join(ROOT, "tests", "golden", "ref_nthroot.json")))
+    doc = {p: [{n: {"re": v[0], "imag": v[1]} for n, v in by_n.items()}, {}] for p, by_n in roots.items()}
+    with open(os.path.join(d, "qis_63.json"), "w") as f:
+        json.dump(doc, f, indent=1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k,kl,nphi", [(5, 6, 8192), (16, 17, 32768)])
+def test_cxx_layer_loads_cupolys_roots_from_its_coprimes_dir(gpu, host_lib, tmp_path, k, kl, nphi):
+    """With CUPOLY_COPRIMES_DIR set, CUDAEngine::init takes cuPoly's NTHROOT and the C++
+    layer's DGT-domain bytes are cuPoly's: at nphi 8192 / k 5 / kl 6 they equal the bytes
+    cuPoly itself produced on the same input (tests/golden/cupoly_ref_golden.json); at
+    nphi 32768 / k 16 / kl 17 (beyond cuPoly's 30-prime limit) they equal the oracle's
+    transform with cuPoly's roots.  Without the variable the layer keeps its canonical
+    root, says so on stderr, and the bytes equal the oracle's with that root."""
+    import json
+
+    import numpy as np
+
+    from oracle import coracle as CO
+    from oracle import pyoracle as O
+    from tests.common import fold, random_poly_residues, sha
+    exe = _compile(os.path.join(CXX_DIR, "dgt_bytes.cpp"), str(tmp_path / "dgt_bytes"))
+    Q, B = O.bases(k, kl)
+    golden = None
+    gpath = os.path.join(ROOT, "tests", "golden", "cupoly_ref_golden.json")
+    if os.path.exists(gpath):
+        golden = next((c for c in json.load(open(gpath))["cases"]
+                       if c["op"] == "dgt" and (c["k"], c["kl"], c["nphi"]) == (k, kl, nphi)), None)
+    if golden is not None:
+        from tests.golden.gen_cupoly_golden import inputs
+        x = inputs("dgt", k, kl, nphi, golden["seed"]).reshape(k + kl, nphi)
+    else:
+        x = random_poly_residues(77, Q + B, nphi)
+    fin, fout = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    x.astype(np.uint64).tofile(fin)
+    rdir = tmp_path / "coprimes"
+    rdir.mkdir()
+    _write_cupoly_root_dir(str(rdir))
+    env = dict(os.environ, CUPOLY_COPRIMES_DIR=str(rdir))
+    r = subprocess.run([exe, str(k), str(kl), str(nphi), fin, fout], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(fout, dtype=np.uint64).reshape(k + kl, nphi // 2, 2)
+    roots = json.load(open(os.path.join(ROOT, "tests", "golden", "ref_nthroot.json")))
+    want = CO.dgt(fold(x)[None], Q + B, xi=[tuple(roots[str(p)][str(nphi // 2)]) for p in Q + B])[0]
+    assert np.array_equal(got, want)
+    if golden is not None:
+        assert sha(got) == golden["sha256"]
+    env.pop("CUPOLY_COPRIMES_DIR")
+    r = subprocess.run([exe, str(k), str(kl), str(nphi), fin, fout], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "CUPOLY_COPRIMES_DIR" in r.stderr
+    got = np.fromfile(fout, dtype=np.uint64).reshape(k + kl, nphi // 2, 2)
+    assert np.array_equal(got, CO.dgt(fold(x)[None], Q + B)[0])

@@ -143,14 +143,14 @@ def test_reference_rns_tests(gpu, logq2, nphi):
     # simple scaling vs round(t x / q) mod t
     a, b = cp.poly_t(), cp.poly_t()
     cp.poly_init(ctx, a)
-    cp.Sampler.sample(ctx, a, cp.UNIFORM)
+    cp.Sampler.sample(ctx, a, cp.UNIFORM_MOD_Q)
     A = [cp.poly_get_coeff(ctx, a, i) for i in range(nphi)]
     cp.poly_simple_scaling_tDivQ(ctx, b, a)
     assert [cp.poly_get_coeff(ctx, b, i) for i in range(nphi)] == [(2 * t * x + q) // (2 * q) % t for x in A]
     # complex scaling: |b - t c / q| < 2 in the reference; here exact round(t c / q)
     aq2, ab2, out = cp.poly_t(), cp.poly_t(), cp.poly_t()
     cp.poly_init(ctx, aq2)
-    cp.Sampler.sample(ctx, aq2, cp.UNIFORM)
+    cp.Sampler.sample(ctx, aq2, cp.UNIFORM_MOD_Q)
     C = [cp.poly_get_coeff(ctx, aq2, i) for i in range(nphi)]
     cp.poly_basis_extension_Q_to_B(ctx, ab2, aq2)
     cp.poly_complex_scaling_tDivQ(ctx, out, aq2, ab2)
