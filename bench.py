@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-next", action="store_true", help="skip the CRT / xi-rho / wire / CKKS measurements")
-    ap.add_argument("--serving-requests", type=int, default=10000)
+    ap.add_argument("--serving-requests", type=int, default=50000)
     return ap.parse_args()
 
 
@@ -591,43 +591,63 @@ def run_ours(args, D: Dist):
     ev1.record(stream)
     torch.cuda.synchronize()
     polymul_value = NPm * 6 / (ev0.elapsed_time(ev1) / 1e3)
-    del pa, pb, pc, pouts, ppm, qa, qb, qc
+    # the timed outputs must be the bytes of one plain cp_polymul call on the same operands
+    pref = e1.empty(QBase, NPm)
+    e1.polymul(pref, pa, pb, QBase, e1.polymul_workspace(QBase, NPm), NPm)
+    torch.cuda.synchronize()
+    if not (torch.equal(pref, pouts[0]) and torch.equal(pref, pouts[1])):
+        raise RuntimeError("pipelined polymul outputs differ from a single cp_polymul call")
+    del pa, pb, pc, pouts, ppm, qa, qb, qc, pref
 
     # ---- mixed-size batch: 1024 products, nphi in {2048..16384}, k in 1..8, one CUDA graph ----
     from cupoly_b200.batch import MixedPolymul, random_specs
     mixed_specs = random_specs(1024, seed)
     # two instances (own buffers), their graphs replayed alternately on two streams: two
     # consecutive batches in flight
-    mps = [MixedPolymul(mixed_specs) for _ in range(2)]
-    for mp in mps:
-        for g in mp.groups.values():  # residues below 2^62 are valid for every prime of the table
-            g["a"].random_(0, 1 << 62)
-            g["b"].random_(0, 1 << 62)
-        mp.capture()
-    mp = mps[0]
     m_streams = [torch.cuda.Stream(), torch.cuda.Stream()]
 
-    def mixed_batches(n):
+    def mixed_batches(mps_, n):
         for ms_ in m_streams:
             ms_.wait_stream(stream)
         for i in range(n):
             with torch.cuda.stream(m_streams[i & 1]):
-                mps[i & 1].graph.replay()
+                mps_[i & 1].graph.replay()
         for ms_ in m_streams:
             stream.wait_stream(ms_)
 
-    mixed_batches(2)
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    mixed_batches(6)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    mixed_ms = ev0.elapsed_time(ev1) / 6
+    # three forms of the same batch: the per-size-group launches in one graph (in sequence, or
+    # one parallel branch per group), and ONE persistent launch over a tile work list
+    mixed_forms, mixed_launches = {}, {}
+    for form in ("sequence", "branches", "tiles"):
+        mps = [MixedPolymul(mixed_specs, mode="tiles" if form == "tiles" else "graph") for _ in range(2)]
+        for mp in mps:
+            for g in mp.groups.values():  # residues below 2^62 are valid for every prime of the table
+                g["a"].random_(0, 1 << 62)
+                g["b"].random_(0, 1 << 62)
+            mp.capture(branches=form == "branches")
+        mixed_batches(mps, 2)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        mixed_batches(mps, 6)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        mixed_forms[form] = ev0.elapsed_time(ev1) / 6
+        mixed_launches[form] = mps[0].launches_per_run()
+        mixed_bytes = mps[0].algorithmic_bytes()
+        del mps, mp
+        torch.cuda.empty_cache()
+    best = min(mixed_forms, key=mixed_forms.get)
+    mixed_ms = mixed_forms[best]
     mixed = {"config": "1024 products, nphi uniform in {2048, 4096, 8192, 16384}, k uniform in 1..8 (seeded), "
-                       "one CUDA graph of %d launches per batch, 2 batches in flight" % mp.launches_per_run(),
+                       "2 batches in flight; fastest of three forms: %s" % best,
+             "form": {"sequence": "one CUDA graph, per size group a fused cp_polymul_list (3 launches)",
+                      "branches": "the same graph with one parallel branch per size group",
+                      "tiles": "one persistent launch (cp_polymul_tiles) over a work list of tiles"}[best],
+             "launches_per_batch": mixed_launches[best],
              "polymul_per_s": round(1024 / (mixed_ms / 1e3), 1), "ms_per_batch": round(mixed_ms, 3),
-             "algorithmic_GB_per_s": round(mp.algorithmic_bytes() / (mixed_ms / 1e3) / 1e9, 1)}
-    del mp, mps
+             "ms_per_batch_by_form": {k_: round(v_, 4) for k_, v_ in mixed_forms.items()},
+             "launches_by_form": mixed_launches,
+             "algorithmic_GB_per_s": round(mixed_bytes / (mixed_ms / 1e3) / 1e9, 1)}
     torch.cuda.empty_cache()
 
     # ---- north-star configuration: nphi = 16384 (N = 2^14 coefficients), |Q| = 10, batched vs plain ----
@@ -767,7 +787,7 @@ def run_ours(args, D: Dist):
                          # kernel, 3072 residues of N = 4096) from one ncu capture; writes read low
                          # because dirty lines are still in L2 when the kernel ends
                          "traffic": 347860480 if (e.N == 4096 and 4 * P * K_B == 3072) else None,
-                         "traffic_source": "ncu capture summarised in profiles/k_dgt_fwd_nphi8192_k5_ncu.md",
+                         "traffic_source": "ncu capture",
                          "kernel": "k_dgt_fwd (forward DGT, %d residues of N=%d per launch, timed alone)" %
                                    (4 * P * K_B, e.N),
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback",

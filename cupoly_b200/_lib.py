@@ -69,6 +69,9 @@ SIGNATURES = {
     "cp_polymul_workspace_bytes": (C.c_size_t, [_vp, _i, _i]),
     "cp_polymul": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),
     "cp_polymul_list": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
+    "cp_polymul_tiles_workspace_bytes": (C.c_size_t, []),
+    "cp_polymul_tiles": (_i, [C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
+                              C.POINTER(_i), _vp, _i, _vp, C.c_size_t, _vp]),
     "cp_add": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
     "cp_sub": (_i, [_vp, _vp, _vp, _vp, _i, _vp]),
     "cp_double_add": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),

@@ -7,7 +7,11 @@ instance is one entry of a work list (data pointer implied by its position,
 prime index = its residue number), and one fused `cp_polymul_list` serves the
 whole group whatever the mix of widths: an out-of-place forward DGT per
 operand and an inverse DGT that forms the products while loading.  All
-groups' launches are captured once in a CUDA graph and replayed.
+groups' launches are captured once in a CUDA graph and replayed (in sequence,
+or as one parallel branch per size group).  mode="tiles" runs the whole batch
+as ONE persistent launch instead (cp_polymul_tiles): one CTA per SM walks a
+device work list of same-size tiles, each residue's forward transforms,
+product and inverse done in shared memory in one pass over HBM.
 
 `BFVBatch`: the fused BFV multiplication chain over a fixed batch of pairs,
 captured in a CUDA graph.
@@ -18,30 +22,48 @@ overlapped with the chain.
 """
 from __future__ import annotations
 
+import ctypes as C
 from collections import OrderedDict
 from typing import List, Sequence, Tuple
 
 import numpy as np
 import torch
 
+from . import _lib
 from .engine import FORWARD, INVERSE, QBase, Engine, _ptr, _stream, from_u64, to_u64
 from ._lib import call
 
 
+TILE_SIZES = (2048, 4096, 8192, 16384)  # ring sizes of the single-launch form (N = 2^10 .. 2^13)
+
+
 class MixedPolymul:
-    def __init__(self, specs: Sequence[Tuple[int, int]], kmax: int = 8, autotune: bool = False):
-        """specs[i] = (nphi_i, k_i) with 1 <= k_i <= kmax."""
+    def __init__(self, specs: Sequence[Tuple[int, int]], kmax: int = 8, autotune: bool = False,
+                 mode: str = "graph"):
+        """specs[i] = (nphi_i, k_i) with 1 <= k_i <= kmax.
+
+        mode "graph": per size group one fused cp_polymul_list (3 launches) with the
+        group engine's tuned plan, all captured in one CUDA graph (see capture);
+        mode "tiles": the whole batch in ONE persistent launch (cp_polymul_tiles) over
+        a device work list of same-size tiles; every size must be in TILE_SIZES."""
+        if mode not in ("graph", "tiles"):
+            raise ValueError("mode must be 'graph' or 'tiles'")
+        self.mode = mode
         self.specs = list(specs)
         self.groups = OrderedDict()  # nphi -> dict
         for i, (nphi, k) in enumerate(self.specs):
             if not 1 <= k <= kmax:
                 raise ValueError("k must be in [1, kmax]")
+            if mode == "tiles" and nphi not in TILE_SIZES:
+                raise ValueError("the single-launch form covers nphi in %s" % (TILE_SIZES,))
             self.groups.setdefault(nphi, {"inst": []})["inst"].append(i)
         self.where = {}  # instance -> (nphi, first residue row)
         for nphi, g in self.groups.items():
             lr = 0
             lc = 0
-            if autotune:
+            if mode == "tiles":  # the tile kernel's plan: radix 8, the whole transform in one CTA
+                lr, lc = 3, (nphi // 2).bit_length() - 1
+            elif autotune:
                 from .autotune import best_plan
 
                 lr, lc = best_plan(nphi)
@@ -63,6 +85,35 @@ class MixedPolymul:
             g["wb"] = torch.empty_like(g["a"])
             g["c"] = torch.empty_like(g["a"])
         self.graph = None
+        if mode == "tiles":
+            self._build_tiles()
+
+    def _build_tiles(self):
+        """The device work list: each size group's rows cut into tiles of 8192 / N
+        rows, largest transforms first (they take longest per tile)."""
+        rows = []
+        for lg, nphi in reversed(list(enumerate(TILE_SIZES))):
+            g = self.groups.get(nphi)
+            if g is None:
+                continue
+            per = 16384 // nphi
+            rows += [(lg, r0, min(per, g["rows"] - r0)) for r0 in range(0, g["rows"], per)]
+        self.ntiles = len(rows)
+        self.tiles = torch.tensor(rows, dtype=torch.int32, device="cuda").reshape(-1, 3)
+        L = _lib.lib()
+        self.tile_ws = torch.empty(((L.cp_polymul_tiles_workspace_bytes() + 15) // 16, 2), dtype=torch.int64,
+                                   device="cuda")
+        vp = C.c_void_p
+        self._tile_args = [(vp * 4)() for _ in range(5)]
+        self._tile_rows = (C.c_int * 4)()
+        eng, cc, aa, bb, rr = self._tile_args
+        for lg, nphi in enumerate(TILE_SIZES):
+            g = self.groups.get(nphi)
+            if g is None:
+                continue
+            eng[lg] = g["engine"].handle
+            cc[lg], aa[lg], bb[lg], rr[lg] = (g[x].data_ptr() for x in ("c", "a", "b", "rid"))
+            self._tile_rows[lg] = g["rows"]
 
     # ---- data ----
     def set_inputs(self, i: int, a_rows: np.ndarray, b_rows: np.ndarray):
@@ -82,18 +133,42 @@ class MixedPolymul:
         return np.concatenate([x[..., 0], x[..., 1]], axis=-1)
 
     # ---- execution ----
+    def _launch_group(self, g, stream):
+        # fused: 2 out-of-place forward DGTs, inverse with products on load
+        e, n, rid = g["engine"], g["rows"], g["rid"]
+        call("cp_polymul_list", e.handle, _ptr(g["c"]), _ptr(g["a"]), _ptr(g["b"]), _ptr(g["wa"]),
+             _ptr(g["wb"]), _ptr(rid), n, _stream(stream))
+
     def _launch(self, stream=None):
-        s = _stream(stream)
-        for g in self.groups.values():  # fused: 2 out-of-place forward DGTs, inverse with products on load
-            e, n, rid = g["engine"], g["rows"], g["rid"]
-            call("cp_polymul_list", e.handle, _ptr(g["c"]), _ptr(g["a"]), _ptr(g["b"]), _ptr(g["wa"]),
-                 _ptr(g["wb"]), _ptr(rid), n, s)
+        if self.mode == "tiles":
+            eng, cc, aa, bb, rr = self._tile_args
+            call("cp_polymul_tiles", eng, cc, aa, bb, rr, self._tile_rows, _ptr(self.tiles), self.ntiles,
+                 _ptr(self.tile_ws), self.tile_ws.numel() * 8, _stream(stream))
+            return
+        for g in self.groups.values():
+            self._launch_group(g, stream)
+
+    def _launch_branches(self, stream):
+        """Every size group on a stream of its own, forked from and joined back into
+        `stream`: in a captured graph the groups become parallel branches, so one
+        group's last partial wave of CTAs overlaps the others' launches."""
+        if self.mode == "tiles":
+            raise ValueError("the single-launch form has no per-group branches")
+        if not hasattr(self, "_branch_streams"):
+            self._branch_streams = [torch.cuda.Stream() for _ in self.groups]
+        for g, bs in zip(self.groups.values(), self._branch_streams):
+            bs.wait_stream(stream)
+            self._launch_group(g, bs)
+        for bs in self._branch_streams:
+            stream.wait_stream(bs)
 
     def run(self):
         """Eager execution (also warms up every kernel before capture)."""
         self._launch()
 
-    def capture(self):
+    def capture(self, branches: bool = False):
+        """Capture every group's launches in one CUDA graph: in sequence on one
+        stream, or (branches=True) as one parallel branch per size group."""
         self._launch()  # first launches set kernel attributes outside the capture
         torch.cuda.synchronize()
         self.graph = torch.cuda.CUDAGraph()
@@ -101,7 +176,10 @@ class MixedPolymul:
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             with torch.cuda.graph(self.graph, stream=s):
-                self._launch(stream=s)
+                if branches:
+                    self._launch_branches(s)
+                else:
+                    self._launch(stream=s)
         torch.cuda.current_stream().wait_stream(s)
         return self.graph
 
@@ -111,7 +189,7 @@ class MixedPolymul:
         self.graph.replay()
 
     def launches_per_run(self) -> int:
-        return 3 * len(self.groups)
+        return 1 if self.mode == "tiles" else 3 * len(self.groups)
 
     def algorithmic_bytes(self) -> int:
         """24 nphi k bytes per product: read a, b and write c (16 B per Gaussian element)."""
@@ -149,6 +227,14 @@ class BFVBatch:
         self.graph.replay()
 
 
+def _check_tensor(x: torch.Tensor, shape, what: str):
+    """Refuse a tensor the batched kernels would read or write past: they take
+    raw pointers and the batch's polynomial count."""
+    if tuple(x.shape) != tuple(shape) or x.dtype != torch.int64 or not x.is_contiguous() or not x.is_cuda:
+        raise ValueError("%s must be a contiguous int64 CUDA tensor of shape %s, got %s %s%s" %
+                         (what, tuple(shape), x.dtype, tuple(x.shape), "" if x.is_contiguous() else " (strided)"))
+
+
 class PipelinedBFV:
     """BFV multiplication of consecutive device-resident batches, `lanes` of them in flight.
 
@@ -172,11 +258,24 @@ class PipelinedBFV:
         """batches[i] = (a0, a1, b0, b1): npairs polynomials each, DGT domain, on the
         device; outputs[i] (3 npairs polynomials) receives its result.  The work is
         ordered after what `stream` (default: the current stream) has queued."""
+        if len(batches) != len(outputs):
+            raise ValueError("PipelinedBFV.run: %d batches but %d outputs" % (len(batches), len(outputs)))
+        shape = (self.P, self.e.k, self.e.N, 2)
+        for ins, out in zip(batches, outputs):
+            if len(ins) != 4:
+                raise ValueError("PipelinedBFV.run: a batch is (a0, a1, b0, b1)")
+            for x in ins:
+                _check_tensor(x, shape, "input")
+            _check_tensor(out, (3 * self.P,) + shape[1:], "output")
         cur = stream if stream is not None else torch.cuda.current_stream()
         for s in self.streams:
             s.wait_stream(cur)
         for i, (ins, out) in enumerate(zip(batches, outputs)):
             j = i % self.lanes
+            # The caller's tensors are used on a lane stream: keep the caching
+            # allocator from reusing their memory until that stream is done.
+            for x in (*ins, out):
+                x.record_stream(self.streams[j])
             self.e.bfv_mul_batch(out, *ins, self.P, self.ws[j], stream=self.streams[j])
 
     def join(self, stream=None):
@@ -203,12 +302,24 @@ class PipelinedPolymul:
         self.streams = [torch.cuda.Stream() for _ in range(lanes)]
 
     def run(self, batches, outputs, stream=None):
-        """batches[i] = (a, b), npolys polynomials each; outputs[i] receives a b."""
+        """batches[i] = (a, b), npolys polynomials each; outputs[i] receives a b.
+
+        Every a, b and output must hold exactly npolys contiguous polynomials of
+        the base (a short final batch needs its own PipelinedPolymul): the kernels
+        read and write npolys polynomials whatever the tensors hold."""
+        if len(batches) != len(outputs):
+            raise ValueError("PipelinedPolymul.run: %d batches but %d outputs" % (len(batches), len(outputs)))
+        shape = (self.P, self.e.n_residues(self.base), self.e.N, 2)
+        for (a, b), out in zip(batches, outputs):
+            for x, what in ((a, "a"), (b, "b"), (out, "output")):
+                _check_tensor(x, shape, what)
         cur = stream if stream is not None else torch.cuda.current_stream()
         for s in self.streams:
             s.wait_stream(cur)
         for i, ((a, b), out) in enumerate(zip(batches, outputs)):
             j = i % self.lanes
+            for x in (a, b, out):
+                x.record_stream(self.streams[j])
             self.e.polymul(out, a, b, self.base, self.ws[j], self.P, stream=self.streams[j])
 
     def join(self, stream=None):

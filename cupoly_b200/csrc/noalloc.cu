@@ -10,12 +10,17 @@
 // instead.
 //
 // The scratch is a file-scope __device__ array of CP_NOALLOC_SCRATCH_BYTES
-// (8 MiB).  Every GPU that loads this library holds it until the process
-// exits.  In host code `g_noalloc_scratch` names a host-side stand-in, not a
-// device address: it must never be passed to a kernel.  The device address is
-// obtained with cudaGetSymbolAddress once per device, with that device
-// current, on the first call made on that device; that first call should
-// therefore come before any stream capture.
+// (8 MiB).  It exists on a GPU once this library's device code is loaded
+// there: with CUDA's default lazy module loading that happens at the first
+// use of the module on that device, typically this entry point's first call,
+// and then it stays until the process exits.  That first call per device is a
+// warm-up: loading the module (and the 8 MiB with it) may itself allocate and
+// synchronise; every later call allocates nothing.  In host code
+// `g_noalloc_scratch` names a host-side stand-in, not a device address: it must
+// never be passed to a kernel.  The device address is obtained with
+// cudaGetSymbolAddress once per device, with that device current, on the first
+// call made on that device; that first call should therefore come before any
+// stream capture.  The current device must be the engine's device.
 //
 // All calls share the one array and it keeps whatever the last call left
 // there.  Nothing in it needs to start at zero: every region the chain uses
@@ -78,6 +83,17 @@ extern "C" int cp_bfv_mul_noalloc(const cp_engine* e, void* c0, void* c1, void* 
                   need, kScratchBytes);
     cpoly::set_error(msg);
     return CP_ERR_UNSUPPORTED;
+  }
+  int dev = -1;
+  if (cudaError_t err = cudaGetDevice(&dev)) return cpoly::cuda_fail("cp_bfv_mul_noalloc: cudaGetDevice", err);
+  if (dev != e->e.device) {
+    char msg[160];
+    std::snprintf(msg, sizeof msg,
+                  "cp_bfv_mul_noalloc: the current device (%d) is not the engine's device (%d); the static scratch "
+                  "is per device",
+                  dev, e->e.device);
+    cpoly::set_error(msg);
+    return CP_ERR_INVALID;
   }
   void* ws = nullptr;
   if (int rc = scratch_address(&ws)) return rc;

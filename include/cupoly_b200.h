@@ -156,6 +156,23 @@ int cp_polymul(const cp_engine* e, void* c, const void* a, const void* b, int ba
                void* stream);
 int cp_polymul_list(const cp_engine* e, void* c, const void* a, const void* b, void* wa, void* wb,
                     const int* rid_list, int nlist, void* stream);
+/* ---- the mixed-size batch of negacyclic products in ONE persistent launch (no
+ *      counterpart in cuPoly: one parameter set per process there).  Size group
+ *      lg = 0..3 holds rows[lg] residues of ring size N = 2^(10 + lg) (nphi 2048 ..
+ *      16384): coefficient-domain rows a[lg], b[lg] -> c[lg] (each rows[lg] x N x 16
+ *      bytes; c may alias a or b), residue i using prime rid[lg][i] (device int array)
+ *      of engines[lg].  engines[lg] must have N = 2^(10 + lg) and the whole-CTA
+ *      radix-8 plan (cp_engine_set_plan(e, 3, 10 + lg)); groups with rows[lg] = 0 may
+ *      pass NULL.  `tiles` (device) lists ntiles tiles {lg, first row, count} as three
+ *      ints each, count <= 8192 / N: one CTA per SM walks the list, each tile's
+ *      residues transformed side by side in shared memory (forward a, forward b,
+ *      product, inverse, in one pass over HBM).  Workspace: at least
+ *      cp_polymul_tiles_workspace_bytes() bytes of device memory (the current
+ *      device's SM count x 128 KB). ---- */
+size_t cp_polymul_tiles_workspace_bytes(void);
+int cp_polymul_tiles(const cp_engine* const* engines, void* const* c, const void* const* a, const void* const* b,
+                     const int* const* rid, const int* rows, const void* tiles, int ntiles, void* workspace,
+                     size_t workspace_bytes, void* stream);
 
 /* ---- pointwise, DGT domain: replace DGTEngine::execute_{add,sub,double_add,
  *      mul_dgt_gi,mul_dgt_u64,muladd,dr2}_dgt (src/cuda/dgt.cu:1096-1499) ---- */
@@ -235,12 +252,16 @@ int cp_bfv_mul(const cp_engine* e, void* c0, void* c1, void* c2, const void* a0,
  * forbids later allocation, code that must not take cudaMalloc's implicit
  * synchronisation, a plugin host with no allocator).  No counterpart in
  * cuPoly.  Scratch is a static device array of CP_NOALLOC_SCRATCH_BYTES inside
- * the library, held by every GPU that loads it until exit; parameter sets
- * needing more (cp_workspace_bytes(e) > CP_NOALLOC_SCRATCH_BYTES, e.g. nphi
- * 16384 with k = 10) return CP_ERR_UNSUPPORTED.  The first call on a device
- * looks up the array's device address, so make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU race; serialise
- * them.  Allocates nothing (no cudaMalloc/cudaFree). */
+ * the library, present on a GPU from the first use of the library's device
+ * code there until exit; parameter sets needing more (cp_workspace_bytes(e) >
+ * CP_NOALLOC_SCRATCH_BYTES, e.g. nphi 16384 with k = 10) return
+ * CP_ERR_UNSUPPORTED.  The current device must be the engine's
+ * (CP_ERR_INVALID otherwise).  The first call on a device is a warm-up: it may
+ * load the library's device code (and with it the array) and looks up the
+ * array's device address, so make it before any stream capture and before the
+ * part of the program that must not allocate.  All calls share the array:
+ * calls that overlap on the GPU race; serialise them.  Calls after the first
+ * allocate nothing (no cudaMalloc/cudaFree). */
 #define CP_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
 int cp_bfv_mul_noalloc(const cp_engine* e, void* c0, void* c1, void* c2, const void* a0, const void* a1,
                        const void* b0, const void* b1, void* stream);

@@ -339,3 +339,90 @@ def test_pipelined_polymul_equals_single_calls(gpu):
         e.polymul(ref, a, b, QBase, ws, P)
         torch.cuda.synchronize()
         assert torch.equal(ref, out)
+
+
+def test_mixed_polymul_benchmark_draw_all_1024_instances(gpu):
+    """The benchmark's mixed batch exactly: random_specs(1024, 0xC0FFEE) (nphi in
+    {2048 .. 16384}, k in 1..8), seeded operands per instance; every instance's product
+    is bit-exact against the oracle, for the graph in sequence and for the graph with
+    one parallel branch per size group."""
+    import torch
+    from cupoly_b200.batch import MixedPolymul, random_specs
+    specs = random_specs(1024, 0xC0FFEE)
+    mp = MixedPolymul(specs)
+    by_shape = {}
+    for i, (nphi, k) in enumerate(specs):
+        a = random_poly_residues(30000 + i, O.PRIMES[:k], nphi)
+        b = random_poly_residues(40000 + i, O.PRIMES[:k], nphi)
+        mp.set_inputs(i, a, b)
+        by_shape.setdefault((nphi, k), []).append((i, a, b))
+    want = {}
+    for (nphi, k), items in by_shape.items():
+        c = CO.polymul(np.stack([a for _, a, _ in items]), np.stack([b for _, _, b in items]), O.PRIMES[:k])
+        for (i, _, _), ci in zip(items, c):
+            want[i] = ci
+    for branches in (False, True):
+        for g in mp.groups.values():
+            g["c"].fill_(-1)
+        mp.capture(branches=branches)
+        mp.replay()
+        torch.cuda.synchronize()
+        for i in range(len(specs)):
+            assert np.array_equal(mp.result(i), want[i]), (i, specs[i], branches)
+    # the single persistent launch over the same draw
+    mt = MixedPolymul(specs, mode="tiles")
+    assert mt.launches_per_run() == 1
+    for i, (nphi, k) in enumerate(specs):
+        mt.set_inputs(i, random_poly_residues(30000 + i, O.PRIMES[:k], nphi),
+                      random_poly_residues(40000 + i, O.PRIMES[:k], nphi))
+    for g in mt.groups.values():
+        g["c"].fill_(-1)
+    mt.capture()
+    mt.replay()
+    torch.cuda.synchronize()
+    for i in range(len(specs)):
+        assert np.array_equal(mt.result(i), want[i]), (i, specs[i], "tiles")
+
+
+@pytest.mark.parametrize("specs", [[(2048, 1)], [(16384, 3)], [(4096, 2), (2048, 8), (8192, 1), (16384, 5)],
+                                   [(2048, 3)] * 5 + [(4096, 3)] * 3])
+def test_single_launch_polymul_tiles(gpu, specs):
+    """cp_polymul_tiles: partial and full tiles of every size, bit-exact against the
+    oracle and against the graph form, with outputs aliasing an input."""
+    import torch
+    from cupoly_b200.batch import MixedPolymul
+    mt = MixedPolymul(specs, mode="tiles")
+    data = []
+    for i, (nphi, k) in enumerate(specs):
+        a = random_poly_residues(500 + i, O.PRIMES[:k], nphi)
+        b = random_poly_residues(600 + i, O.PRIMES[:k], nphi)
+        mt.set_inputs(i, a, b)
+        data.append((a, b))
+    mt.run()
+    torch.cuda.synchronize()
+    for i, (nphi, k) in enumerate(specs):
+        a, b = data[i]
+        assert np.array_equal(mt.result(i), CO.polymul(a[None], b[None], O.PRIMES[:k])[0]), (i, nphi, k)
+    for g in mt.groups.values():  # c aliasing a
+        g["c"] = g["a"]
+    mt._build_tiles()
+    mt.run()
+    torch.cuda.synchronize()
+    for i, (nphi, k) in enumerate(specs):
+        a, b = data[i]
+        assert np.array_equal(mt.result(i), CO.polymul(a[None], b[None], O.PRIMES[:k])[0]), (i, nphi, k)
+
+
+def test_single_launch_polymul_rejects_other_plans(gpu):
+    """The tile kernel needs each size's whole-CTA radix-8 plan; an engine with another
+    plan is refused before launch."""
+    import ctypes as C
+    from cupoly_b200 import _lib
+    from cupoly_b200.batch import MixedPolymul
+    mt = MixedPolymul([(4096, 2)], mode="tiles")
+    g = mt.groups[4096]
+    g["engine"].set_plan(2, 11)
+    eng, cc, aa, bb, rr = mt._tile_args
+    rc = _lib.lib().cp_polymul_tiles(eng, cc, aa, bb, rr, mt._tile_rows, C.c_void_p(mt.tiles.data_ptr()),
+                                     mt.ntiles, C.c_void_p(mt.tile_ws.data_ptr()), mt.tile_ws.numel() * 8, None)
+    assert rc == 1 and b"radix-8 plan" in _lib.lib().cp_last_error()

@@ -51,6 +51,26 @@ def test_noalloc_matches_workspace_entry_point_on_consecutive_calls(gpu):
             assert torch.equal(g, r)
 
 
+def test_noalloc_warm_calls_leave_free_device_memory_unchanged(gpu):
+    """After the first call on the device (the warm-up that may load the
+    library's device code and its static scratch), calls take no device memory:
+    cudaMemGetInfo's free bytes are the same before and after two more calls."""
+    import torch
+    from cupoly_b200 import _lib
+    from cupoly_b200.engine import Engine
+    e = Engine(5, 6, 8192, 256)
+    ins = _inputs(e, 5)
+    got = [e.empty(0) for _ in range(3)]
+    assert _noalloc(e, got, ins) == 0, _lib.lib().cp_last_error()  # warm-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        assert _noalloc(e, got, ins) == 0, _lib.lib().cp_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_rejects_parameter_sets_beyond_the_static_scratch(gpu):
     from cupoly_b200 import _lib
     from cupoly_b200.engine import Engine
