@@ -37,11 +37,13 @@ struct TileGroup {
   const ulonglong2* b;
   ulonglong2* c;
   const int* rid;       // engine prime of each row
+  int rows;
   DgtArgs A;            // the engine's tables
 };
 
 struct TileArgs {
   TileGroup g[4];  // index log2(N) - 10
+  int* err;        // set when a tile of the list is out of range (it is skipped)
 };
 
 struct Tile {
@@ -284,6 +286,13 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   ulonglong2* slot = ws + (size_t)blockIdx.x * kTileElems;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const Tile tl = tiles[t];
+    // a tile naming an absent group, rows outside it, or more rows than fit is skipped
+    const bool ok = tl.lg >= 0 && tl.lg < 4 && args.g[tl.lg].rid != nullptr && tl.count >= 1 &&
+                    tl.count <= (8 >> tl.lg) && tl.row0 >= 0 && tl.row0 + tl.count <= args.g[tl.lg].rows;
+    if (!ok) {
+      if (threadIdx.x == 0) atomicExch(args.err, 1);
+      continue;
+    }
     switch (tl.lg) {
       case 0: tile_polymul<10>(args.g[0], tl.row0, tl.count, smem, slot); break;
       case 1: tile_polymul<11>(args.g[1], tl.row0, tl.count, smem, slot); break;
@@ -335,8 +344,14 @@ extern "C" int cp_polymul_tiles(const cp_engine* const* engines, void* const* c,
     g.a = reinterpret_cast<const ulonglong2*>(a[lg]);
     g.b = reinterpret_cast<const ulonglong2*>(b[lg]);
     g.c = reinterpret_cast<ulonglong2*>(c[lg]);
-    g.rid = rid[lg];
+    g.rid = rows[lg] > 0 ? rid[lg] : nullptr;
+    g.rows = rows[lg];
     g.A = DgtArgs{e.d_tab, e.layout.stride, e.layout, e.d_mc, nullptr};
+    if (!args.err) args.err = e.d_err;
+  }
+  if (ntiles > 0 && !args.err) {
+    set_error("cp_polymul_tiles: no engine given");
+    return CP_ERR_INVALID;
   }
   if (ntiles <= 0) return CP_OK;
   int dev = 0, sms = 0;

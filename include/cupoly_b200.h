@@ -166,9 +166,10 @@ int cp_polymul_list(const cp_engine* e, void* c, const void* a, const void* b, v
  *      pass NULL.  `tiles` (device) lists ntiles tiles {lg, first row, count} as three
  *      ints each, count <= 8192 / N: one CTA per SM walks the list, each tile's
  *      residues transformed side by side in shared memory (forward a, forward b,
- *      product, inverse, in one pass over HBM).  Workspace: at least
- *      cp_polymul_tiles_workspace_bytes() bytes of device memory (the current
- *      device's SM count x 128 KB). ---- */
+ *      product, inverse, in one pass over HBM).  A tile outside its group is skipped
+ *      and sets the device error flag of the first engine given (cp_engine_check).
+ *      Workspace: at least cp_polymul_tiles_workspace_bytes() bytes of device
+ *      memory (the current device's SM count x 128 KB). ---- */
 size_t cp_polymul_tiles_workspace_bytes(void);
 int cp_polymul_tiles(const cp_engine* const* engines, void* const* c, const void* const* a, const void* const* b,
                      const int* const* rid, const int* rows, const void* tiles, int ntiles, void* workspace,
