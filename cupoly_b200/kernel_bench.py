@@ -23,6 +23,9 @@ Workloads (names for --only):
                      operands read + 1 written
   dot_batch          cp_dot_batch: the xi decomposition of 128 polynomials against 5 shared key
                      polynomials, nphi 8192, k 5; bytes = decompositions + keys read + results written
+  mixed_tiles, mixed_graph
+                     the benchmark's mixed batch of 1024 negacyclic products (nphi 2048..16384,
+                     k 1..8, seeded draw): one persistent launch, or 3 launches per size group
   bfv_chain, bfv_chain_target, bfv_chain_large
                      the batched BFV multiplication chain (cp_bfv_mul_batch) at nphi 8192 / k 5 /
                      128 pairs, nphi 16384 / k 10 / 32 pairs and nphi 32768 / k 16 / t 65537 / 64
@@ -202,6 +205,23 @@ def workloads():
                 % (P, k), e)
 
     W["dot_batch"] = dot_batch
+
+    def mixed(mode):
+        def build():
+            from .batch import MixedPolymul, random_specs
+            mp = MixedPolymul(random_specs(1024, 0xC0FFEE), mode=mode)
+            for g in mp.groups.values():  # residues below 2^62 are valid for every prime of the table
+                g["a"].random_(0, 1 << 62)
+                g["b"].random_(0, 1 << 62)
+            e = next(iter(mp.groups.values()))["engine"]
+            return (mp.run, mp.algorithmic_bytes(),
+                    "mixed batch of 1024 polymuls (nphi 2048..16384, k 1..8), %s" %
+                    ("one persistent launch (cp_polymul_tiles)" if mode == "tiles"
+                     else "3 launches per size group (cp_polymul_list)"), e)
+        return build
+
+    W["mixed_tiles"] = mixed("tiles")
+    W["mixed_graph"] = mixed("graph")
     W["bfv_chain"] = chain(8192, 5, 256, 128)
     W["bfv_chain_target"] = chain(16384, 10, 256, 32)
     W["bfv_chain_large"] = chain(32768, 16, 65537, 64)
