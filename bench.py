@@ -14,9 +14,10 @@ streams, device-timed, max over ranks);
 `e2e` repeats it through the C ABI with pinned host buffers and the
 host<->device copies inside the timed region; `plain` is the per-call form
 (one cp_bfv_mul per pair); `polymul` is the batched DGT polymul/s of the
-nphi = 4096, k = 2 configuration.  With --impl reference the C oracle (the
-CPU restatement of the reference path; cuPoly itself cannot be built here) is
-timed on the host cores.
+nphi = 4096, k = 2 configuration; `cupoly_gpu` times cuPoly's own kernels
+per call when its sources were compiled into oracle/_ref.  With --impl
+reference the C oracle (the CPU restatement of the reference path: cuPoly has
+no CPU implementation of it) is timed on the host cores.
 """
 from __future__ import annotations
 
@@ -44,6 +45,7 @@ def parse():
     ap.add_argument("--pairs", type=int, default=128, help="ciphertext pairs per step (batched form)")
     ap.add_argument("--plain-pairs", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cupoly-gpu", action="store_true", help="skip timing cuPoly's own kernels")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-next", action="store_true", help="skip the CRT / xi-rho / wire / CKKS measurements")
@@ -390,6 +392,35 @@ def next_rows(seed: int, hbm_peak: float):
                                               "rescale": round(mb_resc * 1e3 / PB, 2)}}
     del a, qb, r, c, ab, qbb, rb, wsb
     torch.cuda.empty_cache()
+    return out
+
+
+CUPOLY_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cupoly_ref_driver")
+
+
+def cupoly_gpu_times():
+    """cuPoly's own per-call GPU times on this GPU, when its sources were compiled here
+    (oracle/cupoly_ref/Makefile): the polymul at nphi 4096, k 2 (two forward DGTs,
+    poly_mul, one inverse DGT per call) and the BFV multiplication chain at nphi 8192,
+    k 5, kl 6 (four poly_basis_extension_Q_to_B, poly_dr2 over Q and B, three
+    poly_complex_scaling_tDivQ per pair), each timed with CUDA events over 200 calls.
+    Context for the per-call forms here; the reference arm stays the CPU restatement."""
+    if not os.path.exists(CUPOLY_DRIVER):
+        return {"unavailable": "cuPoly's sources were not compiled into oracle/_ref"}
+    import tempfile
+
+    out = {}
+    for name, (k, nphi) in {"polymul_nphi4096_k2": (2, 4096), "bfv_mul_nphi8192_k5_kl6": (5, 8192)}.items():
+        with tempfile.TemporaryDirectory() as d:
+            f = os.path.join(d, "t.json")
+            r = subprocess.run([CUPOLY_DRIVER, "time", str(k), str(k + 1), str(nphi), "200", "-", f],
+                               capture_output=True, text=True, timeout=300)
+            if r.returncode != 0:
+                return {"unavailable": "cuPoly driver failed: " + (r.stderr or r.stdout)[-200:]}
+            t = json.load(open(f))
+        ms = t["polymul_ms"] if name.startswith("polymul") else t["bfv_mul_ms"]
+        out[name] = {"ms_per_call": round(ms, 4), "per_s": round(1e3 / ms, 1)}
+    out["source"] = "cuPoly 0.3.5 library (its own kernels), one call per polymul / pair, CUDA events"
     return out
 
 
@@ -753,6 +784,8 @@ def run_ours(args, D: Dist):
         del ex, sch
         torch.cuda.empty_cache()
 
+    cupoly_gpu = cupoly_gpu_times() if D.rank == 0 and not args.no_cupoly_gpu else None
+
     cpu = None
     if D.rank == 0 and not args.no_cpu_baseline:
         rate, done, el, cores = cpu_bfv_rate(10.0)
@@ -792,6 +825,7 @@ def run_ours(args, D: Dist):
                                    (4 * P * K_B, e.N),
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback",
                          "int": int_roof},
+            "cupoly_gpu": cupoly_gpu,
             "large": large,
             "next_rows": nxt,
             "serving": serving,
