@@ -119,6 +119,7 @@ struct Engine {
   // word offsets inside d_hps
   struct HpsOffsets {
     int qb_inv, qb_inv_s, qb_hor, qb_hor_s, qb_half;           // Q -> B
+    int q_lift, b_lift;  // MRC digits of T - 1, T = S - floor(S FPERROR): the lift threshold of Q, of B
     int bq_inv, bq_inv_s, bq_hor, bq_hor_s;                    // B -> Q
     int qt_hor, qt_hor_s;                                      // Q -> t
     int q_mod_b, q_mod_b_s;        // Q mod b_j

@@ -8,7 +8,10 @@
 // use only word-size modular arithmetic:
 //  * base conversion: mixed-radix digits d_i of X (MRC), then X mod m as the
 //    dot product sum_i d_i (prod_{l<i} s_l mod m), accumulated in 192 bits
-//    and reduced once per target;
+//    and reduced once per target.  The lift is cuPoly's, decided exactly:
+//    X in [0, S) is read as X - S when S - X <= S FPERROR (cuPoly's v rounds
+//    up there), which makes the small negative values that the scaled BFV
+//    tensor produces come out negative, as in cuPoly;
 //  * complex scaling: with r the centred lift of (t x_i mod q_i) over Q,
 //    round(t X / Q) = (t X - r) / Q, hence
 //    round(t X / Q) mod b_j = (t y_j - [r]_{b_j}) Q^-1 mod b_j;
@@ -133,9 +136,13 @@ __device__ __forceinline__ double u32_to_double(uint32_t x) {  // exact, FP64 pi
   return __hiloint2double(0x43300000, (int)x) - 4503599627370496.0;
 }
 
+// cuPoly's lift: X in [0, S) is read as X - S when X / S >= 1 - FPERROR (see
+// lift_threshold_digits in tables.cu); this is the fraction side of that test.
+constexpr double kLiftFrac = 1.0 - 1e-9;
+
 template <int NS>
 __device__ __forceinline__ bool fast_v(const uint64_t (&y)[NS], const uint64_t* __restrict__ invd, bool half, int& v,
-                                       bool& above) {
+                                       bool& above, bool lift = false, bool* neg = nullptr) {
   double f = 0.0;
 #pragma unroll
   for (int i = 0; i < NS; ++i) {  // y = yh 2^32 + yl, both halves exact in FP64
@@ -148,7 +155,8 @@ __device__ __forceinline__ bool fast_v(const uint64_t (&y)[NS], const uint64_t* 
   v = (int)fl;
   above = fr >= 0.5;
   const double d = 0x1p-36;
-  return fr > d && fr < 1.0 - d && (!half || fabs(fr - 0.5) > d);
+  if (lift) *neg = fr > kLiftFrac;
+  return fr > d && fr < 1.0 - d && (!half || fabs(fr - 0.5) > d) && (!lift || fabs(fr - kLiftFrac) > d);
 }
 
 // (sum_i y_i hmod_i + negv) mod m: lazy 192-bit sum (< 25 * 2^126), one reduction.
@@ -170,6 +178,7 @@ struct ConvArgs {
   const uint64_t* hor_s;
   const uint64_t* pm;  // mixed-radix weights [target][source]
   const uint64_t *W, *pinv, *pinv_s;  // Garner constants of the source base
+  const uint64_t* lift;               // MRC digits of the source base's lift threshold minus one
   int src_off, dst_off, ndst, N;
   long long in_stride, out_stride;  // per polynomial, in elements
 };
@@ -185,8 +194,13 @@ __device__ __noinline__ void ext_exact(uint64_t* ow, const uint64_t* iw, int j, 
     d[i] = iw[2 * ((size_t)i * a.N + j) + comp];
   }
   mrc_any<NS>(d, s, a.inv, a.inv_s, a.mc + a.src_off, a.W, a.pinv, a.pinv_s);
-  for (int t = 0; t < a.ndst; ++t)
-    ow[2 * ((size_t)t * a.N + j) + comp] = dot_mod<NS>(d, a.pm + t * NS, a.mc[a.dst_off + t]);
+  const bool neg = above_half<NS>(d, a.lift);  // cuPoly's lift: X - S
+  for (int t = 0; t < a.ndst; ++t) {
+    const ModConst mt = a.mc[a.dst_off + t];
+    uint64_t r = dot_mod<NS>(d, a.pm + t * NS, mt);
+    if (neg) r = add_mod(r, __ldg(a.f.negv + t * (NS + 1) + 1), mt.p);
+    ow[2 * ((size_t)t * a.N + j) + comp] = r;
+  }
 }
 
 // X mod m_j for every target j; one thread per Gaussian element (2 coefficients).
@@ -208,10 +222,15 @@ __global__ void __launch_bounds__(128) k_basis_ext(ulonglong2* __restrict__ out,
     }
     mrc_any<NS>(dr, s, a.inv, a.inv_s, a.mc + a.src_off, a.W, a.pinv, a.pinv_s);
     mrc_any<NS>(di, s, a.inv, a.inv_s, a.mc + a.src_off, a.W, a.pinv, a.pinv_s);
+    const bool nr = above_half<NS>(dr, a.lift), ni = above_half<NS>(di, a.lift);  // cuPoly's lift: X - S
     for (int t = 0; t < a.ndst; ++t) {
       const ModConst mt = a.mc[a.dst_off + t];
       const uint64_t* w = a.pm + t * NS;
-      out[blockIdx.y * a.out_stride + (size_t)t * a.N + j] = make_ulonglong2(dot_mod<NS>(dr, w, mt), dot_mod<NS>(di, w, mt));
+      const uint64_t ns = __ldg(a.f.negv + t * (NS + 1) + 1);  // -S mod m
+      uint64_t rr = dot_mod<NS>(dr, w, mt), ri = dot_mod<NS>(di, w, mt);
+      if (nr) rr = add_mod(rr, ns, mt.p);
+      if (ni) ri = add_mod(ri, ns, mt.p);
+      out[blockIdx.y * a.out_stride + (size_t)t * a.N + j] = make_ulonglong2(rr, ri);
     }
   } else if constexpr (NS < 8) {  // small bases: both coefficients together (ILP)
     uint64_t yr[NS], yi[NS];
@@ -223,10 +242,12 @@ __global__ void __launch_bounds__(128) k_basis_ext(ulonglong2* __restrict__ out,
       yi[i] = shoup_mul(x.y, h, hs, p);
     }
     int vr, vi;
-    bool ab;
-    const bool okr = fast_v<NS>(yr, a.f.invd, false, vr, ab);
-    const bool oki = fast_v<NS>(yi, a.f.invd, false, vi, ab);
+    bool ab, nr, ni;
+    const bool okr = fast_v<NS>(yr, a.f.invd, false, vr, ab, true, &nr);
+    const bool oki = fast_v<NS>(yi, a.f.invd, false, vi, ab, true, &ni);
     if (okr && oki) {
+      vr += nr ? 1 : 0;  // cuPoly's lift: X - S
+      vi += ni ? 1 : 0;
       for (int t = 0; t < a.ndst; ++t) {
         const ModConst mt = a.mc[a.dst_off + t];
         const uint64_t* hm = a.f.hmod + t * NS;
@@ -247,8 +268,9 @@ __global__ void __launch_bounds__(128) k_basis_ext(ulonglong2* __restrict__ out,
         y[i] = shoup_mul(iw[2 * ((size_t)i * a.N + j) + comp], __ldg(a.f.hinv + i), __ldg(a.f.hinv_s + i),
                          a.mc[a.src_off + i].p);
       int v;
-      bool above;
-      if (fast_v<NS>(y, a.f.invd, false, v, above)) {
+      bool above, neg;
+      if (fast_v<NS>(y, a.f.invd, false, v, above, true, &neg)) {
+        v += neg ? 1 : 0;  // cuPoly's lift: X - S
         for (int t = 0; t < a.ndst; ++t)
           ow[2 * ((size_t)t * a.N + j) + comp] =
               fast_dot<NS>(y, a.f.hmod + t * NS, __ldg(a.f.negv + t * (NS + 1) + v), a.mc[a.dst_off + t]);
@@ -491,6 +513,7 @@ int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int n
     a.pm = e.d_hps + e.ho.qb_pm;
     a.f = Fast{e.d_hps + e.ho.fq_hinv, e.d_hps + e.ho.fq_hinv_s, e.d_hps + e.ho.fq_hmod, e.d_hps + e.ho.fq_negv,
                e.d_hps + e.ho.fq_invd};
+    a.lift = e.d_hps + e.ho.q_lift;
     a.src_off = 0;
     a.dst_off = e.k;
     a.ndst = e.kl;
@@ -505,6 +528,7 @@ int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int n
     a.pm = e.d_hps + e.ho.bq_pm;
     a.f = Fast{e.d_hps + e.ho.fb_hinv, e.d_hps + e.ho.fb_hinv_s, e.d_hps + e.ho.fb_hmod, e.d_hps + e.ho.fb_negv,
                e.d_hps + e.ho.fb_invd};
+    a.lift = e.d_hps + e.ho.b_lift;
     a.src_off = e.k;
     a.dst_off = 0;
     a.ndst = e.k;

@@ -88,6 +88,42 @@ std::vector<uint64_t> mrc_digits(const std::vector<uint64_t>& r, const std::vect
   return d;
 }
 
+// Mixed-radix digits of T - 1 for the lift threshold T = S - floor(S F) of the
+// base s (S = prod s_i; F = 4835703278458517 / 2^82, the double nearest 1e-9,
+// cuPoly's FPERROR).  cuPoly lifts X in [0, S) to X - S exactly when its double
+// sum of X / S lands within FPERROR of 1 (src/cuda/cudaengine.cu:513-534,
+// 690-703), i.e. when S - X <= S F: X >= T.  The kernels test X > T - 1 on the
+// digits.
+std::vector<uint64_t> lift_threshold_digits(const std::vector<uint64_t>& s) {
+  std::vector<uint64_t> S{1};
+  auto mul_word = [](std::vector<uint64_t>& a, uint64_t w) {
+    unsigned __int128 carry = 0;
+    for (auto& x : a) {
+      const unsigned __int128 t = (unsigned __int128)x * w + carry;
+      x = (uint64_t)t;
+      carry = t >> 64;
+    }
+    if (carry) a.push_back((uint64_t)carry);
+  };
+  for (auto p : s) mul_word(S, p);
+  mul_word(S, 4835703278458517ull);  // S F 2^82
+  // U = floor(S F): shift right by 82 bits
+  std::vector<uint64_t> U;
+  const size_t w = 82 / 64, b = 82 % 64;
+  for (size_t i = w; i < S.size(); ++i) {
+    uint64_t v = S[i] >> b;
+    if (i + 1 < S.size()) v |= S[i + 1] << (64 - b);
+    U.push_back(v);
+  }
+  std::vector<uint64_t> r(s.size());
+  for (size_t i = 0; i < s.size(); ++i) {
+    unsigned __int128 acc = 0;  // U mod s_i, most significant limb first
+    for (size_t l = U.size(); l-- > 0;) acc = ((acc << 64) | U[l]) % s[i];
+    r[i] = s[i] - 1 - (uint64_t)acc;  // (T - 1) mod s_i = (-U - 1) mod s_i
+  }
+  return mrc_digits(r, s);
+}
+
 void parallel_for(int n, const std::function<void(int)>& f) {
   unsigned hw = std::thread::hardware_concurrency();
   int nt = (int)std::min<unsigned>(hw ? hw : 1, 16);
@@ -296,6 +332,8 @@ int build_tables(Engine& e) {
     std::vector<uint64_t> half(Q.size());
     for (size_t i = 0; i < Q.size(); ++i) half[i] = (Q[i] - 1) / 2;  // (Q-1)/2 mod q_i
     e.ho.qb_half = append(mrc_digits(half, Q));
+    e.ho.q_lift = append(lift_threshold_digits(Q));
+    e.ho.b_lift = append(lift_threshold_digits(B));
   }
   {
     std::vector<uint64_t> v, c;

@@ -35,11 +35,11 @@ def lib():
         L.oc_num_threads.restype = C.c_int
         L.oc_set_threads.argtypes = [C.c_int]
         L.oc_dgt.argtypes = [_u64p, C.c_int, C.c_int, C.c_int, _u64p, _u64p, _u64p, C.c_int]
-        L.oc_basis_ext.argtypes = [_u64p, _u64p, C.c_long, _u64p, C.c_int, _u64p, C.c_int]
+        L.oc_basis_ext.argtypes = [_u64p, _u64p, C.c_long, _u64p, C.c_int, _u64p, C.c_int, _u64p]
         L.oc_complex_scaling.argtypes = [_u64p, _u64p, _u64p, C.c_long, _u64p, C.c_int, _u64p, C.c_int, C.c_uint64]
         L.oc_simple_scaling.argtypes = [_u64p, _u64p, C.c_long, _u64p, C.c_int, C.c_uint64]
         L.oc_polymul.argtypes = [_u64p, _u64p, _u64p, C.c_int, C.c_int, C.c_int, _u64p, _u64p, _u64p]
-        L.oc_bfv_mul.argtypes = [_u64p] * 7 + [C.c_int] * 4 + [_u64p, _u64p, _u64p, C.c_uint64]
+        L.oc_bfv_mul.argtypes = [_u64p] * 7 + [C.c_int] * 4 + [_u64p, _u64p, _u64p, C.c_uint64, _u64p, _u64p]
         _L = L
     return _L
 
@@ -76,10 +76,11 @@ def polymul(a: np.ndarray, b: np.ndarray, primes) -> np.ndarray:
 
 
 def basis_ext(x: np.ndarray, src, dst) -> np.ndarray:
-    """x: (nsrc, count) residue rows -> (ndst, count) exact X mod d."""
+    """x: (nsrc, count) residue rows -> (ndst, count): X mod d with cuPoly's lift
+    (pyoracle.basis_extension_exact), decided exactly."""
     x = _arr(x)
     out = np.empty((len(dst), x.shape[1]), dtype=np.uint64)
-    lib().oc_basis_ext(out, x, x.shape[1], _arr(src), len(src), _arr(dst), len(dst))
+    lib().oc_basis_ext(out, x, x.shape[1], _arr(src), len(src), _arr(dst), len(dst), _arr(pyoracle.lift_digits(src)))
     return out
 
 
@@ -104,7 +105,7 @@ def bfv_mul(a0, a1, b0, b1, Q, B, t):
     primes = list(Q) + list(B)
     c0, c1, c2 = (np.empty_like(a0) for _ in range(3))
     lib().oc_bfv_mul(c0, c1, c2, a0, a1, b0, b1, npairs, k, len(B), nphi, _arr(primes), _gens(primes),
-                     _xis(primes, nphi // 2), t)
+                     _xis(primes, nphi // 2), t, _arr(pyoracle.lift_digits(Q)), _arr(pyoracle.lift_digits(B)))
     return c0, c1, c2
 
 

@@ -295,16 +295,37 @@ static uint64_t* mrc_inverses(const uint64_t* s, int n) {
   return inv;
 }
 
-/* out[j][c] = X_c mod dst_j for X_c = crt(in[.][c]) in [0, prod(src)); count coefficients per residue. */
+/* mixed-radix digits d > h, compared from the most significant */
+static int digits_gt(const uint64_t* d, const uint64_t* h, int n) {
+  for (int i = n - 1; i >= 0; --i)
+    if (d[i] != h[i]) return d[i] > h[i];
+  return 0;
+}
+static uint64_t prod_mod(const uint64_t* s, int n, uint64_t m) {
+  uint64_t r = 1 % m;
+  for (int i = 0; i < n; ++i) r = mulmod(r, s[i] % m, m);
+  return r;
+}
+/* X mod m with cuPoly's lift: X - S when X > lift (the digits of the threshold minus
+ * one, pyoracle.lift_digits) -- cuPoly's FPERROR rounding of the overflow count,
+ * src/cuda/cudaengine.cu:513-534, 690-703. */
+static uint64_t lifted(const uint64_t* d, const uint64_t* s, int n, uint64_t m, const uint64_t* lift) {
+  uint64_t r = horner(d, s, n, m);
+  if (lift && digits_gt(d, lift, n)) r = submod(r, prod_mod(s, n, m), m);
+  return r;
+}
+
+/* out[j][c] = lift(X_c) mod dst_j for X_c = crt(in[.][c]) in [0, prod(src)); count coefficients per
+ * residue; lift = digits of the lift threshold minus one (NULL: no lift). */
 void oc_basis_ext(uint64_t* out, const uint64_t* in, long count, const uint64_t* src, int ns, const uint64_t* dst,
-                  int nd) {
+                  int nd, const uint64_t* lift) {
   uint64_t* inv = mrc_inverses(src, ns);
 #pragma omp parallel for schedule(static)
   for (long c = 0; c < count; ++c) {
     uint64_t z[64], d[64];
     for (int i = 0; i < ns; ++i) z[i] = in[(size_t)i * count + c];
     mrc_digits(d, z, src, ns, inv);
-    for (int j = 0; j < nd; ++j) out[(size_t)j * count + c] = horner(d, src, ns, dst[j]);
+    for (int j = 0; j < nd; ++j) out[(size_t)j * count + c] = lifted(d, src, ns, dst[j], lift);
   }
   free(inv);
 }
@@ -406,11 +427,12 @@ void oc_polymul(uint64_t* c, const uint64_t* a, const uint64_t* b, int npolys, i
 
 /* BFV multiplication chain in the coefficient domain for npairs ciphertext
  * pairs: inputs a0, a1, b0, b1 as [npairs][k][nphi] rows mod Q; outputs
- * c0, c1, c2 as [npairs][k][nphi] = ((round(t/Q * tensor) mod B) mod q_i).
+ * c0, c1, c2 as [npairs][k][nphi] = ((round(t/Q * tensor) mod B) mod q_i), both base
+ * conversions with cuPoly's lift (lift_q, lift_b: threshold digits of Q and B).
  * primes = Q ++ B (k + kl), gens their primitive roots, xi[k + kl][2]. */
 void oc_bfv_mul(uint64_t* c0, uint64_t* c1, uint64_t* c2, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0,
                 const uint64_t* b1, int npairs, int k, int kl, int nphi, const uint64_t* primes, const uint64_t* gens,
-                const uint64_t* xi, uint64_t t) {
+                const uint64_t* xi, uint64_t t, const uint64_t* lift_q, const uint64_t* lift_b) {
   const int N = nphi / 2, nr = k + kl;
   const uint64_t* Q = primes;
   const uint64_t* B = primes + k;
@@ -430,7 +452,7 @@ void oc_bfv_mul(uint64_t* c0, uint64_t* c1, uint64_t* c2, const uint64_t* a0, co
         uint64_t z[64], d[64];
         for (int i = 0; i < k; ++i) z[i] = ins[v][(size_t)i * nphi + c];
         mrc_digits(d, z, Q, k, inv);
-        for (int j = 0; j < kl; ++j) ext[((size_t)v * nr + k + j) * nphi + c] = horner(d, Q, k, B[j]);
+        for (int j = 0; j < kl; ++j) ext[((size_t)v * nr + k + j) * nphi + c] = lifted(d, Q, k, B[j], lift_q);
       }
     }
     /* tensor product over every prime via the DGT */
@@ -479,7 +501,7 @@ void oc_bfv_mul(uint64_t* c0, uint64_t* c1, uint64_t* c2, const uint64_t* a0, co
         uint64_t z[64], d[64];
         for (int j = 0; j < kl; ++j) z[j] = ub[(size_t)j * nphi + c];
         mrc_digits(d, z, B, kl, invb);
-        for (int i = 0; i < k; ++i) outs[o][(size_t)i * nphi + c] = horner(d, B, kl, Q[i]);
+        for (int i = 0; i < k; ++i) outs[o][(size_t)i * nphi + c] = lifted(d, B, kl, Q[i], lift_b);
       }
     }
     free(ub); free(ten); free(ext);

@@ -36,6 +36,9 @@
 //   bfvmul  IN: a0, a1, b0, b1 over Q.  OUT: c0, c1, c2 over Q: the four
 //           extensions Q -> B, poly_dr2 over Q and over B, and one complex
 //           scaling per output.
+//   bfvtrace  IN as bfvmul.  OUT: the chain stage by stage: the four B
+//           extensions, the tensor over Q (3 polys) and over B (3 polys), the
+//           scaled B words of c0 (ctx->d_coefs_B) and c0.
 //   xirho   IN: a over Q.  OUT: poly_xi_bfv(a) (k polys over Q), then
 //           poly_rho_bfv(a) (k polys over Q).
 //   time    IN unused; t the iteration count is argv[5] as for the others.
@@ -268,6 +271,37 @@ int run_op(const std::string& op, int k, int kl, int nphi, uint64_t t, Context* 
     for (int o = 0; o < 3; ++o) download(ctx, &c[o], out);
     for (poly_t* p : {&a[0], &a[1], &a[2], &a[3], &aB[0], &aB[1], &aB[2], &aB[3], &tq[0], &tq[1], &tq[2], &tb[0],
                       &tb[1], &tb[2], &c[0], &c[1], &c[2]})
+      poly_free(ctx, p);
+  } else if (op == "bfvtrace") {
+    // The chain of bfvmul stage by stage (coefficient domain): the four extensions
+    // Q -> B, the tensor over Q and over B, then for c0 the scaled B residues cuPoly
+    // leaves in ctx->d_coefs_B ([kl][2N] words) and c0 itself.
+    const std::vector<uint64_t> in = read_u64(in_path);
+    need(in, 4 * qw, "bfvtrace");
+    poly_t a[4], aB[4], tq[3], tb[3], c0;
+    for (int v = 0; v < 4; ++v) upload(ctx, &a[v], QBase, in.data() + v * qw);
+    for (int v = 0; v < 4; ++v) {
+      poly_init(ctx, &aB[v], BBase);
+      poly_basis_extension_Q_to_B(ctx, &aB[v], &a[v]);
+      download(ctx, &aB[v], out);
+    }
+    for (int o = 0; o < 3; ++o) {
+      poly_init(ctx, &tq[o], QBase);
+      poly_init(ctx, &tb[o], BBase);
+    }
+    poly_dr2(ctx, &tq[0], &tq[1], &tq[2], &a[0], &a[1], &a[2], &a[3]);
+    poly_dr2(ctx, &tb[0], &tb[1], &tb[2], &aB[0], &aB[1], &aB[2], &aB[3]);
+    for (int o = 0; o < 3; ++o) download(ctx, &tq[o], out);
+    for (int o = 0; o < 3; ++o) download(ctx, &tb[o], out);
+    poly_init(ctx, &c0, QBase);
+    poly_complex_scaling_tDivQ(ctx, &c0, &tq[0], &tb[0]);
+    check(cudaStreamSynchronize(ctx->get_stream()), "complex scaling");
+    const size_t o0 = out.size();
+    out.resize(o0 + bw);
+    check(cudaMemcpy(out.data() + o0, ctx->d_coefs_B, bw * 8, cudaMemcpyDeviceToHost), "d_coefs_B");
+    download(ctx, &c0, out);
+    for (poly_t* p : {&a[0], &a[1], &a[2], &a[3], &aB[0], &aB[1], &aB[2], &aB[3], &tq[0], &tq[1], &tq[2], &tb[0],
+                      &tb[1], &tb[2], &c0})
       poly_free(ctx, p);
   } else if (op == "xirho") {
     const std::vector<uint64_t> in = read_u64(in_path);

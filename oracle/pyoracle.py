@@ -368,14 +368,35 @@ def crt(residues, primes):
     return x % M
 
 
+# cuPoly's FPERROR (``include/cuPoly/settings.h:105``) as the exact value of the double 1e-9.
+FPERROR_NUM, FPERROR_DEN = (1e-9).as_integer_ratio()
+
+
+def lift_threshold(S: int) -> int:
+    """T = S - floor(S FPERROR): cuPoly's base conversions read X in [T, S) as X - S.
+
+    cuPoly's overflow count v is floor(sum_i y_i / s_i) unless that double lies
+    within FPERROR of an integer, where it is rounded instead
+    (``src/cuda/cudaengine.cu:513-534, 690-703``); with sum = v + X / S, v rounds
+    up exactly when 1 - X / S <= FPERROR, i.e. S - X <= S FPERROR."""
+    return S - S * FPERROR_NUM // FPERROR_DEN
+
+
+def cupoly_lift(X: int, S: int) -> int:
+    """The integer cuPoly's base conversion takes for X in [0, S): X, or X - S at or above
+    the threshold (small negative values, as the scaled BFV tensor produces)."""
+    return X - S if X >= lift_threshold(S) else X
+
+
 def basis_extension_exact(xs, src, dst):
-    """X mod d_j for X = crt(xs, src) in [0, prod(src)).
+    """cupoly_lift(X) mod d_j for X = crt(xs, src) in [0, prod(src)), decided exactly.
 
     cuPoly computes this with a floating-point correction v
-    (``src/cuda/cudaengine.cu:483-649, 659-796``); its tests assert the exact
-    value (``tests/unit_tests/test_bfv_mode.cu:640-730``).
+    (``src/cuda/cudaengine.cu:483-649, 659-796``); its tests assert X mod d_j on
+    random X (``tests/unit_tests/test_bfv_mode.cu:640-730``), where the two agree.
     """
-    X = crt(xs, src)
+    S = prod(src)
+    X = cupoly_lift(crt(xs, src), S)
     return [X % d for d in dst]
 
 
@@ -392,11 +413,22 @@ def complex_scaling_exact(xq, yb, Q, B, t):
 
 
 def complex_scaling_tdivq_exact(xq, yb, Q, B, t):
-    """((round(t X / Q) mod B) mod q_i): ``poly_complex_scaling_tDivQ`` (``polynomial.cu:350-404``)."""
+    """``poly_complex_scaling_tDivQ`` (``polynomial.cu:350-404``): Y = round(t X / Q) mod B,
+    then its B -> Q conversion with cuPoly's lift (``basis_extension_exact``)."""
     Qp, Bp = prod(Q), prod(B)
     X = crt(list(xq) + list(yb), list(Q) + list(B))
-    r = (2 * t * X + Qp) // (2 * Qp) % Bp
+    r = cupoly_lift((2 * t * X + Qp) // (2 * Qp) % Bp, Bp)
     return [r % q for q in Q]
+
+
+def lift_digits(src):
+    """Mixed-radix digits of lift_threshold(prod(src)) - 1 over src (for the C oracle)."""
+    T1 = lift_threshold(prod(src)) - 1
+    d, rest, base = [], T1, 1
+    for s in src:  # X = sum_i d_i prod_{l<i} s_l
+        d.append((rest // base) % s)
+        base *= s
+    return d
 
 
 def simple_scaling_exact(xq, Q, t):
@@ -585,18 +617,26 @@ def cupoly_float_complex_scaling_tdivq(xq, yb, Q, B, t):
     return cupoly_float_ext_b_to_q(cupoly_float_complex_scaling(xq, yb, Q, B, t), Q, B)
 
 
-def cupoly_float_simple_scaling(xq, Q, t):
+def cupoly_float_simple_scaling(xq, Q, t, raw=False):
     """cuPoly's simple_scaling for one coefficient, t a power of two (``cudaengine.cu:323-362``,
-    tomega from ``:1494-1509``): integer parts masked mod t, fraction parts summed in double."""
+    tomega from ``:1494-1509``): integer parts and fraction parts of x tomega summed, the
+    fraction parts' low words in double and added back by llrint.
+
+    The kernel masks with its constant d_RNST - 1, but nothing ever writes d_RNST
+    (declared at ``cudaengine.cu:93``; no cudaMemcpyToSymbol of it in the precompute,
+    ``:1337-1673``), so the mask is 2^64 - 1 and the device word is the sum mod 2^64
+    (``raw=True``).  Reduced mod t -- as cuPoly's download does for TBase,
+    ``polynomial.cu:289`` -- it is the value the kernel intends (the default)."""
     assert t > 0 and t & (t - 1) == 0
     result, acc = 0, 0.0
     for x, (ti, frac) in zip(xq, _cupoly_tomega(tuple(Q), t)):
-        vint = (x * ti) & _U64 & (t - 1)
+        vint = (x * ti) & _U64
         c = (frac * x) >> 64
         hi, lo = c >> 64, c & _U64
         acc = acc + float(lo) * 2.0 ** -64
-        result = (result + ((vint + (hi & (t - 1))) & (t - 1))) & _U64
-    return (result + round(acc)) & (t - 1)
+        result = (result + ((vint + hi) & _U64)) & _U64
+    word = (result + round(acc)) & _U64
+    return word if raw else word & (t - 1)
 
 
 # ----------------------------------------------------------------------------

@@ -40,16 +40,24 @@ def test_basis_extension_exact(gpu, k, kl, nphi):
     assert np.array_equal(unfold(_host(outq))[0], CO.basis_ext(yb, e.B, e.Q))
 
 
-def test_basis_extension_edges(gpu):
-    """X = 0, 1, Q-1, (Q-1)/2: exact lift (cuPoly's float v maps X near Q to X - Q)."""
+@pytest.mark.parametrize("k", [3, 7, 10])
+def test_basis_extension_edges(gpu, k):
+    """cuPoly's lift on both sides of its threshold T = Q - floor(Q FPERROR): X below T
+    converts as X, X from T up as X - Q (cuPoly's v rounds up within FPERROR of an
+    integer, src/cuda/cudaengine.cu:513-534), in the digit path (k < 7) and the fast
+    path with its exact fallback (k >= 7); also B -> Q."""
     from cupoly_b200.engine import Engine
-    e = Engine(3, 0, 32, 256)
-    Qp = O.prod(e.Q)
-    vals = [0, 1, Qp - 1, (Qp - 1) // 2, (Qp + 1) // 2, 12345] + [Qp - 1 - i for i in range(26)]
-    xq = np.array([[v % q for v in vals] for q in e.Q], dtype=np.uint64)
-    out = e.empty(1)
-    e.basis_ext_q_to_b(out, _dev(fold(xq)[None]))
-    assert unfold(_host(out))[0].tolist() == [[v % b for v in vals] for b in e.B]
+    e = Engine(k, 0, 64, 256)
+    for src, dst, fwd in ((e.Q, e.B, True), (e.B, e.Q, False)):
+        S = O.prod(src)
+        T = O.lift_threshold(S)
+        vals = [0, 1, S - 1, (S - 1) // 2, (S + 1) // 2, 12345, T - 1, T, T + 1, T - 2, S - 2]
+        vals += [T + (S - T) * i // 26 for i in range(26)] + [T - 1 - (i << 40) for i in range(17)]
+        xs = np.array([[v % q for v in vals] for q in src], dtype=np.uint64)
+        out = e.empty(1 if fwd else 0)
+        (e.basis_ext_q_to_b if fwd else e.basis_ext_b_to_q)(out, _dev(fold(xs)[None]))
+        want = [[O.cupoly_lift(v, S) % m for v in vals] for m in dst]
+        assert unfold(_host(out))[0].tolist() == want
 
 
 @pytest.mark.parametrize("k,nphi,t", [(1, 32, 256), (2, 2048, 256), (5, 8192, 256), (3, 4096, 65537),
@@ -263,10 +271,11 @@ def test_scaling_exact_fallback_edges(gpu, k):
 @pytest.mark.parametrize("k,t", [(2, 256), (5, 256), (5, 65536)])
 def test_device_matches_cupolys_float_path_where_it_is_exact(gpu, k, t):
     """Against a word-for-word restatement of cuPoly's double-precision HPS kernels
-    (oracle/pyoracle.py cupoly_float_*): on random coefficients the device's Q -> B,
-    B -> Q, complex and simple scaling agree with cuPoly's path everywhere; at X = Q - 1
-    and next to the half-integer rounding boundary, the only places cuPoly's path
-    differs from the exact value, the device gives the exact one."""
+    (oracle/pyoracle.py cupoly_float_*): on random coefficients and at X = Q - 1, Q - 2
+    (above the lift threshold) the device's Q -> B, B -> Q, complex and simple scaling
+    agree with cuPoly's path everywhere; next to the half-integer rounding boundary,
+    the only place cuPoly's path differs from the exact value, the device gives the
+    exact one."""
     from cupoly_b200.engine import Engine
     nphi = 512
     e = Engine(k, 0, nphi, t)
@@ -303,10 +312,9 @@ def test_device_matches_cupolys_float_path_where_it_is_exact(gpu, k, t):
             diff["complex"].append(c)
         if t & (t - 1) == 0 and int(ot[c]) != O.cupoly_float_simple_scaling(xs, Q, t):
             diff["simple"].append(c)
-    # cuPoly misreads X = Q - 1 (and Q - 2) as negative; the device is exact there
-    assert set(diff["q_to_b"]) <= {0, 1} and 0 in diff["q_to_b"]
-    assert [int(v) for v in ob[:, 0]] == [(Qp - 1) % b for b in B]
-    assert set(diff["b_to_q"]) <= {0, 1}
+    # X = Q - 1 and Q - 2 lie above cuPoly's lift threshold: both read them as X - Q
+    assert diff["q_to_b"] == [] and diff["b_to_q"] == []
+    assert [int(v) for v in ob[:, 0]] == [(Qp - 1 - Qp) % b for b in B]
     # scaling: disagreements only at the engineered half-integer edges, where the device is exact
     assert set(diff["complex"]) <= edge_c
     for c in diff["complex"]:

@@ -102,12 +102,20 @@ def test_golden_hps_c_oracle():
 
 
 def test_basis_extension_edges():
-    """Exact lift of X in [0, Q): 0, 1, Q-1 and (Q-1)/2 (cuPoly's float v misreads X near Q)."""
-    Q, B = O.bases(3, 4)
-    Qp = O.prod(Q)
-    for X in [0, 1, Qp - 1, (Qp - 1) // 2, (Qp + 1) // 2]:
-        xs = np.array([[X % q] for q in Q], dtype=np.uint64)
-        assert CO.basis_ext(xs, Q, B)[:, 0].tolist() == [X % b for b in B]
+    """cuPoly's lift, decided exactly: X in [0, Q) reads as X - Q from the threshold
+    T = Q - floor(Q FPERROR) on (cuPoly rounds its overflow count up within FPERROR of
+    an integer, src/cuda/cudaengine.cu:513-534), as X below it; the C and Python
+    restatements agree on both sides of T."""
+    for k in (1, 3, 6):
+        Q, B = O.bases(k, k + 1)
+        Qp = O.prod(Q)
+        T = O.lift_threshold(Qp)
+        assert Qp - T == Qp * O.FPERROR_NUM // O.FPERROR_DEN
+        for X in [0, 1, (Qp - 1) // 2, (Qp + 1) // 2, T - 2, T - 1, T, T + 1, Qp - 2, Qp - 1]:
+            want = [(X - Qp if X >= T else X) % b for b in B]
+            xs = np.array([[X % q] for q in Q], dtype=np.uint64)
+            assert CO.basis_ext(xs, Q, B)[:, 0].tolist() == want
+            assert O.basis_extension_exact([X % q for q in Q], Q, B) == want
 
 
 def test_scaling_rounding_edges():
@@ -157,7 +165,7 @@ def test_c_bfv_mul_matches_bigint_definition():
     for T, cc in zip(tens, c):
         for j in range(nphi):
             X = T[j] % (Qp * Bp)
-            r = (2 * t * X + Qp) // (2 * Qp) % Bp
+            r = O.cupoly_lift((2 * t * X + Qp) // (2 * Qp) % Bp, Bp)  # small negatives stay negative
             assert [r % q for q in Q] == cc[0][:, j].tolist()
 
 
@@ -261,10 +269,10 @@ def test_cupoly_complex_scaling_constants_break_beyond_512_bits():
 
 
 def test_cupoly_float_path_is_off_at_its_edges():
-    """Where cuPoly's float path is wrong: X = Q - 1 reads as X - Q (v rounded up within
-    FPERROR), and t X / Q within 1/Q of a half-integer rounds the wrong way about half
-    the time -- each time by exactly one.  The exact definitions used here and on the
-    device are right at both."""
+    """cuPoly's float path reads X = Q - 1 as X - Q (v rounded up within FPERROR) -- the
+    lift the exact definitions follow too -- and rounds t X / Q within 1/Q of a
+    half-integer the wrong way about half the time, each time by exactly one; the
+    exact definitions used here and on the device are right there."""
     import random
     rng = random.Random(7)
     for k in (1, 3, 5):
@@ -272,7 +280,7 @@ def test_cupoly_float_path_is_off_at_its_edges():
         Qp, Bp = O.prod(Q), O.prod(B)
         xs = [(Qp - 1) % q for q in Q]
         assert O.cupoly_float_ext_q_to_b(xs, Q, B) == [(Qp - 1 - Qp) % b for b in B]
-        assert O.basis_extension_exact(xs, Q, B) == [(Qp - 1) % b for b in B]
+        assert O.basis_extension_exact(xs, Q, B) == [(Qp - 1 - Qp) % b for b in B]
         ti, wrong = pow(256, -1, Qp), 0
         for h in ((Qp - 1) // 2, (Qp + 1) // 2, (Qp - 3) // 2, (Qp + 3) // 2):
             for _ in range(3):
