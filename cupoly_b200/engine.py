@@ -134,7 +134,8 @@ class Engine:
         self.primes: List[int] = [int(x) for x in buf]
         self.Q = self.primes[: self.k]
         self.B = self.primes[self.k:]
-        self._ws: Optional[torch.Tensor] = None
+        self._wsbuf: Optional[torch.Tensor] = None
+        self.device = torch.cuda.current_device()
 
     # ---- DGT plan ----
     def set_plan(self, log_radix: int, log_cta: int = 0):
@@ -185,6 +186,37 @@ class Engine:
     def base_primes(self, base: int) -> List[int]:
         return {QBase: self.Q, BBase: self.B, QBBase: self.primes, TBase: [self.t]}[base]
 
+    # ---- argument checks (every device buffer is checked before its pointer crosses the C ABI) ----
+    def _buf(self, t, base: int, npolys: int = 1, name: str = "buffer", words: int = 2):
+        """Pointer of t after checking that it is a contiguous int64 tensor on this engine's
+        device holding at least npolys polynomials over base (`words` 64-bit words per
+        element: 2 for Gaussian residues, 1 for cp_mul_u64's multipliers)."""
+        if not isinstance(t, torch.Tensor):
+            raise TypeError("%s must be a torch tensor" % name)
+        if t.dtype != torch.int64 or not t.is_cuda or not t.is_contiguous():
+            raise ValueError("%s must be a contiguous int64 CUDA tensor" % name)
+        if t.device.index != self.device:
+            raise ValueError("%s is on cuda:%s, the engine on cuda:%d" % (name, t.device.index, self.device))
+        need = int(npolys) * self.n_residues(base) * self.N * words
+        if npolys < 1 or t.numel() < need:
+            raise ValueError("%s holds %d words, %d polynomials over base %d need %d"
+                             % (name, t.numel(), npolys, base, need))
+        return C.c_void_p(t.data_ptr())
+
+    def _bufs(self, base: int, npolys: int = 1, **bufs):
+        """_buf of each keyword argument, in order."""
+        return [self._buf(t, base, npolys, name) for name, t in bufs.items()]
+
+    def _ws(self, t, nbytes: int, name: str = "workspace"):
+        """Pointer of a device workspace after checking it holds nbytes bytes."""
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or not t.is_contiguous():
+            raise ValueError("%s must be a contiguous CUDA tensor" % name)
+        if t.device.index != self.device:
+            raise ValueError("%s is on cuda:%s, the engine on cuda:%d" % (name, t.device.index, self.device))
+        if t.numel() * t.element_size() < nbytes:
+            raise ValueError("%s holds %d bytes, the call needs %d" % (name, t.numel() * t.element_size(), nbytes))
+        return C.c_void_p(t.data_ptr())
+
     # ---- memory ----
     def empty(self, base: int = QBase, npolys: int = 1) -> torch.Tensor:
         return torch.empty((npolys, self.n_residues(base), self.N, 2), dtype=torch.int64, device="cuda")
@@ -193,10 +225,10 @@ class Engine:
         return torch.zeros((npolys, self.n_residues(base), self.N, 2), dtype=torch.int64, device="cuda")
 
     def workspace(self) -> torch.Tensor:
-        if self._ws is None:
+        if self._wsbuf is None:
             n = _lib.lib().cp_workspace_bytes(self._h)
-            self._ws = torch.empty(((n + 15) // 16, 2), dtype=torch.int64, device="cuda")
-        return self._ws
+            self._wsbuf = torch.empty(((n + 15) // 16, 2), dtype=torch.int64, device="cuda")
+        return self._wsbuf
 
     # ---- roots ----
     def set_nthroot(self, xi: Sequence[Sequence[int]]):
@@ -219,22 +251,22 @@ class Engine:
     # ---- DGT ----
     def dgt(self, x: torch.Tensor, base: int, direction: int, npolys: Optional[int] = None, stream=None):
         n = x.shape[0] if npolys is None else npolys
-        call("cp_dgt", self._h, _ptr(x), base, direction, n, 0, _stream(stream))
+        call("cp_dgt", self._h, self._buf(x, base, n, "x"), base, direction, n, 0, _stream(stream))
         return x
 
     # ---- pointwise ----
     def add(self, c, a, b, base, stream=None):
-        call("cp_add", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
+        call("cp_add", self._h, *self._bufs(base, c=c, a=a, b=b), base, _stream(stream))
 
     def sub(self, c, a, b, base, stream=None):
-        call("cp_sub", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
+        call("cp_sub", self._h, *self._bufs(base, c=c, a=a, b=b), base, _stream(stream))
 
     def double_add(self, c1, a1, b1, c2, a2, b2, base, stream=None):
-        call("cp_double_add", self._h, _ptr(c1), _ptr(a1), _ptr(b1), _ptr(c2), _ptr(a2), _ptr(b2), base,
+        call("cp_double_add", self._h, *self._bufs(base, c1=c1, a1=a1, b1=b1, c2=c2, a2=a2, b2=b2), base,
              _stream(stream))
 
     def mul(self, c, a, b, base, stream=None):
-        call("cp_mul", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
+        call("cp_mul", self._h, *self._bufs(base, c=c, a=a, b=b), base, _stream(stream))
 
     def polymul_workspace(self, base: int, npolys: int) -> torch.Tensor:
         n = _lib.lib().cp_polymul_workspace_bytes(self._h, base, npolys)
@@ -243,17 +275,19 @@ class Engine:
     def polymul(self, c, a, b, base, workspace, npolys=None, stream=None):
         """c = a b mod (x^nphi + 1) per residue, coefficient domain in and out (fused: 3 launches)."""
         n = c.shape[0] if npolys is None else npolys
-        call("cp_polymul", self._h, _ptr(c), _ptr(a), _ptr(b), base, n, _ptr(workspace), _stream(stream))
+        ws = self._ws(workspace, _lib.lib().cp_polymul_workspace_bytes(self._h, base, n))
+        call("cp_polymul", self._h, *self._bufs(base, n, c=c, a=a, b=b), base, n, ws, _stream(stream))
 
     def mul_batch(self, c, a, b, base, npolys=None, stream=None):
         n = c.shape[0] if npolys is None else npolys
-        call("cp_mul_batch", self._h, _ptr(c), _ptr(a), _ptr(b), base, n, _stream(stream))
+        call("cp_mul_batch", self._h, *self._bufs(base, n, c=c, a=a, b=b), base, n, _stream(stream))
 
     def mul_u64(self, c, a, b, base, stream=None):
-        call("cp_mul_u64", self._h, _ptr(c), _ptr(a), _ptr(b), base, _stream(stream))
+        call("cp_mul_u64", self._h, *self._bufs(base, c=c, a=a), self._buf(b, base, 1, "b", words=1), base,
+             _stream(stream))
 
     def muladd(self, d, a, b, c, base, stream=None):
-        call("cp_muladd", self._h, _ptr(d), _ptr(a), _ptr(b), _ptr(c), base, _stream(stream))
+        call("cp_muladd", self._h, *self._bufs(base, d=d, a=a, b=b, c=c), base, _stream(stream))
 
     def dot(self, c, a, b, base, stream=None):
         """c = sum_i a[i] b[i] in the DGT domain, one pass (cuPoly's poly_dot).
@@ -263,28 +297,30 @@ class Engine:
         if len(a) != len(b) or not a:
             raise ValueError("dot: a and b must be non-empty and of equal length")
         n = len(a)
-        pa = (C.c_void_p * n)(*[_ptr(x) for x in a])
-        pb = (C.c_void_p * n)(*[_ptr(x) for x in b])
-        call("cp_dot", self._h, _ptr(c), pa, pb, n, base, _stream(stream))
+        pa = (C.c_void_p * n)(*[self._buf(x, base, 1, "a[%d]" % i) for i, x in enumerate(a)])
+        pb = (C.c_void_p * n)(*[self._buf(x, base, 1, "b[%d]" % i) for i, x in enumerate(b)])
+        call("cp_dot", self._h, self._buf(c, base, 1, "c"), pa, pb, n, base, _stream(stream))
 
     def dot_batch(self, c, a, b, n, npolys, base, b_shared=False, stream=None):
         """Polynomial q of c = sum_{t<n} a[q n + t] b[q n + t] (b[t] when b_shared), one launch."""
-        call("cp_dot_batch", self._h, _ptr(c), _ptr(a), _ptr(b), n, npolys, 1 if b_shared else 0, base,
-             _stream(stream))
+        pc = self._buf(c, base, npolys, "c")
+        pa = self._buf(a, base, n * npolys, "a")
+        pb = self._buf(b, base, n if b_shared else n * npolys, "b")
+        call("cp_dot_batch", self._h, pc, pa, pb, n, npolys, 1 if b_shared else 0, base, _stream(stream))
 
     def dr2(self, c21, c22, c23, c01, c02, c11, c12, base, stream=None):
-        call("cp_dr2", self._h, _ptr(c21), _ptr(c22), _ptr(c23), _ptr(c01), _ptr(c02), _ptr(c11), _ptr(c12),
+        call("cp_dr2", self._h, *self._bufs(base, c21=c21, c22=c22, c23=c23, c01=c01, c02=c02, c11=c11, c12=c12),
              base, _stream(stream))
 
     def negate(self, b, a, base, stream=None):
-        call("cp_negate", self._h, _ptr(b), _ptr(a), base, _stream(stream))
+        call("cp_negate", self._h, *self._bufs(base, b=b, a=a), base, _stream(stream))
 
     def op_by_int(self, b, a, base, x, op, stream=None):
-        call("cp_op_by_int", self._h, _ptr(b), _ptr(a), base, int(x), op, _stream(stream))
+        call("cp_op_by_int", self._h, *self._bufs(base, b=b, a=a), base, int(x), op, _stream(stream))
 
     def double_op_by_int(self, b1, a1, b2, a2, base, x1, x2, op, stream=None):
-        call("cp_double_op_by_int", self._h, _ptr(b1), _ptr(a1), _ptr(b2), _ptr(a2), base, int(x1), int(x2), op,
-             _stream(stream))
+        call("cp_double_op_by_int", self._h, *self._bufs(base, b1=b1, a1=a1, b2=b2, a2=a2), base, int(x1), int(x2),
+             op, _stream(stream))
 
     # ---- CKKS (CKKS engines) ----
     @classmethod
@@ -292,15 +328,16 @@ class Engine:
         return cls(k, kl, nphi, 2, log_radix, ckks_prec=prec)
 
     def ckks_modulus_raising(self, out_qb, in_q, level: int, stream=None):
-        call("cp_ckks_modulus_raising", self._h, _ptr(out_qb), _ptr(in_q), level, _ptr(self.workspace()),
-             _stream(stream))
+        call("cp_ckks_modulus_raising", self._h, self._buf(out_qb, QBBase, 1, "out_qb"), self._buf(in_q, QBase, 1, "in_q"),
+             level, _ptr(self.workspace()), _stream(stream))
 
     def ckks_modulus_reduction(self, out_q, in_qb, level: int, stream=None):
-        call("cp_ckks_modulus_reduction", self._h, _ptr(out_q), _ptr(in_qb), level, _ptr(self.workspace()),
-             _stream(stream))
+        call("cp_ckks_modulus_reduction", self._h, self._buf(out_q, QBase, 1, "out_q"),
+             self._buf(in_qb, QBBase, 1, "in_qb"), level, _ptr(self.workspace()), _stream(stream))
 
     def ckks_rescale(self, a, b, level: int, stream=None):
-        call("cp_ckks_rescale", self._h, _ptr(a), _ptr(b), level, _stream(stream))
+        pb = self._buf(b, QBase, 1, "b") if b is not None else _ptr(None)
+        call("cp_ckks_rescale", self._h, self._buf(a, QBase, 1, "a"), pb, level, _stream(stream))
 
     def ckks_batch_workspace(self, npolys: int) -> torch.Tensor:
         n = int(_lib.lib().cp_ckks_batch_workspace_bytes(self._h, npolys))
@@ -308,36 +345,43 @@ class Engine:
 
     def ckks_modulus_raising_batch(self, out_qb, in_q, level: int, workspace, npolys=None, stream=None):
         n = in_q.shape[0] if npolys is None else npolys
-        call("cp_ckks_modulus_raising_batch", self._h, _ptr(out_qb), _ptr(in_q), level, n, _ptr(workspace),
-             _stream(stream))
+        ws = self._ws(workspace, _lib.lib().cp_ckks_batch_workspace_bytes(self._h, n))
+        call("cp_ckks_modulus_raising_batch", self._h, self._buf(out_qb, QBBase, n, "out_qb"),
+             self._buf(in_q, QBase, n, "in_q"), level, n, ws, _stream(stream))
 
     def ckks_modulus_reduction_batch(self, out_q, in_qb, level: int, workspace, npolys=None, stream=None):
         n = in_qb.shape[0] if npolys is None else npolys
-        call("cp_ckks_modulus_reduction_batch", self._h, _ptr(out_q), _ptr(in_qb), level, n, _ptr(workspace),
-             _stream(stream))
+        ws = self._ws(workspace, _lib.lib().cp_ckks_batch_workspace_bytes(self._h, n))
+        call("cp_ckks_modulus_reduction_batch", self._h, self._buf(out_q, QBase, n, "out_q"),
+             self._buf(in_qb, QBBase, n, "in_qb"), level, n, ws, _stream(stream))
 
     def ckks_rescale_batch(self, x, level: int, npolys=None, stream=None):
         n = x.shape[0] if npolys is None else npolys
-        call("cp_ckks_rescale_batch", self._h, _ptr(x), n, level, _stream(stream))
+        call("cp_ckks_rescale_batch", self._h, self._buf(x, QBase, n, "x"), n, level, _stream(stream))
 
     def ckks_xi(self, out, a, stream=None):
-        call("cp_ckks_xi", self._h, _ptr(out), _ptr(a), _stream(stream))
+        call("cp_ckks_xi", self._h, *self._bufs(QBase, out=out, a=a), _stream(stream))
 
     def ckks_rho(self, out, a, stream=None):
-        call("cp_ckks_rho", self._h, _ptr(out), _ptr(a), _stream(stream))
+        call("cp_ckks_rho", self._h, *self._bufs(QBase, out=out, a=a), _stream(stream))
 
     # ---- coefficient I/O (big integers <-> residues, on the device) ----
     def crt(self, out, coefs_limbs: torch.Tensor, base: int = QBase, stream=None):
         """Residues of big-integer coefficients: coefs_limbs is (npolys, nphi, nlimbs) int64 (uint64 limbs)."""
         npolys, nphi, nlimbs = coefs_limbs.shape
-        assert nphi == self.nphi
-        call("cp_crt", self._h, _ptr(out), _ptr(coefs_limbs), nlimbs, base, npolys, _stream(stream))
+        if nphi != self.nphi or coefs_limbs.dtype != torch.int64 or not coefs_limbs.is_contiguous():
+            raise ValueError("crt: coefs_limbs must be a contiguous int64 (npolys, nphi, nlimbs) tensor")
+        call("cp_crt", self._h, self._buf(out, base, npolys, "out"), _ptr(coefs_limbs), nlimbs, base, npolys,
+             _stream(stream))
         return out
 
     def icrt(self, coefs_limbs: torch.Tensor, x, base: int = QBase, stream=None):
         """Big-integer coefficients in [0, prod of the base) from coefficient-domain residues."""
         npolys, nphi, nlimbs = coefs_limbs.shape
-        call("cp_icrt", self._h, _ptr(coefs_limbs), nlimbs, _ptr(x), base, npolys, _stream(stream))
+        if nphi != self.nphi or coefs_limbs.dtype != torch.int64 or not coefs_limbs.is_contiguous():
+            raise ValueError("icrt: coefs_limbs must be a contiguous int64 (npolys, nphi, nlimbs) tensor")
+        call("cp_icrt", self._h, _ptr(coefs_limbs), nlimbs, self._buf(x, base, npolys, "x"), base, npolys,
+             _stream(stream))
         return coefs_limbs
 
     def wire_bytes(self, base: int, npolys: int = 1) -> int:
@@ -351,11 +395,12 @@ class Engine:
         if out is not None:
             if out.dtype != np.uint8 or out.size < n or not out.flags["C_CONTIGUOUS"]:
                 raise ValueError("export_residues: out must be a contiguous uint8 array of wire_bytes")
-            call("cp_export_residues", self._h, C.c_void_p(out.ctypes.data), out.size, _ptr(x), base, x.shape[0],
-                 domain, _stream(stream))
+            call("cp_export_residues", self._h, C.c_void_p(out.ctypes.data), out.size,
+                 self._buf(x, base, x.shape[0], "x"), base, x.shape[0], domain, _stream(stream))
             return out
         buf = C.create_string_buffer(n)
-        call("cp_export_residues", self._h, buf, n, _ptr(x), base, x.shape[0], domain, _stream(stream))
+        call("cp_export_residues", self._h, buf, n, self._buf(x, base, x.shape[0], "x"), base, x.shape[0], domain,
+             _stream(stream))
         return buf.raw
 
     def import_residues(self, x, data, base: int, stream=None) -> int:
@@ -366,60 +411,68 @@ class Engine:
             src, size = C.c_void_p(np.ascontiguousarray(data).ctypes.data), data.size
         else:
             src, size = data, len(data)
-        call("cp_import_residues", self._h, _ptr(x), src, size, base, x.shape[0], C.byref(dom), _stream(stream))
+        call("cp_import_residues", self._h, self._buf(x, base, x.shape[0], "x"), src, size, base, x.shape[0],
+             C.byref(dom), _stream(stream))
         return dom.value
 
     # ---- HPS (coefficient domain) ----
     def basis_ext_q_to_b(self, out_b, in_q, npolys=1, stream=None):
-        call("cp_basis_ext_q_to_b", self._h, _ptr(out_b), _ptr(in_q), npolys, _stream(stream))
+        call("cp_basis_ext_q_to_b", self._h, self._buf(out_b, BBase, npolys, "out_b"),
+             self._buf(in_q, QBase, npolys, "in_q"), npolys, _stream(stream))
 
     def basis_ext_b_to_q(self, out_q, in_b, npolys=1, stream=None):
-        call("cp_basis_ext_b_to_q", self._h, _ptr(out_q), _ptr(in_b), npolys, _stream(stream))
+        call("cp_basis_ext_b_to_q", self._h, self._buf(out_q, QBase, npolys, "out_q"),
+             self._buf(in_b, BBase, npolys, "in_b"), npolys, _stream(stream))
 
     def complex_scaling(self, out_b, in_q, in_b, npolys=1, stream=None):
-        call("cp_complex_scaling", self._h, _ptr(out_b), _ptr(in_q), _ptr(in_b), npolys, _stream(stream))
+        call("cp_complex_scaling", self._h, self._buf(out_b, BBase, npolys, "out_b"),
+             self._buf(in_q, QBase, npolys, "in_q"), self._buf(in_b, BBase, npolys, "in_b"), npolys, _stream(stream))
 
     def simple_scaling(self, out_t, in_q, stream=None):
-        call("cp_simple_scaling", self._h, _ptr(out_t), _ptr(in_q), _stream(stream))
+        call("cp_simple_scaling", self._h, self._buf(out_t, TBase, 1, "out_t"), self._buf(in_q, QBase, 1, "in_q"),
+             _stream(stream))
 
     def xi(self, out, a, stream=None):
-        call("cp_xi", self._h, _ptr(out), _ptr(a), _stream(stream))
+        call("cp_xi", self._h, self._buf(out, QBase, self.k, "out"), self._buf(a, QBase, 1, "a"), _stream(stream))
 
     def xi_batch(self, out, a, npolys=None, stream=None):
         """out (npolys * k, k, N, 2): the xi decomposition of each of the npolys polynomials of a."""
         n = a.shape[0] if npolys is None else npolys
-        call("cp_xi_batch", self._h, _ptr(out), _ptr(a), n, _stream(stream))
+        call("cp_xi_batch", self._h, self._buf(out, QBase, n * self.k, "out"), self._buf(a, QBase, n, "a"), n,
+             _stream(stream))
 
     def rho_batch(self, out, a, npolys=None, stream=None):
         n = a.shape[0] if npolys is None else npolys
-        call("cp_rho_batch", self._h, _ptr(out), _ptr(a), n, _stream(stream))
+        call("cp_rho_batch", self._h, self._buf(out, QBase, n * self.k, "out"), self._buf(a, QBase, n, "a"), n,
+             _stream(stream))
 
     def rho(self, out, a, stream=None):
-        call("cp_rho", self._h, _ptr(out), _ptr(a), _stream(stream))
+        call("cp_rho", self._h, self._buf(out, QBase, self.k, "out"), self._buf(a, QBase, 1, "a"), _stream(stream))
 
     # ---- composite (DGT domain) ----
     def poly_basis_extension_q_to_b(self, out_b, in_q, stream=None):
-        call("cp_poly_basis_extension_q_to_b", self._h, _ptr(out_b), _ptr(in_q), _ptr(self.workspace()),
-             _stream(stream))
+        call("cp_poly_basis_extension_q_to_b", self._h, self._buf(out_b, BBase, 1, "out_b"),
+             self._buf(in_q, QBase, 1, "in_q"), _ptr(self.workspace()), _stream(stream))
 
     def poly_basis_extension_q_to_qb(self, out_qb, in_q, stream=None):
-        call("cp_poly_basis_extension_q_to_qb", self._h, _ptr(out_qb), _ptr(in_q), _ptr(self.workspace()),
-             _stream(stream))
+        call("cp_poly_basis_extension_q_to_qb", self._h, self._buf(out_qb, QBBase, 1, "out_qb"),
+             self._buf(in_q, QBase, 1, "in_q"), _ptr(self.workspace()), _stream(stream))
 
     def poly_basis_extension_b_to_q(self, out_q, in_b, stream=None):
-        call("cp_poly_basis_extension_b_to_q", self._h, _ptr(out_q), _ptr(in_b), _ptr(self.workspace()),
-             _stream(stream))
+        call("cp_poly_basis_extension_b_to_q", self._h, self._buf(out_q, QBase, 1, "out_q"),
+             self._buf(in_b, BBase, 1, "in_b"), _ptr(self.workspace()), _stream(stream))
 
     def poly_complex_scaling_tdivq(self, out_q, in_q, in_b, flags=0, stream=None):
-        call("cp_poly_complex_scaling_tdivq", self._h, _ptr(out_q), _ptr(in_q), _ptr(in_b), flags,
-             _ptr(self.workspace()), _stream(stream))
-
-    def poly_simple_scaling_tdivq(self, out_t, in_q, stream=None):
-        call("cp_poly_simple_scaling_tdivq", self._h, _ptr(out_t), _ptr(in_q), _ptr(self.workspace()),
+        call("cp_poly_complex_scaling_tdivq", self._h, self._buf(out_q, QBase, 1, "out_q"),
+             self._buf(in_q, QBase, 1, "in_q"), self._buf(in_b, BBase, 1, "in_b"), flags, _ptr(self.workspace()),
              _stream(stream))
 
+    def poly_simple_scaling_tdivq(self, out_t, in_q, stream=None):
+        call("cp_poly_simple_scaling_tdivq", self._h, self._buf(out_t, TBase, 1, "out_t"),
+             self._buf(in_q, QBase, 1, "in_q"), _ptr(self.workspace()), _stream(stream))
+
     def bfv_mul(self, c0, c1, c2, a0, a1, b0, b1, stream=None):
-        call("cp_bfv_mul", self._h, _ptr(c0), _ptr(c1), _ptr(c2), _ptr(a0), _ptr(a1), _ptr(b0), _ptr(b1),
+        call("cp_bfv_mul", self._h, *self._bufs(QBase, c0=c0, c1=c1, c2=c2, a0=a0, a1=a1, b0=b0, b1=b1),
              _ptr(self.workspace()), _stream(stream))
 
     def bfv_mul_batch_workspace(self, npairs: int) -> torch.Tensor:
@@ -428,18 +481,22 @@ class Engine:
 
     def bfv_mul_batch(self, c, a0, a1, b0, b1, npairs, workspace, stream=None):
         """c: (3 * npairs, k, N, 2); inputs (npairs, k, N, 2), all DGT domain."""
-        call("cp_bfv_mul_batch", self._h, _ptr(c), _ptr(a0), _ptr(a1), _ptr(b0), _ptr(b1), npairs, _ptr(workspace),
-             _stream(stream))
+        ws = self._ws(workspace, _lib.lib().cp_bfv_mul_batch_workspace_bytes(self._h, npairs))
+        call("cp_bfv_mul_batch", self._h, self._buf(c, QBase, 3 * npairs, "c"),
+             *self._bufs(QBase, npairs, a0=a0, a1=a1, b0=b0, b1=b1), npairs, ws, _stream(stream))
 
     # ---- sampler ----
     def sample(self, out, base, kind, seed, stream_id, npolys=None, to_dgt=True, stream=None):
         n = out.shape[0] if npolys is None else npolys
-        call("cp_sample", self._h, _ptr(out), base, kind, int(seed), int(stream_id), n, 1 if to_dgt else 0,
-             _stream(stream))
+        call("cp_sample", self._h, self._buf(out, base, n, "out"), base, kind, int(seed), int(stream_id), n,
+             1 if to_dgt else 0, _stream(stream))
 
     def sample_ids(self, out, base, kind, seed, stream_ids: torch.Tensor, to_dgt=True, stream=None):
         """Polynomial i of `out` drawn with stream id stream_ids[i] (int32 device tensor)."""
-        call("cp_sample_ids", self._h, _ptr(out), base, kind, int(seed), _ptr(stream_ids), int(stream_ids.numel()),
+        if stream_ids.dtype != torch.int32 or not stream_ids.is_cuda or not stream_ids.is_contiguous():
+            raise ValueError("sample_ids: stream_ids must be a contiguous int32 CUDA tensor")
+        n = int(stream_ids.numel())
+        call("cp_sample_ids", self._h, self._buf(out, base, n, "out"), base, kind, int(seed), _ptr(stream_ids), n,
              1 if to_dgt else 0, _stream(stream))
 
     # ---- host helpers (folded layout) ----

@@ -10,7 +10,9 @@
 //  * errors throw std::runtime_error (cuPoly: assert / exit(1));
 //  * every d_coefs buffer is allocated for a QB polynomial, so a poly_t can
 //    change base (e.g. as the output of a basis extension) without reallocation;
-//  * HPS results are exact for every input (cuPoly's float paths are within 1);
+//  * HPS scaling is exact round(t X / Q) for every input (cuPoly's float path is
+//    within 1); base conversions lift X within FPERROR of the modulus to X - S as
+//    cuPoly does, decided exactly (cuPoly decides it in double precision);
 //  * poly_complex_scaling_tDivQ leaves its inputs unchanged (cuPoly
 //    inverse-transforms them in place);
 //  * poly_are_equal compares every coefficient up to the degree (cuPoly skips

@@ -212,7 +212,10 @@ int cp_double_op_by_int(const cp_engine* e, void* b1, const void* a1, void* b2, 
 
 /* ---- HPS, coefficient domain: replace CUDAEngine::execute_polynomial_basis_ext_Q_to_B /
  *      _B_to_Q / _complex_scaling / _simple_scaling (src/cuda/cudaengine.cu:304-798).
- *      Exact: X mod m for the unique X in [0, Q) (resp. [0, B)); round(t X / Q). */
+ *      X mod m for the X in [0, S) with the given residues (S = Q, resp. B), lifted as
+ *      cuPoly lifts it: X - S when S - X <= S FPERROR (FPERROR = 1e-9, cuPoly's
+ *      tolerance, settings.h:105; cuPoly's double overflow count rounds up there),
+ *      decided exactly; complex scaling: exact round(t X / Q) mod b_j. */
 int cp_basis_ext_q_to_b(const cp_engine* e, void* out_b, const void* in_q, int npolys, void* stream);
 int cp_basis_ext_b_to_q(const cp_engine* e, void* out_q, const void* in_b, int npolys, void* stream);
 int cp_complex_scaling(const cp_engine* e, void* out_b, const void* in_q, const void* in_b, int npolys,

@@ -96,6 +96,17 @@ void write_u64(const std::string& path, const std::vector<uint64_t>& v) {
 
 int nphi_of() { return 2 * CUDAEngine::N; }
 
+// Every copy goes on the Context's stream and is waited for.  cuPoly builds with
+// --default-stream per-thread, so a plain cudaMemcpy runs on the per-thread stream,
+// which does not order with the Context's stream: a pageable host-to-device copy may
+// still be in flight when the next kernel on the Context's stream reads its target,
+// and a device-to-device copy returns before it has run.
+void copy(Context* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, const char* what) {
+  check(cudaStreamSynchronize(ctx->get_stream()), what);
+  check(cudaMemcpyAsync(dst, src, bytes, kind, ctx->get_stream()), what);
+  check(cudaStreamSynchronize(ctx->get_stream()), what);
+}
+
 // Rows [nres][nphi] at `rows` -> poly p over `base`, in cuPoly's DGT domain.
 void upload(Context* ctx, poly_t* p, int base, const uint64_t* rows) {
   poly_init(ctx, p, base);
@@ -106,8 +117,7 @@ void upload(Context* ctx, poly_t* p, int base, const uint64_t* rows) {
       h[(size_t)r * N + j].re = rows[(size_t)r * nphi + j];
       h[(size_t)r * N + j].imag = rows[(size_t)r * nphi + j + N];
     }
-  check(cudaStreamSynchronize(ctx->get_stream()), "sync before upload");
-  check(cudaMemcpy(p->d_coefs, h.data(), h.size() * sizeof(GaussianInteger), cudaMemcpyHostToDevice), "upload");
+  copy(ctx, p->d_coefs, h.data(), h.size() * sizeof(GaussianInteger), cudaMemcpyHostToDevice, "upload");
   DGTEngine::execute_dgt(p->d_coefs, base, FORWARD, ctx);
   check(cudaStreamSynchronize(ctx->get_stream()), "forward DGT");
   p->status = RNSSTATE;
@@ -121,12 +131,11 @@ void download(Context* ctx, poly_t* p, std::vector<uint64_t>& out) {
   const size_t bytes = (size_t)nres * N * sizeof(GaussianInteger);
   GaussianInteger* tmp = nullptr;
   check(cudaMalloc((void**)&tmp, bytes), "cudaMalloc");
-  check(cudaStreamSynchronize(ctx->get_stream()), "sync before download");
-  check(cudaMemcpy(tmp, p->d_coefs, bytes, cudaMemcpyDeviceToDevice), "copy");
+  copy(ctx, tmp, p->d_coefs, bytes, cudaMemcpyDeviceToDevice, "copy");
   DGTEngine::execute_dgt(tmp, base, INVERSE, ctx);
   check(cudaStreamSynchronize(ctx->get_stream()), "inverse DGT");
   std::vector<GaussianInteger> h((size_t)nres * N);
-  check(cudaMemcpy(h.data(), tmp, bytes, cudaMemcpyDeviceToHost), "download");
+  copy(ctx, h.data(), tmp, bytes, cudaMemcpyDeviceToHost, "download");
   check(cudaFree(tmp), "cudaFree");
   const size_t o = out.size();
   out.resize(o + (size_t)nres * nphi);
@@ -140,10 +149,9 @@ void download(Context* ctx, poly_t* p, std::vector<uint64_t>& out) {
 void raw_download(Context* ctx, poly_t* p, std::vector<uint64_t>& out) {
   const int nres = CUDAEngine::get_n_residues(p->base);
   const size_t words = (size_t)nres * CUDAEngine::N * 2;
-  check(cudaStreamSynchronize(ctx->get_stream()), "sync");
   const size_t o = out.size();
   out.resize(o + words);
-  check(cudaMemcpy(out.data() + o, p->d_coefs, words * 8, cudaMemcpyDeviceToHost), "raw download");
+  copy(ctx, out.data() + o, p->d_coefs, words * 8, cudaMemcpyDeviceToHost, "raw download");
 }
 
 void need(const std::vector<uint64_t>& in, size_t words, const char* op) {
@@ -253,8 +261,7 @@ int run_op(const std::string& op, int k, int kl, int nphi, uint64_t t, Context* 
     // The result is residue 0 of b's buffer in the coefficient domain
     // (cudaengine.cu:323-362 writes a[cid] for every Gaussian element).
     std::vector<GaussianInteger> h(CUDAEngine::N);
-    check(cudaStreamSynchronize(ctx->get_stream()), "simple scaling");
-    check(cudaMemcpy(h.data(), b.d_coefs, h.size() * sizeof(GaussianInteger), cudaMemcpyDeviceToHost), "download");
+    copy(ctx, h.data(), b.d_coefs, h.size() * sizeof(GaussianInteger), cudaMemcpyDeviceToHost, "download");
     out.resize((size_t)nphi);
     for (int j = 0; j < CUDAEngine::N; ++j) {
       out[j] = h[j].re;
@@ -295,10 +302,9 @@ int run_op(const std::string& op, int k, int kl, int nphi, uint64_t t, Context* 
     for (int o = 0; o < 3; ++o) download(ctx, &tb[o], out);
     poly_init(ctx, &c0, QBase);
     poly_complex_scaling_tDivQ(ctx, &c0, &tq[0], &tb[0]);
-    check(cudaStreamSynchronize(ctx->get_stream()), "complex scaling");
     const size_t o0 = out.size();
     out.resize(o0 + bw);
-    check(cudaMemcpy(out.data() + o0, ctx->d_coefs_B, bw * 8, cudaMemcpyDeviceToHost), "d_coefs_B");
+    copy(ctx, out.data() + o0, ctx->d_coefs_B, bw * 8, cudaMemcpyDeviceToHost, "d_coefs_B");
     download(ctx, &c0, out);
     for (poly_t* p : {&a[0], &a[1], &a[2], &a[3], &aB[0], &aB[1], &aB[2], &aB[3], &tq[0], &tq[1], &tq[2], &tb[0],
                       &tb[1], &tb[2], &c0})

@@ -72,3 +72,29 @@ def sha(a: np.ndarray) -> str:
 def gi_rows_to_list(res: np.ndarray):
     """(N, 2) uint64 -> list of (re, im) Python tuples."""
     return [(int(a), int(b)) for a, b in res.tolist()]
+
+
+def cupoly_chain_restated(x: np.ndarray, Q, B, t: int) -> np.ndarray:
+    """cuPoly's BFV multiplication chain (4 x poly_basis_extension_Q_to_B, poly_dr2 over Q and
+    over B, 3 x poly_complex_scaling_tDivQ; src/arithmetic/polynomial.cu:350-470, 951-1000)
+    restated: its float base extension and float complex scaling (oracle/pyoracle.py) around
+    the exact tensor.  x: (4, k, nphi) coefficient rows of a0, a1, b0, b1; returns (3, k, nphi)."""
+    from oracle import coracle as CO
+    from oracle import pyoracle as O
+
+    k = len(Q)
+
+    def cols(rows):
+        return [[int(v) for v in rows[:, j]] for j in range(rows.shape[1])]
+
+    ext = [np.array([O.cupoly_float_ext_q_to_b(v, Q, B) for v in cols(x[i])], dtype=np.uint64).T for i in range(4)]
+    qb = [np.concatenate([x[i], ext[i]]) for i in range(4)]
+    P = list(Q) + list(B)
+    a0, a1, b0, b1 = (CO.polymul(qb[i][None], qb[j][None], P)[0] for i, j in [(0, 2), (0, 3), (1, 2), (1, 3)])
+    t1 = np.array([[(int(u) + int(v)) % p for u, v in zip(a1[r], b0[r])] for r, p in enumerate(P)], dtype=np.uint64)
+    outs = []
+    for ten in (a0, t1, b1):
+        tq, tb = cols(ten[:k]), cols(ten[k:])
+        outs.append(np.array([O.cupoly_float_complex_scaling_tdivq(a, b, Q, B, t) for a, b in zip(tq, tb)],
+                             dtype=np.uint64).T)
+    return np.stack(outs)

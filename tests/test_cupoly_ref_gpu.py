@@ -29,7 +29,7 @@ import pytest
 
 from oracle import coracle as CO
 from oracle import pyoracle as O
-from tests.common import fold, random_poly_residues, sha, unfold
+from tests.common import cupoly_chain_restated, fold, random_poly_residues, sha, unfold
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
@@ -129,12 +129,22 @@ def test_basis_extension_equals_cupolys(gpu, c):
 @pytest.mark.parametrize("c", _cases("sscale"), ids=_id)
 def test_simple_scaling_equals_cupolys(gpu, c):
     from cupoly_b200.engine import to_u64
-    k, nphi = c["k"], c["nphi"]
+    k, nphi, t = c["k"], c["nphi"], c["t"]
     e = _engine(k, c["kl"], nphi, c["t"])
-    a = _to_dgt(e, _inputs(c).reshape(k, nphi), 0)
+    x = _inputs(c).reshape(k, nphi)
+    a = _to_dgt(e, x, 0)
     out = e.empty(3)
     e.poly_simple_scaling_tdivq(out, a)
-    assert _same(c, unfold(to_u64(out))[0, 0])
+    got = unfold(to_u64(out))[0, 0]
+    # cuPoly's words are its unreduced sums (its d_RNST is never set); reduced mod t
+    # they are cuPoly's scaled values, which this library gives exactly.
+    cx = [[int(v) for v in x[:, j]] for j in range(nphi)]
+    raw = np.array([O.cupoly_float_simple_scaling(v, e.Q, t, raw=True) for v in cx], dtype=np.uint64)
+    assert sha(raw) == c["sha256"]
+    exact = np.array([O.simple_scaling_exact(v, e.Q, t) for v in cx], dtype=np.uint64)
+    assert np.array_equal(got, exact)
+    for j in np.nonzero(raw % np.uint64(t) != exact)[0]:
+        assert (int(raw[j]) - int(exact[j])) % t in (1, t - 1)
 
 
 @pytest.mark.parametrize("c", _cases("cscale"), ids=_id)
@@ -180,9 +190,13 @@ def test_bfv_chain_equals_cupolys(gpu, c):
     got = np.stack([_coeffs(e, o, 0)[0] for o in outs])
     if _same(c, got):
         return
+    # cuPoly's float complex scaling is off by one on some coefficients (at k = 6 often):
+    # the device gives the exact product, and cuPoly's recorded words are its restated chain
     exact = CO.bfv_mul(*[x[i][None] for i in range(4)], e.Q, e.B, t)
-    assert all(np.array_equal(g, ex[0]) for g, ex in zip(got, exact))
-    pytest.fail("cuPoly's chain differs from the exact product at nphi %d, k %d" % (nphi, k))
+    restated = cupoly_chain_restated(x, e.Q, e.B, t)
+    assert sha(restated) == c["sha256"]
+    for g, ex, r in zip(got, exact, restated):
+        _only_rounding_differences(g, ex[0], r, e.Q)
 
 
 @pytest.mark.skipif(not os.path.exists(DRIVER), reason="cuPoly's sources were not compiled here")

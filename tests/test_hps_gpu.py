@@ -52,7 +52,8 @@ def test_basis_extension_edges(gpu, k):
         S = O.prod(src)
         T = O.lift_threshold(S)
         vals = [0, 1, S - 1, (S - 1) // 2, (S + 1) // 2, 12345, T - 1, T, T + 1, T - 2, S - 2]
-        vals += [T + (S - T) * i // 26 for i in range(26)] + [T - 1 - (i << 40) for i in range(17)]
+        vals += [T + (S - T) * i // 26 for i in range(26)] + [T - 1 - (i << 40) for i in range(27)]
+        assert len(vals) == e.nphi
         xs = np.array([[v % q for v in vals] for q in src], dtype=np.uint64)
         out = e.empty(1 if fwd else 0)
         (e.basis_ext_q_to_b if fwd else e.basis_ext_b_to_q)(out, _dev(fold(xs)[None]))
