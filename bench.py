@@ -13,11 +13,13 @@ inputs resident in HBM (batched form, two consecutive batches in flight on two
 streams, device-timed, max over ranks);
 `e2e` repeats it through the C ABI with pinned host buffers and the
 host<->device copies inside the timed region; `plain` is the per-call form
-(one cp_bfv_mul per pair); `polymul` is the batched DGT polymul/s of the
-nphi = 4096, k = 2 configuration; `cupoly_gpu` times cuPoly's own kernels
-per call when its sources were compiled into oracle/_ref.  With --impl
-reference the C oracle (the CPU restatement of the reference path: cuPoly has
-no CPU implementation of it) is timed on the host cores.
+(one cp_bfv_mul per pair); `plain_cxx` times the same per-call sequences as
+`cupoly_gpu` through this library's C++ drop-in layer; `polymul` is the
+batched DGT polymul/s of the nphi = 4096, k = 2 configuration.  Two reference
+legs run on rank 0: `cupoly_gpu` times cuPoly's own kernels per call when its
+sources were compiled into oracle/_ref, and `cpu_baseline` the C oracle (the
+CPU restatement of the reference path: cuPoly has no CPU implementation of it)
+on the host cores.  With --impl reference the C oracle is the timed arm.
 """
 from __future__ import annotations
 
@@ -199,7 +201,9 @@ def run_reference(args, D: Dist):
         "cpu_baseline": {"value": round(v, 3), "unit": "hom-mul/s", "cores": cores, "kind": "port",
                          "sample": "%d pairs per step, C restatement (oracle/cpoly_oracle.c), OpenMP" % per_step},
         "e2e": {"value": round(v, 3), "unit": "hom-mul/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "cuPoly needs NTL/GMP/gtest and cannot be built here; the oracle's C port of its path is timed",
+        "note": ("cuPoly runs this path only on the GPU (NTL appears only in its tests), so the oracle's C port "
+                 "of the path is the CPU implementation timed; cupoly_gpu holds cuPoly's own kernels per call"),
+        "cupoly_gpu": None if args.no_cupoly_gpu else cupoly_gpu_times(),
     }
     print(json.dumps(line), flush=True)
 
@@ -396,6 +400,7 @@ def next_rows(seed: int, hbm_peak: float):
 
 
 CUPOLY_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cupoly_ref_driver")
+PERCALL = os.path.join(ROOT, "cupoly_b200", "lib", "cupoly_percall")
 
 
 def cupoly_gpu_times():
@@ -404,7 +409,7 @@ def cupoly_gpu_times():
     poly_mul, one inverse DGT per call) and the BFV multiplication chain at nphi 8192,
     k 5, kl 6 (four poly_basis_extension_Q_to_B, poly_dr2 over Q and B, three
     poly_complex_scaling_tDivQ per pair), each timed with CUDA events over 200 calls.
-    Context for the per-call forms here; the reference arm stays the CPU restatement."""
+    A reference leg beside the per-call forms; the reference arm's value stays the CPU restatement."""
     if not os.path.exists(CUPOLY_DRIVER):
         return {"unavailable": "cuPoly's sources were not compiled into oracle/_ref"}
     import tempfile
@@ -421,6 +426,26 @@ def cupoly_gpu_times():
         ms = t["polymul_ms"] if name.startswith("polymul") else t["bfv_mul_ms"]
         out[name] = {"ms_per_call": round(ms, 4), "per_s": round(1e3 / ms, 1)}
     out["source"] = "cuPoly 0.3.5 library (its own kernels), one call per polymul / pair, CUDA events"
+    return out
+
+
+def dropin_percall_times():
+    """This library's C++ drop-in layer (libcupoly.so, cuPoly's API) per call, the same two
+    call sequences as cupoly_gpu_times on the same sizes: cupoly_b200/host/bench/percall.cpp,
+    CUDA events on the Context's stream over 200 calls."""
+    if not os.path.exists(PERCALL):
+        return {"unavailable": "cupoly_b200/lib/cupoly_percall was not built"}
+    out = {}
+    for name, (k, nphi) in {"polymul_nphi4096_k2": (2, 4096), "bfv_mul_nphi8192_k5_kl6": (5, 8192)}.items():
+        r = subprocess.run([PERCALL, str(k), str(k + 1), str(nphi), "200"], capture_output=True, text=True,
+                           timeout=300)
+        if r.returncode != 0:
+            raise RuntimeError("cupoly_percall failed: " + (r.stderr or r.stdout)[-300:])
+        t = json.loads(r.stdout.strip().splitlines()[-1])
+        ms = t["polymul_ms"] if name.startswith("polymul") else t["bfv_mul_ms"]
+        out[name] = {"ms_per_call": round(ms, 4), "per_s": round(1e3 / ms, 1)}
+    out["source"] = ("this library's C++ layer (libcupoly.so), one call sequence per product / pair as in "
+                     "cupoly_gpu, CUDA events")
     return out
 
 
@@ -784,8 +809,12 @@ def run_ours(args, D: Dist):
         del ex, sch
         torch.cuda.empty_cache()
 
-    cupoly_gpu = cupoly_gpu_times() if D.rank == 0 and not args.no_cupoly_gpu else None
+    percall_cxx = dropin_percall_times() if D.rank == 0 else None
 
+    # ---- reference legs, rank 0 only: cuPoly's own kernels per call on this GPU (when its
+    # sources were compiled into oracle/_ref) and the CPU restatement of the path on the host
+    # cores; the only places this arm executes anything under oracle/ ----
+    cupoly_gpu = cupoly_gpu_times() if D.rank == 0 and not args.no_cupoly_gpu else None
     cpu = None
     if D.rank == 0 and not args.no_cpu_baseline:
         rate, done, el, cores = cpu_bfv_rate(10.0)
@@ -806,6 +835,7 @@ def run_ours(args, D: Dist):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "host_link": pcie},
             "plain": {"value": round(plain_value, 2), "unit": "hom-mul/s",
                       "form": "one cp_bfv_mul call per pair (cuPoly's per-call composition)", "pairs": PP},
+            "plain_cxx": percall_cxx,
             "batched_over_plain": round(value / D.world / plain_value, 2),
             "polymul": ({"value": round(polymul_value, 1), "unit": "polymul/s",
                          "config": "nphi=4096, k=2, batch 1024 (fused: 2 forward DGTs, inverse with products on load), 2 batches in flight",

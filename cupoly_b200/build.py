@@ -34,6 +34,7 @@ LIBPATH = os.path.join(LIBDIR, LIBNAME)
 HOSTDIR = os.path.join(HERE, "host")
 INCDIR = os.path.abspath(os.path.join(HERE, "..", "include"))
 CXXLIB = os.path.join(LIBDIR, "libcupoly.so")
+PERCALL = os.path.join(LIBDIR, "cupoly_percall")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
@@ -104,6 +105,19 @@ def build_host(force: bool = False) -> str:
     return CXXLIB
 
 
+def build_percall(force: bool = False) -> str:
+    """Compile the per-call timing program of the C++ layer (host/bench/percall.cpp) into
+    lib/cupoly_percall; bench.py runs it beside cuPoly's own per-call times."""
+    src = os.path.join(HOSTDIR, "bench", "percall.cpp")
+    if force or _stale(PERCALL, [src, CXXLIB]):
+        cxx = shutil.which("g++") or "g++"
+        cmd = [cxx, "-O2", "-Wall"] + cxx_flags() + [src, "-o", PERCALL] + cxx_link_flags()
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("g++ failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))
+    return PERCALL
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJDIR, exist_ok=True)
     sources = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
@@ -115,6 +129,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
     build_host(force)
+    build_percall(force)
     if verbose:
         print(LIBPATH)
         print(CXXLIB)

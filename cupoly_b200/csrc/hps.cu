@@ -49,9 +49,9 @@ __device__ __forceinline__ void mrc_garner(uint64_t (&d)[NS], const ModConst* __
   for (int i = 1; i < NS; ++i) {
     uint64_t l = 0, h = 0, t = 0;
 #pragma unroll
-    for (int j = 0; j < i; ++j) mac192(l, h, t, d[j], __ldg(W + i * NS + j));
+    for (int j = 0; j < i; ++j) mac192_w(l, h, t, d[j], __ldg(W + i * NS + j));
     const ModConst m = mcs[i];
-    const uint64_t sum = red192(l, h, t, m.p, m.r1, m.r2);
+    const uint64_t sum = red192_w(l, h, t, m.p, m.r1, m.r2);
     d[i] = shoup_mul(d[i] + m.p - sum, __ldg(pinv + i), __ldg(pinv_s + i), m.p);
   }
 }
@@ -106,8 +106,8 @@ __device__ __forceinline__ uint64_t dot_mod(const uint64_t (&d)[NS], const uint6
                                             const ModConst& mt) {
   uint64_t l = 0, h = 0, t = 0;
 #pragma unroll
-  for (int i = 0; i < NS; ++i) mac192(l, h, t, d[i], __ldg(w + i));
-  return red192(l, h, t, mt.p, mt.r1, mt.r2);
+  for (int i = 0; i < NS; ++i) mac192_w(l, h, t, d[i], __ldg(w + i));
+  return red192_w(l, h, t, mt.p, mt.r1, mt.r2);
 }
 
 // digits > (prod - 1) / 2 ?
@@ -165,8 +165,8 @@ __device__ __forceinline__ uint64_t fast_dot(const uint64_t (&y)[NS], const uint
                                              const ModConst& mt) {
   uint64_t l = negv, h = 0, t = 0;
 #pragma unroll
-  for (int i = 0; i < NS; ++i) mac192(l, h, t, y[i], __ldg(hmod + i));
-  return red192(l, h, t, mt.p, mt.r1, mt.r2);
+  for (int i = 0; i < NS; ++i) mac192_w(l, h, t, y[i], __ldg(hmod + i));
+  return red192_w(l, h, t, mt.p, mt.r1, mt.r2);
 }
 
 struct ConvArgs {

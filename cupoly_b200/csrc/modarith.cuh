@@ -34,6 +34,23 @@ struct ModConst {
   uint64_t pm;      // 1: p = 2^63 - c with c < 2^31 - 1 (pm_red applies); 0: generic path
 };
 
+#ifdef __CUDA_ARCH__
+// hi:lo = a * b as four 32 x 32 -> 64 multiply-adds, each folding the previous carry
+// in (a 32 x 32 product plus one 32-bit addend, or plus two for the top word, stays
+// below 2^64): the low and high words of one product share their partial products.
+__device__ __forceinline__ void mul128(uint64_t a, uint64_t b, uint64_t& lo, uint64_t& hi) {
+  asm("{\n\t.reg .u32 a0, a1, b0, b1, r0, r1, s1, c0, c1, c2;\n\t.reg .u64 t0, t1, t2, t3, x;\n\t"
+      "mov.b64 {a0, a1}, %2;\n\tmov.b64 {b0, b1}, %3;\n\t"
+      "mul.wide.u32 t0, a0, b0;\n\tmov.b64 {r0, c0}, t0;\n\t"
+      "cvt.u64.u32 x, c0;\n\tmad.wide.u32 t1, a0, b1, x;\n\tmov.b64 {s1, c1}, t1;\n\t"
+      "cvt.u64.u32 x, s1;\n\tmad.wide.u32 t2, a1, b0, x;\n\tmov.b64 {r1, c2}, t2;\n\t"
+      "cvt.u64.u32 x, c1;\n\tmad.wide.u32 t3, a1, b1, x;\n\t"
+      "cvt.u64.u32 x, c2;\n\tadd.u64 %1, t3, x;\n\tmov.b64 %0, {r0, r1};\n\t}"
+      : "=l"(lo), "=l"(hi)
+      : "l"(a), "l"(b));
+}
+#endif
+
 // Three-word accumulation (t:h:l) += a * b, for lazily reduced dot products.
 CP_HD void mac192(uint64_t& l, uint64_t& h, uint64_t& t, uint64_t a, uint64_t b) {
 #ifdef __CUDA_ARCH__
@@ -51,6 +68,20 @@ CP_HD void mac192(uint64_t& l, uint64_t& h, uint64_t& t, uint64_t a, uint64_t b)
 #endif
 }
 
+// mac192 with the product formed by mul128: fewer 32-bit multiplies; used by the base
+// conversions, whose dot products are bound by the integer multiply pipe.
+CP_HD void mac192_w(uint64_t& l, uint64_t& h, uint64_t& t, uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+  uint64_t pl, ph;
+  mul128(a, b, pl, ph);
+  asm("add.cc.u64 %0, %0, %3;\n\taddc.cc.u64 %1, %1, %4;\n\taddc.u64 %2, %2, 0;"
+      : "+l"(l), "+l"(h), "+l"(t)
+      : "l"(pl), "l"(ph));
+#else
+  mac192(l, h, t, a, b);
+#endif
+}
+
 // (t 2^128 + h 2^64 + l) mod p for t < 2^8, using r1 = 2^64 mod p < 2^32 and
 // r2 = 2^128 mod p: fold the high words down three times, then at most two
 // subtractions (the value is below 2^64 < 3p).
@@ -63,6 +94,29 @@ CP_HD uint64_t red192(uint64_t l, uint64_t h, uint64_t t, uint64_t p, uint64_t r
   // w = lo(z) + hi(z) r1 < 2^64 + 2^34; one carry at most
   const uint64_t zl = (uint64_t)z, zh = (uint64_t)(z >> 64);
   uint64_t w = zl + zh * r1;
+  if (w < zl) w += r1;
+  w = w >= p ? w - p : w;
+  w = w >= p ? w - p : w;
+  return w;
+}
+
+// red192 with every product written as 32 x 32 -> 64 multiplies (r1 < 2^32, t < 2^8):
+// seven wide multiplies; used by the base conversions.
+CP_HD uint64_t red192_w(uint64_t l, uint64_t h, uint64_t t, uint64_t p, uint64_t r1, uint64_t r2) {
+  const uint64_t r = (uint32_t)r1;
+  // y = l + h r1 + t r2 < 2^97
+  const uint64_t a0 = (uint64_t)(uint32_t)h * r, a1 = (h >> 32) * r;       // h r1 = a0 + a1 2^32
+  const uint64_t b0 = (uint64_t)(uint32_t)t * (uint32_t)r2;                 // t r2 = b0 + b1 2^32
+  const uint64_t b1 = (uint64_t)(uint32_t)t * (uint32_t)(r2 >> 32);
+  const unsigned __int128 y = (unsigned __int128)l + a0 + b0 + ((unsigned __int128)a1 << 32) +
+                              ((unsigned __int128)b1 << 32);
+  // z = lo(y) + hi(y) r1 < 2^67, hi(y) < 2^34
+  const uint64_t yh = (uint64_t)(y >> 64);
+  const unsigned __int128 z = (unsigned __int128)(uint64_t)y + (uint64_t)(uint32_t)yh * r +
+                              ((unsigned __int128)((yh >> 32) * r) << 32);
+  // w = lo(z) + hi(z) r1 < 2^64 + 2^35: one carry at most
+  const uint64_t zl = (uint64_t)z, zh = (uint64_t)(z >> 64);
+  uint64_t w = zl + (uint64_t)(uint32_t)zh * r;
   if (w < zl) w += r1;
   w = w >= p ? w - p : w;
   w = w >= p ? w - p : w;
@@ -143,12 +197,23 @@ CP_HD uint64_t red128(uint64_t hi, uint64_t lo, const ModConst& m) {
 
 // Exact a * b mod p for a < p, b < 2^64.
 CP_HD uint64_t mul_mod(uint64_t a, uint64_t b, const ModConst& m) {
+#ifdef __CUDA_ARCH__
+  uint64_t lo, hi;
+  mul128(a, b, lo, hi);
+  return red128(hi, lo, m);
+#else
   return red128(mulhi64(a, b), a * b, m);
+#endif
 }
 
 // 128-bit accumulate helpers (hi:lo += a * b).
 CP_HD void mac128(uint64_t& hi, uint64_t& lo, uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+  uint64_t pl, ph;
+  mul128(a, b, pl, ph);
+#else
   uint64_t pl = a * b, ph = mulhi64(a, b);
+#endif
   lo += pl;
   hi += ph + (lo < pl);
 }
