@@ -45,6 +45,7 @@ SIGNATURES = {
     "cp_engine_set_narrow_plan": (_i, [_vp, _i, _i, C.c_longlong]),
     "cp_engine_get_narrow_plan": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_longlong)]),
     "cp_engine_set_split_mode": (_i, [_vp, _i]),
+    "cp_engine_set_hps_force_exact": (_i, [_vp, _i]),
     "cp_engine_get_split_mode": (_i, [_vp]),
     "cp_ckks_modulus_raising": (_i, [_vp, _vp, _vp, _i, _vp, _vp]),
     "cp_ckks_modulus_reduction": (_i, [_vp, _vp, _vp, _i, _vp, _vp]),

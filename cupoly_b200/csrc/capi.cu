@@ -252,6 +252,14 @@ int cp_engine_set_split_mode(cp_engine* h, int mode) {
 
 int cp_engine_get_split_mode(const cp_engine* h) { return h ? h->e.plan.cluster : -1; }
 
+int cp_engine_set_hps_force_exact(cp_engine* h, int on) {
+  CP_REQUIRE(h, "cp_engine_set_hps_force_exact: NULL engine");
+  CP_REQUIRE(on == 0 || on == 1, "cp_engine_set_hps_force_exact: on must be 0 or 1");
+  cudaDeviceSynchronize();  // conversions in flight keep the form they were launched with
+  h->e.hps_force_exact = on;
+  return CP_OK;
+}
+
 int cp_engine_get_plan(const cp_engine* h, int* log_radix, int* log_cta, int* split_bits) {
   CP_REQUIRE(h, "cp_engine_get_plan: NULL engine");
   if (log_radix) *log_radix = h->e.plan.logR;
@@ -667,7 +675,10 @@ int cp_bfv_mul_batch(const cp_engine* h, void* c, const void* a0, const void* a1
   ulonglong2* CQ = XB + 4 * P * be;                    // [3][P][k]
   ulonglong2* CB = CQ + 3 * P * qe;                    // [3][P][kl]
   ulonglong2* U = CB + 3 * P * be;                     // [3][P][kl]
-  // 1. inverse DGT of the four inputs over Q, gathered into X (no copies)
+  // Every inverse DGT below untwists with a prescaled table (off_untwist_pre), so that it
+  // also applies the first constant product of the conversion that reads its output.
+  // 1. inverse DGT of the four inputs over Q, gathered into X (no copies):
+  //    X = x_i (Q/q_i)^-1 mod q_i
   InvSrc gather{};
   gather.p[0] = reinterpret_cast<const ulonglong2*>(a0);
   gather.p[1] = reinterpret_cast<const ulonglong2*>(a1);
@@ -675,6 +686,7 @@ int cp_bfv_mul_batch(const cp_engine* h, void* c, const void* a0, const void* a1
   gather.p[3] = reinterpret_cast<const ulonglong2*>(b1);
   gather.mode = 2;
   gather.npairs = npairs;
+  gather.untwist = 1;
   {
     NvtxRange r("inverse DGT over Q (4P)");
     CP_TRY(launch_dgt_ex(e, X, nullptr, &gather, CP_QBASE, 4 * npairs, 0, true, st));
@@ -682,22 +694,25 @@ int cp_bfv_mul_batch(const cp_engine* h, void* c, const void* a0, const void* a1
   // 2. exact Q -> B extension, forward DGT over B
   {
     NvtxRange r("Q -> B, forward DGT over B (4P)");
-    CP_TRY(hps_basis_ext(e, XB, X, true, 4 * npairs, st));
+    CP_TRY(hps_basis_ext_pre(e, XB, X, true, 4 * npairs, st));
     CP_TRY(launch_dgt(e, XB, CP_BBASE, 4 * npairs, 0, false, st));
   }
-  // 3. tensor product computed inside the inverse DGTs (Q side from the inputs, B side from XB)
+  // 3. tensor product computed inside the inverse DGTs (Q side from the inputs, B side from
+  //    XB): CQ = t c_i (Q/q_i)^-1 mod q_i, CB = t Q^-1 (B/b_j)^-1 c_j mod b_j
   InvSrc tq = gather;
   tq.mode = 1;
+  tq.untwist = 2;
   NvtxRange r3("tensor products + inverse DGTs (3P over Q and B)");
   CP_TRY(launch_dgt_ex(e, CQ, nullptr, &tq, CP_QBASE, 3 * npairs, 0, true, st));
   InvSrc tb{};
   for (int v = 0; v < 4; ++v) tb.p[v] = XB + v * P * be;
   tb.mode = 1;
   tb.npairs = npairs;
+  tb.untwist = 1;
   CP_TRY(launch_dgt_ex(e, CB, nullptr, &tb, CP_BBASE, 3 * npairs, 0, true, st));
   // 4. round(t X / Q) and B -> Q, then forward DGT of the outputs
   NvtxRange r4("scale t/Q, B -> Q, forward DGT over Q (3P)");
-  CP_TRY(hps_scale_to_q(e, c, CQ, CB, U, 3 * npairs, st));
+  CP_TRY(hps_scale_to_q_pre(e, c, CQ, CB, U, 3 * npairs, st));
   return launch_dgt(e, c, CP_QBASE, 3 * npairs, 0, false, st);
 }
 

@@ -204,7 +204,15 @@ int run_transform(const Engine& e, ulonglong2* data, const ulonglong2* fsrc, con
                   int rid_off, int npolys, long long poly_stride, bool inverse, cudaStream_t st, const int* rid_list) {
   const PlanSel ps = select_plan(e, (long long)npolys * nres);
   const DgtPlan& P = ps.P;
-  const DgtTableLayout& L = ps.L;
+  DgtTableLayout Lsel = ps.L;
+  if (inverse && isrc.untwist > 0) {  // a prescaled untwist table (off_untwist_pre)
+    if (isrc.untwist > 2) {
+      set_error("dgt: unknown untwist table");
+      return 1;
+    }
+    Lsel.off_untwist = Lsel.off_untwist_pre[isrc.untwist - 1];
+  }
+  const DgtTableLayout& L = Lsel;
   RunFn fn = pick(P.logNc, P.logR);
   if (!fn) {
     set_error("dgt: no kernel for this size");

@@ -49,6 +49,12 @@ struct DgtTableLayout {
   int off_split_inv = 0;
   int off_twist = 0;                    // 3N entries: xi^n as (re, im - re, re + im), Shoup pairs
   int off_untwist = 0;                  // 3N entries: xi^-n N^-1, same form
+  // 3N entries each: xi^-n N^-1 times a per-residue factor, so that an inverse transform
+  // also applies the first constant product of the base conversion that reads its output
+  // (BFV engines; used by the batched multiplication chain):
+  //   [0]: Q residue i: (Q/q_i)^-1 mod q_i;  B residue j: t Q^-1 (B/b_j)^-1 mod b_j;
+  //   [1]: Q residue i: t (Q/q_i)^-1 mod q_i;  B residue j: 1.
+  int off_untwist_pre[2] = {0, 0};
   int stride = 0;                       // entries per residue block
 };
 
@@ -70,10 +76,13 @@ struct DgtArgs {
 //  mode 3: product: the Gaussian product p[0] * p[1] (both in the output's
 //          layout), formed while loading -- pointwise multiply fused into the
 //          inverse transform.
+// `untwist` picks the untwist table of the inverse: 0 the plain xi^-n N^-1, 1 or 2
+// off_untwist_pre[untwist - 1].
 struct InvSrc {
   const ulonglong2* p[4];
   int mode;
   int npairs;
+  int untwist;
 };
 
 // Mixed-radix conversion constants of one (source base -> targets) pair.
@@ -143,6 +152,13 @@ struct Engine {
     int fb_hmod;                   // (B/b_j) mod q_i, [i][j]
     int fb_negv;                   // (-v B) mod q_i, [i][v], v in [0, kl]
     int fb_invd;                   // 1/b_j as double bits, [j]
+    // conversions of prescaled inputs (the untwist tables off_untwist_pre); the recovery
+    // factors undo the prescaling for coefficients that take the exact path
+    int fq_trec, fq_trec_s;        // (t (Q/q_i)^-1)^-1 mod q_i, [i]
+    int fb_rec, fb_rec_s;          // (B/b_j) mod b_j, [j]
+    int cs_brec, cs_brec_s;        // (t Q^-1 (B/b_j)^-1)^-1 mod b_j, [j]
+    int cs_hm2;                    // q_i^-1 (B/b_j)^-1 mod b_j, [j][i]
+    int cs_negw2;                  // (-w (B/b_j)^-1) mod b_j, [j][w], w in [0, k]
     int pow64;                     // 2^(64 l) mod p_r, [residue][kMaxLimbs]
     int pow64m;                    // 2^(64 (l + 1)) mod p_r (Montgomery form of pow64), same shape
     // CKKS (only when ckks_prec != 0); every constant with its Shoup companion
@@ -157,6 +173,7 @@ struct Engine {
   uint64_t t_shoup_one = 0;        // floor(2^64 / t)
   uint64_t h_q_mod_t = 0, h_qinv_t = 0, h_qinv_t_s = 0;  // Q mod t, Q^-1 mod t
   int* d_err = nullptr;            // device-side error flag (sampler rejection exhaustion)
+  int hps_force_exact = 0;         // 1: every base conversion and scaling takes its exact path (tests)
 
   int n_residues(int base) const;
   int rid_offset(int base) const;

@@ -179,19 +179,24 @@ struct ConvArgs {
   const uint64_t* pm;  // mixed-radix weights [target][source]
   const uint64_t *W, *pinv, *pinv_s;  // Garner constants of the source base
   const uint64_t* lift;               // MRC digits of the source base's lift threshold minus one
+  const uint64_t *rec, *rec_s;        // prescaled inputs y_i = x_i (S/s_i)^-1: x_i = y_i (S/s_i)
+  int force_exact;                    // 1: every coefficient takes the exact path
   int src_off, dst_off, ndst, N;
   long long in_stride, out_stride;  // per polynomial, in elements
 };
 
 // Exact path of one coefficient (component comp of element j): mixed-radix
 // digits, then one dot product per target.
+// With `prescaled`, the inputs are y_i = x_i (S/s_i)^-1 and x_i is recovered first.
 template <int NS>
-__device__ __noinline__ void ext_exact(uint64_t* ow, const uint64_t* iw, int j, int comp, const ConvArgs& a) {
+__device__ __noinline__ void ext_exact(uint64_t* ow, const uint64_t* iw, int j, int comp, const ConvArgs& a,
+                                       bool prescaled = false) {
   uint64_t s[NS], d[NS];
 #pragma unroll
   for (int i = 0; i < NS; ++i) {
     s[i] = a.mc[a.src_off + i].p;
     d[i] = iw[2 * ((size_t)i * a.N + j) + comp];
+    if (prescaled) d[i] = shoup_mul(d[i], __ldg(a.rec + i), __ldg(a.rec_s + i), s[i]);
   }
   mrc_any<NS>(d, s, a.inv, a.inv_s, a.mc + a.src_off, a.W, a.pinv, a.pinv_s);
   const bool neg = above_half<NS>(d, a.lift);  // cuPoly's lift: X - S
@@ -206,7 +211,7 @@ __device__ __noinline__ void ext_exact(uint64_t* ow, const uint64_t* iw, int j, 
 // X mod m_j for every target j; one thread per Gaussian element (2 coefficients).
 template <int NS>
 __global__ void __launch_bounds__(128) k_basis_ext(ulonglong2* __restrict__ out, const ulonglong2* __restrict__ in,
-                                                   ConvArgs a) {
+                                                   const __grid_constant__ ConvArgs a) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.N) return;
   const uint64_t* iw = reinterpret_cast<const uint64_t*>(in + blockIdx.y * a.in_stride);
@@ -245,7 +250,7 @@ __global__ void __launch_bounds__(128) k_basis_ext(ulonglong2* __restrict__ out,
     bool ab, nr, ni;
     const bool okr = fast_v<NS>(yr, a.f.invd, false, vr, ab, true, &nr);
     const bool oki = fast_v<NS>(yi, a.f.invd, false, vi, ab, true, &ni);
-    if (okr && oki) {
+    if (okr && oki && !a.force_exact) {
       vr += nr ? 1 : 0;  // cuPoly's lift: X - S
       vi += ni ? 1 : 0;
       for (int t = 0; t < a.ndst; ++t) {
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(128) k_basis_ext(ulonglong2* __restrict__ out,
                          a.mc[a.src_off + i].p);
       int v;
       bool above, neg;
-      if (fast_v<NS>(y, a.f.invd, false, v, above, true, &neg)) {
+      if (!a.force_exact && fast_v<NS>(y, a.f.invd, false, v, above, true, &neg)) {
         v += neg ? 1 : 0;  // cuPoly's lift: X - S
         for (int t = 0; t < a.ndst; ++t)
           ow[2 * ((size_t)t * a.N + j) + comp] =
@@ -281,12 +286,74 @@ __global__ void __launch_bounds__(128) k_basis_ext(ulonglong2* __restrict__ out,
   }
 }
 
+// X mod m_j from prescaled inputs y_i = x_i (S/s_i)^-1 mod s_i, which an inverse DGT with
+// an off_untwist_pre table leaves: the fast path starts at its FP64 sum for every base
+// size (no constant product before it, and no mixed-radix digits for small bases); a
+// coefficient it cannot decide recovers x_i and takes the exact path.
+template <int NS>
+__global__ void __launch_bounds__(128) k_basis_ext_pre(ulonglong2* __restrict__ out, const ulonglong2* __restrict__ in,
+                                                       const __grid_constant__ ConvArgs a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.N) return;
+  const uint64_t* iw = reinterpret_cast<const uint64_t*>(in + blockIdx.y * a.in_stride);
+  uint64_t* ow = reinterpret_cast<uint64_t*>(out + blockIdx.y * a.out_stride);
+  if constexpr (NS < 8) {  // small bases: both coefficients together (ILP)
+    uint64_t yr[NS], yi[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+      const ulonglong2 x = in[blockIdx.y * a.in_stride + (size_t)i * a.N + j];
+      yr[i] = x.x;
+      yi[i] = x.y;
+    }
+    int vr, vi;
+    bool ab, nr, ni;
+    const bool okr = fast_v<NS>(yr, a.f.invd, false, vr, ab, true, &nr);
+    const bool oki = fast_v<NS>(yi, a.f.invd, false, vi, ab, true, &ni);
+    if (okr && oki && !a.force_exact) {
+      vr += nr ? 1 : 0;  // cuPoly's lift: X - S
+      vi += ni ? 1 : 0;
+      for (int t = 0; t < a.ndst; ++t) {
+        const ModConst mt = a.mc[a.dst_off + t];
+        const uint64_t* hm = a.f.hmod + t * NS;
+        const uint64_t* nv = a.f.negv + t * (NS + 1);
+        out[blockIdx.y * a.out_stride + (size_t)t * a.N + j] =
+            make_ulonglong2(fast_dot<NS>(yr, hm, __ldg(nv + vr), mt), fast_dot<NS>(yi, hm, __ldg(nv + vi), mt));
+      }
+    } else {
+      ext_exact<NS>(ow, iw, j, 0, a, true);
+      ext_exact<NS>(ow, iw, j, 1, a, true);
+    }
+  } else {  // large bases: one coefficient at a time (registers)
+#pragma unroll 1
+    for (int comp = 0; comp < 2; ++comp) {
+      uint64_t y[NS];
+#pragma unroll
+      for (int i = 0; i < NS; ++i) y[i] = iw[2 * ((size_t)i * a.N + j) + comp];
+      int v;
+      bool above, neg;
+      if (!a.force_exact && fast_v<NS>(y, a.f.invd, false, v, above, true, &neg)) {
+        v += neg ? 1 : 0;  // cuPoly's lift: X - S
+        for (int t = 0; t < a.ndst; ++t)
+          ow[2 * ((size_t)t * a.N + j) + comp] =
+              fast_dot<NS>(y, a.f.hmod + t * NS, __ldg(a.f.negv + t * (NS + 1) + v), a.mc[a.dst_off + t]);
+      } else {
+        ext_exact<NS>(ow, iw, j, comp, a, true);
+      }
+    }
+  }
+}
+
 struct ScaleArgs {
   Fast fq;  // Q side of the fast path, t folded into hinv
   const ModConst* mc;
   const uint64_t *inv, *inv_s, *hor, *hor_s, *half, *pm;
   const uint64_t *W, *pinv, *pinv_s;  // Garner constants of Q
   const uint64_t *t_q, *t_q_s, *t_b, *t_b_s, *q_mod_b, *qinv_b, *qinv_b_s;
+  // prescaled inputs (k_complex_scaling_pre): Q side y_i = t x_i (Q/q_i)^-1, B side
+  // y'_j = t Q^-1 (B/b_j)^-1 y_j; the output is z_j (B/b_j)^-1, the B -> Q conversion's
+  // prescaled input
+  const uint64_t *trec, *trec_s, *brec, *brec_s, *bhinv, *bhinv_s, *hm2, *negw2;
+  int force_exact;
   int k, kl, N;
   long long q_stride, b_stride, out_stride;
 };
@@ -317,7 +384,8 @@ __device__ __noinline__ void scale_exact_write(uint64_t* ow, const uint64_t* qw,
 template <int NQ>
 __global__ void __launch_bounds__(128) k_complex_scaling(ulonglong2* __restrict__ out_b,
                                                          const ulonglong2* __restrict__ in_q,
-                                                         const ulonglong2* __restrict__ in_b, ScaleArgs a) {
+                                                         const ulonglong2* __restrict__ in_b,
+                                                         const __grid_constant__ ScaleArgs a) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.N) return;
   const uint64_t* qw = reinterpret_cast<const uint64_t*>(in_q + blockIdx.y * a.q_stride);
@@ -367,7 +435,7 @@ __global__ void __launch_bounds__(128) k_complex_scaling(ulonglong2* __restrict_
     bool ar, ai;
     const bool okr = fast_v<NQ>(yr, a.fq.invd, true, vr, ar);
     const bool oki = fast_v<NQ>(yi, a.fq.invd, true, vi, ai);
-    if (okr && oki) {
+    if (okr && oki && !a.force_exact) {
       const int wr = vr + (ar ? 1 : 0), wi = vi + (ai ? 1 : 0);
       for (int t = 0; t < a.kl; ++t) {
         const ModConst mt = a.mc[a.k + t];
@@ -396,7 +464,7 @@ __global__ void __launch_bounds__(128) k_complex_scaling(ulonglong2* __restrict_
         y[i] = shoup_mul(qw[2 * ((size_t)i * a.N + j) + comp], __ldg(a.fq.hinv + i), __ldg(a.fq.hinv_s + i), a.mc[i].p);
       int v;
       bool above;
-      if (fast_v<NQ>(y, a.fq.invd, true, v, above)) {
+      if (!a.force_exact && fast_v<NQ>(y, a.fq.invd, true, v, above)) {
         const int w = v + (above ? 1 : 0);
         for (int t = 0; t < a.kl; ++t) {
           const ModConst mt = a.mc[a.k + t];
@@ -407,6 +475,95 @@ __global__ void __launch_bounds__(128) k_complex_scaling(ulonglong2* __restrict_
         }
       } else {
         scale_exact_write<NQ>(ow, qw, bw, j, comp, a);
+      }
+    }
+  }
+}
+
+// Exact path of the prescaled complex scaling for one coefficient: recover x_i and y_j,
+// round(t X / Q) mod b_j as scale_exact_write, then times (B/b_j)^-1.
+template <int NQ>
+__device__ __noinline__ void scale_exact_pre_write(uint64_t* ow, const uint64_t* qw, const uint64_t* bw, int j,
+                                                   int comp, const ScaleArgs& a) {
+  uint64_t s[NQ], d[NQ];
+#pragma unroll
+  for (int i = 0; i < NQ; ++i) {
+    s[i] = a.mc[i].p;
+    const uint64_t x = shoup_mul(qw[2 * ((size_t)i * a.N + j) + comp], __ldg(a.trec + i), __ldg(a.trec_s + i), s[i]);
+    d[i] = shoup_mul(x, __ldg(a.t_q + i), __ldg(a.t_q_s + i), s[i]);
+  }
+  mrc_any<NQ>(d, s, a.inv, a.inv_s, a.mc, a.W, a.pinv, a.pinv_s);
+  const bool neg = above_half<NQ>(d, a.half);
+  for (int t = 0; t < a.kl; ++t) {
+    const ModConst mt = a.mc[a.k + t];
+    const uint64_t b = mt.p;
+    uint64_t r = dot_mod<NQ>(d, a.pm + t * NQ, mt);
+    if (neg) r = sub_mod(r, __ldg(a.q_mod_b + t), b);
+    const uint64_t y = shoup_mul(bw[2 * ((size_t)t * a.N + j) + comp], __ldg(a.brec + t), __ldg(a.brec_s + t), b);
+    const uint64_t ty = shoup_mul(y, __ldg(a.t_b + t), __ldg(a.t_b_s + t), b);
+    const uint64_t z = shoup_mul(ty + b - r, __ldg(a.qinv_b + t), __ldg(a.qinv_b_s + t), b);
+    ow[2 * ((size_t)t * a.N + j) + comp] = shoup_mul(z, __ldg(a.bhinv + t), __ldg(a.bhinv_s + t), b);
+  }
+}
+
+// round(t X / Q) (B/b_j)^-1 mod b_j from prescaled inputs (see ScaleArgs): with w the
+// centred overflow count, [t X mod Q centred] Q^-1 (B/b_j)^-1 = sum_i y_i q_i^-1 (B/b_j)^-1 -
+// w (B/b_j)^-1, so each output is y'_j minus one dot product -- no constant products.
+template <int NQ>
+__global__ void __launch_bounds__(128) k_complex_scaling_pre(ulonglong2* __restrict__ out_b,
+                                                             const ulonglong2* __restrict__ in_q,
+                                                             const ulonglong2* __restrict__ in_b,
+                                                             const __grid_constant__ ScaleArgs a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.N) return;
+  const uint64_t* qw = reinterpret_cast<const uint64_t*>(in_q + blockIdx.y * a.q_stride);
+  const uint64_t* bw = reinterpret_cast<const uint64_t*>(in_b + blockIdx.y * a.b_stride);
+  uint64_t* ow = reinterpret_cast<uint64_t*>(out_b + blockIdx.y * a.out_stride);
+  if constexpr (NQ < 8) {  // small bases: both coefficients together (ILP)
+    uint64_t yr[NQ], yi[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+      const ulonglong2 x = reinterpret_cast<const ulonglong2*>(qw)[(size_t)i * a.N + j];
+      yr[i] = x.x;
+      yi[i] = x.y;
+    }
+    int vr, vi;
+    bool ar, ai;
+    const bool okr = fast_v<NQ>(yr, a.fq.invd, true, vr, ar);
+    const bool oki = fast_v<NQ>(yi, a.fq.invd, true, vi, ai);
+    if (okr && oki && !a.force_exact) {
+      const int wr = vr + (ar ? 1 : 0), wi = vi + (ai ? 1 : 0);
+      for (int t = 0; t < a.kl; ++t) {
+        const ModConst mt = a.mc[a.k + t];
+        const uint64_t b = mt.p;
+        const uint64_t* hm = a.hm2 + t * NQ;
+        const uint64_t* nw = a.negw2 + t * (NQ + 1);
+        const uint64_t rr = fast_dot<NQ>(yr, hm, __ldg(nw + wr), mt);
+        const uint64_t ri = fast_dot<NQ>(yi, hm, __ldg(nw + wi), mt);
+        const ulonglong2 y = reinterpret_cast<const ulonglong2*>(bw)[(size_t)t * a.N + j];
+        reinterpret_cast<ulonglong2*>(ow)[(size_t)t * a.N + j] = make_ulonglong2(sub_mod(y.x, rr, b), sub_mod(y.y, ri, b));
+      }
+    } else {
+      scale_exact_pre_write<NQ>(ow, qw, bw, j, 0, a);
+      scale_exact_pre_write<NQ>(ow, qw, bw, j, 1, a);
+    }
+  } else {
+#pragma unroll 1
+    for (int comp = 0; comp < 2; ++comp) {
+      uint64_t y[NQ];
+#pragma unroll
+      for (int i = 0; i < NQ; ++i) y[i] = qw[2 * ((size_t)i * a.N + j) + comp];
+      int v;
+      bool above;
+      if (!a.force_exact && fast_v<NQ>(y, a.fq.invd, true, v, above)) {
+        const int w = v + (above ? 1 : 0);
+        for (int t = 0; t < a.kl; ++t) {
+          const ModConst mt = a.mc[a.k + t];
+          const uint64_t r = fast_dot<NQ>(y, a.hm2 + t * NQ, __ldg(a.negw2 + t * (NQ + 1) + w), mt);
+          ow[2 * ((size_t)t * a.N + j) + comp] = sub_mod(bw[2 * ((size_t)t * a.N + j) + comp], r, mt.p);
+        }
+      } else {
+        scale_exact_pre_write<NQ>(ow, qw, bw, j, comp, a);
       }
     }
   }
@@ -478,6 +635,19 @@ int launch_cs_n(ulonglong2* out, const ulonglong2* q, const ulonglong2* b, const
   k_complex_scaling<NQ><<<grid, 128, 0, st>>>(out, q, b, a);
   return check_launch("complex_scaling");
 }
+template <int NS>
+int launch_basis_ext_pre_n(ulonglong2* out, const ulonglong2* in, const ConvArgs& a, int npolys, cudaStream_t st) {
+  dim3 grid((a.N + 127) / 128, npolys);
+  k_basis_ext_pre<NS><<<grid, 128, 0, st>>>(out, in, a);
+  return check_launch("basis_ext_pre");
+}
+template <int NQ>
+int launch_cs_pre_n(ulonglong2* out, const ulonglong2* q, const ulonglong2* b, const ScaleArgs& a, int npolys,
+                    cudaStream_t st) {
+  dim3 grid((a.N + 127) / 128, npolys);
+  k_complex_scaling_pre<NQ><<<grid, 128, 0, st>>>(out, q, b, a);
+  return check_launch("complex_scaling_pre");
+}
 template <int NQ>
 int launch_ss_n(ulonglong2* out, const ulonglong2* q, const SimpleArgs& a, cudaStream_t st) {
   k_simple_scaling<NQ><<<(a.N + 127) / 128, 128, 0, st>>>(out, q, a);
@@ -498,9 +668,10 @@ int launch_ss_n(ulonglong2* out, const ulonglong2* q, const SimpleArgs& a, cudaS
 
 }  // namespace
 
-int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int npolys, cudaStream_t st) {
+static ConvArgs conv_args(const Engine& e, bool q_to_b) {
   ConvArgs a;
   a.mc = e.d_mc;
+  a.force_exact = e.hps_force_exact;
   a.N = e.N;
   if (q_to_b) {
     a.inv = e.d_hps + e.ho.qb_inv;
@@ -514,6 +685,8 @@ int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int n
     a.f = Fast{e.d_hps + e.ho.fq_hinv, e.d_hps + e.ho.fq_hinv_s, e.d_hps + e.ho.fq_hmod, e.d_hps + e.ho.fq_negv,
                e.d_hps + e.ho.fq_invd};
     a.lift = e.d_hps + e.ho.q_lift;
+    a.rec = e.d_hps + e.ho.rho_q;  // (Q/q_i) mod q_i
+    a.rec_s = e.d_hps + e.ho.rho_q_s;
     a.src_off = 0;
     a.dst_off = e.k;
     a.ndst = e.kl;
@@ -529,6 +702,8 @@ int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int n
     a.f = Fast{e.d_hps + e.ho.fb_hinv, e.d_hps + e.ho.fb_hinv_s, e.d_hps + e.ho.fb_hmod, e.d_hps + e.ho.fb_negv,
                e.d_hps + e.ho.fb_invd};
     a.lift = e.d_hps + e.ho.b_lift;
+    a.rec = e.d_hps + e.ho.fb_rec;  // (B/b_j) mod b_j
+    a.rec_s = e.d_hps + e.ho.fb_rec_s;
     a.src_off = e.k;
     a.dst_off = 0;
     a.ndst = e.k;
@@ -536,9 +711,25 @@ int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int n
   const int ns = q_to_b ? e.k : e.kl;
   a.in_stride = (long long)ns * e.N;
   a.out_stride = (long long)a.ndst * e.N;
+  return a;
+}
+
+int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int npolys, cudaStream_t st) {
+  const ConvArgs a = conv_args(e, q_to_b);
+  const int ns = q_to_b ? e.k : e.kl;
   auto* o = reinterpret_cast<ulonglong2*>(out);
   auto* i = reinterpret_cast<const ulonglong2*>(in);
 #define CALL(n) launch_basis_ext_n<n>(o, i, a, npolys, st)
+  CP_SWITCH_NS(ns, CALL)
+#undef CALL
+}
+
+int hps_basis_ext_pre(const Engine& e, void* out, const void* in, bool q_to_b, int npolys, cudaStream_t st) {
+  const ConvArgs a = conv_args(e, q_to_b);
+  const int ns = q_to_b ? e.k : e.kl;
+  auto* o = reinterpret_cast<ulonglong2*>(out);
+  auto* i = reinterpret_cast<const ulonglong2*>(in);
+#define CALL(n) launch_basis_ext_pre_n<n>(o, i, a, npolys, st)
   CP_SWITCH_NS(ns, CALL)
 #undef CALL
 }
@@ -564,6 +755,15 @@ static ScaleArgs scale_args(const Engine& e) {
   a.qinv_b_s = e.d_hps + e.ho.qinv_b_s;
   a.fq = Fast{e.d_hps + e.ho.fq_thinv, e.d_hps + e.ho.fq_thinv_s, e.d_hps + e.ho.fq_hmod, e.d_hps + e.ho.fq_negv,
               e.d_hps + e.ho.fq_invd};
+  a.trec = e.d_hps + e.ho.fq_trec;
+  a.trec_s = e.d_hps + e.ho.fq_trec_s;
+  a.brec = e.d_hps + e.ho.cs_brec;
+  a.brec_s = e.d_hps + e.ho.cs_brec_s;
+  a.bhinv = e.d_hps + e.ho.fb_hinv;
+  a.bhinv_s = e.d_hps + e.ho.fb_hinv_s;
+  a.hm2 = e.d_hps + e.ho.cs_hm2;
+  a.negw2 = e.d_hps + e.ho.cs_negw2;
+  a.force_exact = e.hps_force_exact;
   a.k = e.k;
   a.kl = e.kl;
   a.N = e.N;
@@ -595,6 +795,23 @@ int hps_scale_to_q(const Engine& e, void* out_q, const void* in_q, const void* i
   int rc = hps_complex_scaling(e, scratch_b, in_q, in_b, npolys, st);
   if (rc) return rc;
   return hps_basis_ext(e, out_q, scratch_b, false, npolys, st);
+}
+
+// The chain's form on prescaled inputs (the off_untwist_pre tables): in_q holds
+// t x_i (Q/q_i)^-1 mod q_i and in_b t Q^-1 (B/b_j)^-1 y_j mod b_j; out_q is round(t X / Q)
+// over Q in the coefficient domain.
+int hps_scale_to_q_pre(const Engine& e, void* out_q, const void* in_q, const void* in_b, void* scratch_b, int npolys,
+                       cudaStream_t st) {
+  const ScaleArgs a = scale_args(e);
+  auto* o = reinterpret_cast<ulonglong2*>(scratch_b);
+  auto* q = reinterpret_cast<const ulonglong2*>(in_q);
+  auto* b = reinterpret_cast<const ulonglong2*>(in_b);
+  int rc;
+#define CALL(n) launch_cs_pre_n<n>(o, q, b, a, npolys, st)
+  rc = [&]() -> int { CP_SWITCH_NS(e.k, CALL) }();
+#undef CALL
+  if (rc) return rc;
+  return hps_basis_ext_pre(e, out_q, scratch_b, false, npolys, st);
 }
 
 int hps_simple_scaling(const Engine& e, void* out_t, const void* in_q, cudaStream_t st) {

@@ -30,6 +30,12 @@ int pw_double_op_by_int(const Engine& e, void* b1, const void* a1, void* b2, con
 
 // HPS (coefficient domain, folded Gaussian layout)
 int hps_basis_ext(const Engine& e, void* out, const void* in, bool q_to_b, int npolys, cudaStream_t st);
+// prescaled inputs y_i = x_i (S/s_i)^-1 (an inverse DGT with untwist table off_untwist_pre[0])
+int hps_basis_ext_pre(const Engine& e, void* out, const void* in, bool q_to_b, int npolys, cudaStream_t st);
+// complex scaling and B -> Q of prescaled inputs (inverse DGTs with untwist tables
+// off_untwist_pre[1] over Q and off_untwist_pre[0] over B)
+int hps_scale_to_q_pre(const Engine& e, void* out_q, const void* in_q, const void* in_b, void* scratch_b, int npolys,
+                       cudaStream_t st);
 int hps_complex_scaling(const Engine& e, void* out_b, const void* in_q, const void* in_b, int npolys,
                         cudaStream_t st);
 int hps_scale_to_q(const Engine& e, void* out_q, const void* in_q, const void* in_b, void* scratch_b, int npolys,

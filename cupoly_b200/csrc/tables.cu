@@ -215,10 +215,37 @@ int build_tables(Engine& e) {
   off += 3 * N;
   L.off_untwist = off;
   off += 3 * N;
+  for (int v = 0; v < 2; ++v) {
+    L.off_untwist_pre[v] = off;
+    off += 3 * N;
+  }
   L.stride = (off + 1) & ~1;
   L2.off_twist = L.off_twist;
   L2.off_untwist = L.off_untwist;
+  L2.off_untwist_pre[0] = L.off_untwist_pre[0];
+  L2.off_untwist_pre[1] = L.off_untwist_pre[1];
   L2.stride = L.stride;
+
+  // Per-residue factors of the prescaled untwist tables (off_untwist_pre):
+  //   Q residue i: (Q/q_i)^-1 and t (Q/q_i)^-1 mod q_i;  B residue j: t Q^-1 (B/b_j)^-1 mod b_j and 1.
+  std::vector<uint64_t> pre0(nres, 1), pre1(nres, 1);
+  for (int r = 0; r < nres; ++r) {
+    const uint64_t p = e.primes[r];
+    const bool in_q = r < e.k;
+    const int lo = in_q ? 0 : e.k, hi = in_q ? e.k : nres;
+    uint64_t hat = 1 % p;  // S / s_r mod s_r, S the product of r's base
+    for (int u = lo; u < hi; ++u)
+      if (u != r) hat = h_mulmod(hat, e.primes[u] % p, p);
+    const uint64_t hinv = h_invmod(hat, p), tp = e.t % p;
+    if (in_q) {
+      pre0[r] = hinv;
+      pre1[r] = h_mulmod(tp, hinv, p);
+    } else {
+      uint64_t qm = 1 % p;
+      for (int u = 0; u < e.k; ++u) qm = h_mulmod(qm, e.primes[u] % p, p);
+      pre0[r] = h_mulmod(h_mulmod(tp, h_invmod(qm, p), p), hinv, p);
+    }
+  }
 
   std::vector<ulonglong2> tab((size_t)L.stride * nres);
   parallel_for(nres, [&](int r) {
@@ -278,9 +305,12 @@ int build_tables(Engine& e) {
       put(idx + 1, (w.im + p - w.re) % p);
       put(idx + 2, (uint64_t)(((unsigned __int128)w.re + w.im) % p));
     };
+    const uint64_t f0 = pre0[r], f1 = pre1[r];
     for (int n = 0; n < N; ++n) {
       put_gauss(L.off_twist + 3 * n, a);
       put_gauss(L.off_untwist + 3 * n, b);
+      put_gauss(L.off_untwist_pre[0] + 3 * n, G{h_mulmod(b.re, f0, p), h_mulmod(b.im, f0, p)});
+      put_gauss(L.off_untwist_pre[1] + 3 * n, G{h_mulmod(b.re, f1, p), h_mulmod(b.im, f1, p)});
       a = gmul(a, xi, p);
       b = gmul(b, xii, p);
     }
@@ -471,6 +501,41 @@ int build_tables(Engine& e) {
     fast(Q, B, true, e.ho.fq_hinv, e.ho.fq_hinv_s, &e.ho.fq_thinv, &e.ho.fq_thinv_s, e.ho.fq_hmod, e.ho.fq_negv,
          e.ho.fq_invd);
     fast(B, Q, false, e.ho.fb_hinv, e.ho.fb_hinv_s, nullptr, nullptr, e.ho.fb_hmod, e.ho.fb_negv, e.ho.fb_invd);
+  }
+  {
+    // conversions of prescaled inputs (the off_untwist_pre tables): recovery factors and the
+    // complex scaling's dot constants with Q^-1 (B/b_j)^-1 folded in
+    const size_t k = Q.size(), kl = B.size();
+    auto hat_mod = [&](const std::vector<uint64_t>& s, size_t i) {
+      uint64_t h = 1 % s[i];
+      for (size_t l = 0; l < s.size(); ++l)
+        if (l != i) h = h_mulmod(h, s[l] % s[i], s[i]);
+      return h;
+    };
+    std::vector<uint64_t> trec, trec_s, rec, rec_s, brec, brec_s, hm2, negw2;
+    for (size_t i = 0; i < k; ++i) {  // x_i = y_i (t (Q/q_i)^-1)^-1
+      const uint64_t q = Q[i];
+      const uint64_t th = h_mulmod(e.t % q, h_invmod(hat_mod(Q, i), q), q);
+      push_pair(h_invmod(th, q), q, trec, trec_s);
+    }
+    for (size_t j = 0; j < kl; ++j) {
+      const uint64_t b = B[j];
+      const uint64_t bh = hat_mod(B, j), bhi = h_invmod(bh, b);
+      push_pair(bh, b, rec, rec_s);  // z_j = zhat_j (B/b_j)
+      const uint64_t qinv = h_invmod(prod_mod(Q, b), b);
+      const uint64_t f = h_mulmod(h_mulmod(e.t % b, qinv, b), bhi, b);  // t Q^-1 (B/b_j)^-1
+      push_pair(h_invmod(f, b), b, brec, brec_s);
+      for (size_t i = 0; i < k; ++i) hm2.push_back(h_mulmod(h_invmod(Q[i] % b, b), bhi, b));
+      for (size_t w = 0; w <= k; ++w) negw2.push_back((b - h_mulmod(w % b, bhi, b)) % b);
+    }
+    e.ho.fq_trec = append(trec);
+    e.ho.fq_trec_s = append(trec_s);
+    e.ho.fb_rec = append(rec);
+    e.ho.fb_rec_s = append(rec_s);
+    e.ho.cs_brec = append(brec);
+    e.ho.cs_brec_s = append(brec_s);
+    e.ho.cs_hm2 = append(hm2);
+    e.ho.cs_negw2 = append(negw2);
   }
   {
     std::vector<uint64_t> v;  // 2^(64 l) mod p_r for the limb-to-residue conversion

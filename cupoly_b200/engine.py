@@ -147,6 +147,10 @@ class Engine:
         """0: split stage as its own kernel (HBM pass); 1: inside a thread-block cluster (DSMEM)."""
         call("cp_engine_set_split_mode", self._h, int(mode))
 
+    def set_hps_force_exact(self, on: bool):
+        """Diagnostic: every base conversion and scaling takes its exact path (same results)."""
+        call("cp_engine_set_hps_force_exact", self._h, 1 if on else 0)
+
     def get_split_mode(self) -> int:
         return int(_lib.lib().cp_engine_get_split_mode(self._h))
 

@@ -110,6 +110,11 @@ int cp_engine_get_narrow_plan(const cp_engine* e, int* log_radix, int* log_cta, 
  *     for the plan or the device cannot co-schedule the cluster, mode 1 falls back to 0. */
 int cp_engine_set_split_mode(cp_engine* e, int mode);
 int cp_engine_get_split_mode(const cp_engine* e);
+/* Diagnostic switch (no counterpart in cuPoly): 1 makes every base conversion and scaling
+ * take its exact mixed-radix path instead of the FP64 fast path, 0 (default) restores it.
+ * Results are identical either way; the tests use it to drive the exact paths on ordinary
+ * inputs.  Synchronises the device. */
+int cp_engine_set_hps_force_exact(cp_engine* e, int on);
 int cp_engine_destroy(cp_engine* e);
 int cp_engine_n_residues(const cp_engine* e, int base);
 int cp_engine_nphi(const cp_engine* e);

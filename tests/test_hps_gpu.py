@@ -366,3 +366,50 @@ def test_bfv_mul_batch_at_the_large_configurations_vs_oracle(gpu, k, nphi, t, np
     ref = CO.bfv_mul(*rows, e.Q, e.B, t)
     for j in range(3):
         assert np.array_equal(got[j * npairs:(j + 1) * npairs], ref[j]), (j, k, nphi)
+
+
+@pytest.mark.parametrize("k,nphi,t,npairs", [(1, 2048, 256, 3), (5, 8192, 256, 2), (7, 4096, 65537, 2),
+                                             (10, 16384, 3, 1)])
+def test_bfv_mul_exact_paths_vs_oracle(gpu, k, nphi, t, npairs):
+    """Every base conversion and scaling forced onto its exact path: the batched chain (whose
+    inverse transforms leave prescaled values for the conversions, undone on that path) and the
+    per-call chain still equal the oracle, and so do the plain conversions."""
+    import torch
+    from cupoly_b200.engine import FORWARD, INVERSE, Engine
+    e = Engine(k, 0, nphi, t)
+    rows = [np.stack([random_poly_residues(700 + 10 * i + j, e.Q, nphi) for i in range(npairs)]) for j in range(4)]
+    dev = []
+    for r in rows:
+        d = _dev(fold(r))
+        e.dgt(d, 0, FORWARD)
+        dev.append(d)
+    fast = e.empty(0, 3 * npairs)
+    e.bfv_mul_batch(fast, *dev, npairs, e.bfv_mul_batch_workspace(npairs))
+    e.set_hps_force_exact(True)
+    try:
+        c = e.empty(0, 3 * npairs)
+        e.bfv_mul_batch(c, *dev, npairs, e.bfv_mul_batch_workspace(npairs))
+        outs = [e.empty(0) for _ in range(3)]
+        e.bfv_mul(*outs, *[d[:1] for d in dev])
+        xq = rows[0][0]
+        ob = e.empty(1)
+        e.basis_ext_q_to_b(ob, _dev(fold(xq)[None]))
+        yb = random_poly_residues(701, e.B, nphi)
+        oq = e.empty(0)
+        e.basis_ext_b_to_q(oq, _dev(fold(yb)[None]))
+        cs = e.empty(1)
+        e.complex_scaling(cs, _dev(fold(xq)[None]), _dev(fold(yb)[None]))
+        torch.cuda.synchronize()
+    finally:
+        e.set_hps_force_exact(False)
+    assert torch.equal(fast, c)
+    for j in range(3):
+        assert torch.equal(outs[j][0], c[j * npairs])
+    e.dgt(c, 0, INVERSE)
+    got = unfold(_host(c))
+    ref = CO.bfv_mul(*rows, e.Q, e.B, t)
+    for j in range(3):
+        assert np.array_equal(got[j * npairs:(j + 1) * npairs], ref[j]), (j, k, nphi)
+    assert np.array_equal(unfold(_host(ob))[0], CO.basis_ext(xq, e.Q, e.B))
+    assert np.array_equal(unfold(_host(oq))[0], CO.basis_ext(yb, e.B, e.Q))
+    assert np.array_equal(unfold(_host(cs))[0], CO.complex_scaling(xq, yb, e.Q, e.B, t))
