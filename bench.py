@@ -399,6 +399,26 @@ def next_rows(seed: int, hbm_peak: float):
     return out
 
 
+# Integer-pipe use of the hot kernels, from ncu captures of the same kernels on a B200
+# (sm__pipe_fmaheavy / sm__pipe_alu cycles active and sm__issue_active, % of peak sustained
+# active).  Both 64-bit-integer pipes are half rate; the busier one is the integer roofline.
+INT_COUNTERS = {
+    "source": "ncu capture",
+    "kernels": {
+        "k_dgt_fwd<12,3,0>": {"workload": "forward DGT over B, nphi 8192, 3072 residues",
+                              "fmaheavy_pct": 68.5, "alu_pct": 51.9, "issue_pct": 55.3, "busier_pipe_frac": 0.685},
+        "k_dgt_inv<12,3,0>": {"workload": "the chain's inverse DGTs over Q (gather, tensor), nphi 8192",
+                              "fmaheavy_pct": 70.4, "alu_pct": 54.9, "issue_pct": 57.3, "busier_pipe_frac": 0.704},
+        "k_basis_ext_pre<5>": {"workload": "the chain's Q -> B conversion, 512 polynomials",
+                               "fmaheavy_pct": 70.9, "alu_pct": 64.8, "issue_pct": 63.8, "busier_pipe_frac": 0.709},
+        "k_dgt_inv<11,3,0> products on load": {"workload": "fused polymul, nphi 4096, k 2, 2048 products",
+                                               "fmaheavy_pct": 72.7, "alu_pct": 61.0, "issue_pct": 60.6,
+                                               "busier_pipe_frac": 0.727},
+        "k_polymul_tiles": {"workload": "mixed batch of 1024 products, one launch",
+                            "fmaheavy_pct": 64.7, "alu_pct": 50.9, "issue_pct": 52.1, "busier_pipe_frac": 0.647},
+    },
+}
+
 CUPOLY_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cupoly_ref_driver")
 PERCALL = os.path.join(ROOT, "cupoly_b200", "lib", "cupoly_percall")
 
@@ -602,7 +622,9 @@ def run_ours(args, D: Dist):
                 "shoup_per_launch": ops["shoup"] * nres_launch, "addmod_per_launch": ops["addmod"] * nres_launch,
                 "peak_shoup_per_s": round(peaks_int["shoup"], 1), "peak_addmod_per_s": round(peaks_int["addmod"], 1),
                 "peak_mulmod_per_s": round(peaks_int["mulmod"], 1), "peak_imad32_per_s": round(peaks_int["imad32"], 1),
-                "note": "frac = (Shoup / peak Shoup + adds / peak add) / measured; peaks measured live by cp_calibrate_int"}
+                "note": "frac = (Shoup / peak Shoup + adds / peak add) / measured; peaks measured live by cp_calibrate_int",
+                "counters": INT_COUNTERS,
+                "frac_counter": INT_COUNTERS["kernels"]["k_dgt_fwd<12,3,0>"]["busier_pipe_frac"]}
 
     # ---- polymul/s of the nphi = 4096, k = 2 configuration (batched) ----
     e1 = Engine(2, 3, 4096, 256)

@@ -22,10 +22,11 @@
 // y_i = x_i (S/s_i)^-1 mod s_i, sum_i y_i / s_i = v + X/S for X in [0, S), so
 // X mod m = sum_i y_i (S/s_i) - v S (mod m) -- s Shoup products instead of the
 // s(s-1)/2 of the mixed-radix digits.  v and the side of 1/2 of X/S (the
-// centring) come from an FP64 sum on the otherwise idle FP64 pipe, whose error
-// is below 2^-43; they are used only when the fraction lies at least 2^-36
-// from 0, 1 and 1/2.  Otherwise that coefficient takes the exact mixed-radix
-// path, so every result is exact either way.
+// centring) come from an FP64 sum on the FP64 pipe, whose error is below
+// 2^-43; they are used only when the fraction lies at least 2^-36 from the cut
+// the caller applies (1/2 for the centring, 1 - FPERROR for cuPoly's lift; see
+// fast_v).  Otherwise that coefficient takes the exact mixed-radix path, so
+// every result is exact either way.
 #include "launch.cuh"
 #include "pointwise.cuh"
 
@@ -140,6 +141,15 @@ __device__ __forceinline__ double u32_to_double(uint32_t x) {  // exact, FP64 pi
 // lift_threshold_digits in tables.cu); this is the fraction side of that test.
 constexpr double kLiftFrac = 1.0 - 1e-9;
 
+// Which integer the callers take from the sum f = v + X/S: w = v + [X/S >= c] with the cut
+// c = 1/2 (centring, `half`) or c = kLiftFrac (cuPoly's lift).  Either way w is the integer
+// floor(f + 1 - c), so an error in f moves w only where f + 1 - c lies near an integer, that
+// is where the fraction of f lies near c.  Near 0 and near 1 it does not: a fraction just
+// below 1 read where the true one is just above 0 (or the reverse) changes floor(f) by one
+// and the side of c the other way, and w is the same.  The BFV chain's B -> Q conversion,
+// whose values are small signed integers (fractions within 2^-40 of 0 or 1), therefore takes
+// the fast path.
+
 template <int NS>
 __device__ __forceinline__ bool fast_v(const uint64_t (&y)[NS], const uint64_t* __restrict__ invd, bool half, int& v,
                                        bool& above, bool lift = false, bool* neg = nullptr) {
@@ -156,7 +166,8 @@ __device__ __forceinline__ bool fast_v(const uint64_t (&y)[NS], const uint64_t* 
   above = fr >= 0.5;
   const double d = 0x1p-36;
   if (lift) *neg = fr > kLiftFrac;
-  return fr > d && fr < 1.0 - d && (!half || fabs(fr - 0.5) > d) && (!lift || fabs(fr - kLiftFrac) > d);
+  if (!half && !lift) return fr > d && fr < 1.0 - d;  // a plain floor is uncertain near integers
+  return (!half || fabs(fr - 0.5) > d) && (!lift || fabs(fr - kLiftFrac) > d);
 }
 
 // (sum_i y_i hmod_i + negv) mod m: lazy 192-bit sum (< 25 * 2^126), one reduction.
