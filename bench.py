@@ -407,12 +407,17 @@ INT_COUNTERS = {
     "kernels": {
         "k_dgt_fwd<12,3,0>": {"workload": "forward DGT over B, nphi 8192, 3072 residues",
                               "fmaheavy_pct": 68.5, "alu_pct": 51.9, "issue_pct": 55.3, "busier_pipe_frac": 0.685},
-        "k_dgt_inv<12,3,0>": {"workload": "the chain's inverse DGTs over Q (gather, tensor), nphi 8192",
+        "k_dgt_inv<12,3,0>": {"workload": "the chain's inverse DGT over Q (gather), nphi 8192",
                               "fmaheavy_pct": 70.4, "alu_pct": 54.9, "issue_pct": 57.3, "busier_pipe_frac": 0.704},
         "k_basis_ext_pre<5>": {"workload": "the chain's Q -> B conversion, 512 polynomials",
-                               "fmaheavy_pct": 70.9, "alu_pct": 64.8, "issue_pct": 63.8, "busier_pipe_frac": 0.709},
+                               "fmaheavy_pct": 70.5, "alu_pct": 65.1, "issue_pct": 63.5, "busier_pipe_frac": 0.705},
+        "k_complex_scaling_pre<5>": {"workload": "the chain's complex scaling, 384 polynomials",
+                                     "fmaheavy_pct": 61.2, "alu_pct": 68.0, "issue_pct": 60.8,
+                                     "busier_pipe_frac": 0.680},
+        "k_basis_ext_pre<6>": {"workload": "the chain's B -> Q conversion, 384 polynomials",
+                               "fmaheavy_pct": 67.8, "alu_pct": 64.4, "issue_pct": 62.1, "busier_pipe_frac": 0.678},
         "k_dgt_inv<11,3,0> products on load": {"workload": "fused polymul, nphi 4096, k 2, 2048 products",
-                                               "fmaheavy_pct": 72.7, "alu_pct": 61.0, "issue_pct": 60.6,
+                                               "fmaheavy_pct": 72.7, "alu_pct": 59.0, "issue_pct": 60.0,
                                                "busier_pipe_frac": 0.727},
         "k_polymul_tiles": {"workload": "mixed batch of 1024 products, one launch",
                             "fmaheavy_pct": 64.7, "alu_pct": 50.9, "issue_pct": 52.1, "busier_pipe_frac": 0.647},
