@@ -68,7 +68,10 @@ __device__ __forceinline__ void stage_twiddles(ulonglong2* stw, const ulonglong2
 
 // In-register 2^W-point Gentleman-Sande DIF (natural in, bit-reversed out).
 // rad[j] = w_R^j, R = 2^LOGR; the 2^W-point root is w_R^(2^(LOGR-W)).
-template <int W, int LOGR>
+// LAZY: every output but the first goes straight into a Shoup product (the pass
+// twiddle), which takes any value below 2^64, so the last stage leaves those in
+// [0, 2p) without the final correction.
+template <int W, int LOGR, bool LAZY = false>
 __device__ __forceinline__ void dif_regs(uint64_t* xr, uint64_t* xi, const ulonglong2* rad, uint64_t p) {
 #pragma unroll
   for (int s = 0; s < W; ++s) {
@@ -78,6 +81,13 @@ __device__ __forceinline__ void dif_regs(uint64_t* xr, uint64_t* xi, const ulong
       if ((i & m) == 0) {
         const int j = i & (m - 1);
         const uint64_t ar = xr[i], ai = xi[i], br = xr[i + m], bi = xi[i + m];
+        if (LAZY && s == W - 1) {
+          xr[i] = i == 0 ? add_mod(ar, br, p) : ar + br;
+          xi[i] = i == 0 ? add_mod(ai, bi, p) : ai + bi;
+          xr[i + m] = ar + p - br;
+          xi[i + m] = ai + p - bi;
+          continue;
+        }
         xr[i] = add_mod(ar, br, p);
         xi[i] = add_mod(ai, bi, p);
         if (j == 0) {
@@ -95,7 +105,10 @@ __device__ __forceinline__ void dif_regs(uint64_t* xr, uint64_t* xi, const ulong
 
 // In-register 2^W-point Cooley-Tukey DIT with inverse roots (bit-reversed in,
 // natural out), unscaled.
-template <int W, int LOGR>
+// LAZY: the outputs go to the next inverse pass, which reduces the one element it
+// does not multiply by a twiddle (lazy_in) and feeds the rest to Shoup products;
+// so the last stage leaves every output in [0, 2p) without the final correction.
+template <int W, int LOGR, bool LAZY = false>
 __device__ __forceinline__ void dit_regs(uint64_t* xr, uint64_t* xi, const ulonglong2* rad, uint64_t p) {
   constexpr int R = 1 << LOGR;
 #pragma unroll
@@ -111,6 +124,13 @@ __device__ __forceinline__ void dit_regs(uint64_t* xr, uint64_t* xi, const ulong
           const ulonglong2 w = rad[R - ((j << s) << (LOGR - W))];
           br = shoup_mul(br, w.x, w.y, p);
           bi = shoup_mul(bi, w.x, w.y, p);
+        }
+        if (LAZY && s == 0) {
+          xr[i] = ar + br;
+          xi[i] = ai + bi;
+          xr[i + m] = ar + p - br;
+          xi[i + m] = ai + p - bi;
+          continue;
         }
         xr[i] = add_mod(ar, br, p);
         xi[i] = add_mod(ai, bi, p);
@@ -162,7 +182,7 @@ __device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* s
       xr[v] = a.x;
       xi[v] = a.y;
     }
-    dif_regs<LOGR, LOGR>(xr, xi, srad, p);
+    dif_regs<LOGR, LOGR, (PF > 0)>(xr, xi, srad, p);
     if constexpr (PF > 0) {
       const ulonglong2* tw = C::staged(I) ? stw + C::soff(I) + Lw : tab + L.off_fwd[I] + Lw;
 #pragma unroll
@@ -205,7 +225,11 @@ __device__ __forceinline__ void inv_passes(ulonglong2* sdat, const ulonglong2* s
         xi[v] = shoup_mul(xi[v], w.x, w.y, p);
       }
     }
-    dit_regs<LOGR, LOGR>(xr, xi, srad, p);
+    if constexpr (I < C::NP - 1) {  // written by a lazy pass (I + 1)
+      xr[0] = red2p(xr[0], p);
+      xi[0] = red2p(xi[0], p);
+    }
+    dit_regs<LOGR, LOGR, true>(xr, xi, srad, p);
 #pragma unroll
     for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
     __syncthreads();
@@ -414,7 +438,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
         xr[g * (1 << W) + v] = ar;
         xi[g * (1 << W) + v] = ai;
       }
-      dif_regs<W, LOGR>(xr + g * (1 << W), xi + g * (1 << W), srad, p);
+      dif_regs<W, LOGR, (PF > 0)>(xr + g * (1 << W), xi + g * (1 << W), srad, p);
       if constexpr (PF > 0) {
         const ulonglong2* tw = tab + A.L.off_fwd[0] + Lw;
 #pragma unroll
@@ -569,6 +593,10 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
           xr[v] = shoup_mul(xr[v], w.x, w.y, p);
           xi[v] = shoup_mul(xi[v], w.x, w.y, p);
         }
+      }
+      if constexpr (C::NP > 1) {  // written by the lazy pass 1
+        xr[0] = red2p(xr[0], p);
+        xi[0] = red2p(xi[0], p);
       }
       dit_regs<W, LOGR>(xr, xi, srad, p);
 #pragma unroll

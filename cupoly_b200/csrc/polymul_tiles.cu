@@ -72,7 +72,7 @@ __device__ __noinline__ void tile_fwd_mid(ulonglong2* sdat, const ulonglong2* sr
       xr[v] = x.x;
       xi[v] = x.y;
     }
-    dif_regs<kTileLogR, kTileLogR>(xr, xi, srad, p);
+    dif_regs<kTileLogR, kTileLogR, true>(xr, xi, srad, p);
     const ulonglong2* tw = tab + L.off_fwd[I] + Lw;
 #pragma unroll
     for (int v = 1; v < R; ++v) {
@@ -112,7 +112,9 @@ __device__ __noinline__ void tile_inv_mid(ulonglong2* sdat, const ulonglong2* sr
         xi[v] = shoup_mul(xi[v], w.x, w.y, p);
       }
     }
-    dit_regs<kTileLogR, kTileLogR>(xr, xi, srad, p);
+    xr[0] = red2p(xr[0], p);  // written by a lazy pass
+    xi[0] = red2p(xi[0], p);
+    dit_regs<kTileLogR, kTileLogR, true>(xr, xi, srad, p);
 #pragma unroll
     for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
     __syncthreads();
@@ -144,7 +146,8 @@ __device__ __noinline__ void tile_fwd_first(ulonglong2* sdat, const ulonglong2* 
       xr[v] = ar;
       xi[v] = ai;
     }
-    dif_regs<W, kTileLogR>(xr, xi, srad, p);
+    static_assert(PF > 0, "the first pass is followed by its twiddles");
+    dif_regs<W, kTileLogR, true>(xr, xi, srad, p);
     const ulonglong2* tw = tab + L.off_fwd[0] + Lw;
 #pragma unroll
     for (int v = 1; v < (1 << W); ++v) {
@@ -198,7 +201,7 @@ __device__ __noinline__ void tile_last_b(ulonglong2* sdat, const ulonglong2* sra
     xr[v] = cr;
     xi[v] = ci;
   }
-  dit_regs<kTileLogR, kTileLogR>(xr, xi, srad, m.p);
+  dit_regs<kTileLogR, kTileLogR, true>(xr, xi, srad, m.p);  // the next inverse pass reduces
   // each thread rewrites only the positions it read
 #pragma unroll
   for (int v = 0; v < R; ++v) sdat[pad16(c * R + v)] = make_ulonglong2(xr[v], xi[v]);
@@ -228,6 +231,8 @@ __device__ __noinline__ void tile_inv_last(const ulonglong2* sdat, const ulonglo
       xr[v] = shoup_mul(xr[v], w.x, w.y, p);
       xi[v] = shoup_mul(xi[v], w.x, w.y, p);
     }
+    xr[0] = red2p(xr[0], p);  // written by a lazy pass
+    xi[0] = red2p(xi[0], p);
     dit_regs<W, kTileLogR>(xr, xi, srad, p);
     if (live) {
 #pragma unroll
