@@ -250,8 +250,9 @@ int cp_poly_complex_scaling_tdivq(const cp_engine* e, void* out_q, void* in_q, v
                                   void* workspace, void* stream);
 int cp_poly_simple_scaling_tdivq(const cp_engine* e, void* out_t, const void* in_q, void* workspace, void* stream);
 
-/* ---- BFV homomorphic multiplication kernel chain (BASELINE configuration 2's
- *      step): (c0, c1, c2) = round(t/Q * (a0 + a1 s)(b0 + b1 s)) in Q, all DGT domain.
+/* ---- BFV homomorphic multiplication kernel chain (basis extension Q -> Q u B, DGT
+ *      tensor product, HPS t/Q scaling back to Q):
+ *      (c0, c1, c2) = round(t/Q * (a0 + a1 s)(b0 + b1 s)) in Q, all DGT domain.
  *      cp_bfv_mul is the plain per-call composition of the calls above, in cuPoly's
  *      order (src/arithmetic/polynomial.cu:350-527, 951-999). ---- */
 int cp_bfv_mul(const cp_engine* e, void* c0, void* c1, void* c2, const void* a0, const void* a1, const void* b0,
