@@ -877,7 +877,7 @@ def run_ours(args, D: Dist):
                          # dram__bytes_read.sum + dram__bytes_write.sum of this launch (same
                          # kernel, 3072 residues of N = 4096) from one ncu capture; writes read low
                          # because dirty lines are still in L2 when the kernel ends
-                         "traffic": 347860480 if (e.N == 4096 and 4 * P * K_B == 3072) else None,
+                         "traffic": 362286592 if (e.N == 4096 and 4 * P * K_B == 3072) else None,
                          "traffic_source": "ncu capture",
                          "kernel": "k_dgt_fwd (forward DGT, %d residues of N=%d per launch, timed alone)" %
                                    (4 * P * K_B, e.N),
