@@ -60,6 +60,7 @@ def test_null_engine_calls_fail_cleanly():
     assert L.cp_dot(None, None, None, None, 1, 0, None) == 1
     assert L.cp_dot_batch(None, None, None, None, 1, 1, 0, 0, None) == 1
     assert L.cp_engine_set_narrow_plan(None, 2, 10, 96) == 1
+    assert L.cp_engine_set_hps_force_exact(None, 1) == 1
     assert L.cp_engine_check_async(None, None, None) == 1
     assert L.cp_engine_get_narrow_plan(None, None, None, None) == 1
     assert L.cp_engine_n_residues(None, 0) == -1
@@ -99,3 +100,35 @@ def test_engine_create_reports_a_failed_device_allocation():
         rc = L.cp_engine_create(C.byref(h), 2, 3, 4096, 256, 0)
         assert rc == 4 and not h.value
         assert "cudaMalloc failed for engine tables" in L.cp_last_error().decode()
+
+
+def test_engine_wrapper_checks_buffers_before_the_abi():
+    """Every device pointer the Engine wrapper passes is checked first: a host tensor, a
+    non-int64 tensor or a non-tensor is refused without a CUDA call."""
+    import torch
+
+    from cupoly_b200.engine import Engine
+    e = Engine.__new__(Engine)  # no device needed for the checks below
+    e.k, e.kl, e.N, e.device = 5, 6, 4096, 0
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        e._buf(torch.zeros((1, 5, 4096, 2), dtype=torch.int64), 0, 1, "a")
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        e._buf(torch.zeros((1, 5, 4096, 2), dtype=torch.int32), 0, 1, "a")
+    with pytest.raises(TypeError):
+        e._buf([0] * 10, 0, 1, "a")
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        e._ws(torch.zeros(16, dtype=torch.int64), 128)
+
+
+def test_per_call_timing_program_is_built_and_checks_its_arguments():
+    """build() links cupoly_percall (the C++ layer timed per call, run by bench.py); with bad
+    arguments it prints its usage and exits 2 before touching a GPU."""
+    import subprocess
+
+    from cupoly_b200 import build as B
+    B.build_percall()
+    r = subprocess.run([B.PERCALL], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "usage" in r.stderr
+    r = subprocess.run([B.PERCALL, "0", "1", "4096", "10"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "bad arguments" in r.stderr
+
