@@ -730,7 +730,12 @@ def run_ours(args, D: Dist):
              "polymul_per_s": round(1024 / (mixed_ms / 1e3), 1), "ms_per_batch": round(mixed_ms, 3),
              "ms_per_batch_by_form": {k_: round(v_, 4) for k_, v_ in mixed_forms.items()},
              "launches_by_form": mixed_launches,
-             "algorithmic_GB_per_s": round(mixed_bytes / (mixed_ms / 1e3) / 1e9, 1)}
+             "algorithmic_GB_per_s": round(mixed_bytes / (mixed_ms / 1e3) / 1e9, 1),
+             "frac_hbm": round(mixed_bytes / (mixed_ms / 1e3) / 1e9 / hbm_peak, 4),
+             "busier_pipe_frac": {"sequence": INT_COUNTERS["kernels"]["k_dgt_inv<11,3,0> products on load"][
+                                      "busier_pipe_frac"],
+                                  "tiles": INT_COUNTERS["kernels"]["k_polymul_tiles"]["busier_pipe_frac"],
+                                  "source": "ncu capture (sequence: the fused polymul's kernels at nphi 4096)"}}
     torch.cuda.empty_cache()
 
     # ---- north-star configuration: nphi = 16384 (N = 2^14 coefficients), |Q| = 10, batched vs plain ----
@@ -866,6 +871,8 @@ def run_ours(args, D: Dist):
             "batched_over_plain": round(value / D.world / plain_value, 2),
             "polymul": ({"value": round(polymul_value, 1), "unit": "polymul/s",
                          "config": "nphi=4096, k=2, batch 1024 (fused: 2 forward DGTs, inverse with products on load), 2 batches in flight",
+                         "algorithmic_GB_per_s": round(polymul_value * 24 * 4096 * 2 / 1e9, 1),
+                         "frac_hbm": round(polymul_value * 24 * 4096 * 2 / 1e9 / hbm_peak, 4),
                          "plain_value": round(polymul_plain_value, 1),
                          "plain_form": "one product per call sequence from Python (2 forward DGTs in place, "
                                        "multiply, inverse DGT; 4 calls)"}
