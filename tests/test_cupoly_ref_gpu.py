@@ -228,3 +228,34 @@ def test_live_cupoly_driver_on_fresh_inputs(gpu, k, nphi):
     ob = e.empty(1)
     e.poly_basis_extension_q_to_b(ob, a)
     assert np.array_equal(_coeffs(e, ob, 1)[0].reshape(-1), ref["ext"])
+
+
+@pytest.mark.skipif(not os.path.exists(DRIVER), reason="cuPoly's sources were not compiled here")
+def test_live_cupoly_bfv_chain_on_fresh_inputs(gpu):
+    """cuPoly's own BFV multiplication chain, run now on fresh inputs at nphi 8192, k 5, kl 6:
+    the batched chain of this library gives the exact product, and cuPoly's words are its
+    restated float chain (each difference one of its rounding errors)."""
+    from tests.golden.gen_cupoly_golden import inputs
+    from cupoly_b200.engine import INVERSE, QBase, from_u64, to_u64
+    k, kl, nphi, t = 5, 6, 8192, 256
+    x = inputs("bfvmul", k, kl, nphi, 9901)
+    with tempfile.TemporaryDirectory() as d:
+        x.tofile(os.path.join(d, "in"))
+        subprocess.run([DRIVER, "bfvmul", str(k), str(kl), str(nphi), str(t), os.path.join(d, "in"),
+                        os.path.join(d, "out")], check=True, timeout=300)
+        ref = np.fromfile(os.path.join(d, "out"), dtype=np.uint64).reshape(3, k, nphi)
+    e = _engine(k, kl, nphi, t)
+    rows = x.reshape(4, k, nphi)
+    dev = [_to_dgt(e, rows[i], 0) for i in range(4)]
+    c = e.empty(QBase, 3)
+    e.bfv_mul_batch(c, *dev, 1, e.bfv_mul_batch_workspace(1))
+    e.dgt(c, QBase, INVERSE)
+    got = unfold(to_u64(c)).reshape(3, k, nphi)
+    exact = CO.bfv_mul(*[rows[i][None] for i in range(4)], e.Q, e.B, t)
+    for j in range(3):
+        assert np.array_equal(got[j], exact[j][0])
+    if not np.array_equal(got, ref):
+        restated = cupoly_chain_restated(rows, e.Q, e.B, t)
+        assert np.array_equal(restated, ref)
+        for j in range(3):
+            _only_rounding_differences(got[j], exact[j][0], restated[j], e.Q)
