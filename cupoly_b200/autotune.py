@@ -14,7 +14,10 @@ distributed shared memory; cp_engine_set_split_mode); the cluster form is cached
 with the plan only when it is more than 2 % faster.  `best_narrow_plan(nphi, wide)`
 then picks a second plan for small launches (cp_engine_set_narrow_plan): the
 candidate fastest at 16 residue transforms per launch, and the largest launch
-size at which it still beats the main plan.  Engines created with log_radix = 0
+size at which it still beats the main plan.  The RNS width k enters the choice
+through the launch size: a launch transforms polynomials x k residues, and that
+count selects the main or the small-launch plan at run time, so the plan in use is
+a function of (nphi, k, batch).  Engines created with log_radix = 0
 from Python use the cached plans when they exist and the library default
 (radix 8, c = 13, split kernel, no small-launch plan) otherwise.
 """

@@ -52,6 +52,14 @@ struct Tile {
   int count;  // rows in the tile, 1 .. 8192 / N
 };
 
+// Barrier of the T threads that transform one residue of a tile (named barrier `id`,
+// 1 + the residue's index in the tile).  The residues of a tile are independent, so
+// their thread groups run their passes out of step with each other, as separate
+// CTAs would; only the end of a tile synchronises the whole CTA.
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 // Forward passes I .. NP - 2 of one residue in shared memory (no staged tables:
 // the pass twiddles are read through the read-only cache); thread c of the
 // residue's T threads.
@@ -59,7 +67,7 @@ struct Tile {
 // compiler keeps addresses of every pass live across all of them and spills.
 template <int LOGN, int I>
 __device__ __noinline__ void tile_fwd_mid(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* tab,
-                                             const DgtTableLayout& L, uint64_t p, int c) {
+                                             const DgtTableLayout& L, uint64_t p, int c, int gb) {
   using C = PassCfg<LOGN, kTileLogR>;
   if constexpr (I < C::NP - 1) {
     constexpr int PF = C::field(I), R = 1 << kTileLogR;
@@ -82,15 +90,19 @@ __device__ __noinline__ void tile_fwd_mid(ulonglong2* sdat, const ulonglong2* sr
     }
 #pragma unroll
     for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
-    __syncthreads();
-    tile_fwd_mid<LOGN, I + 1>(sdat, srad, tab, L, p, c);
+    // the next pass reads what the 2^PF threads sharing c >> PF wrote
+    if constexpr ((1 << PF) <= 32)
+      __syncwarp();
+    else
+      group_sync(gb, (1 << LOGN) >> kTileLogR);
+    tile_fwd_mid<LOGN, I + 1>(sdat, srad, tab, L, p, c, gb);
   }
 }
 
 // Inverse passes I .. 1 in shared memory.
 template <int LOGN, int I>
 __device__ __noinline__ void tile_inv_mid(ulonglong2* sdat, const ulonglong2* srad, const ulonglong2* tab,
-                                             const DgtTableLayout& L, uint64_t p, int c) {
+                                             const DgtTableLayout& L, uint64_t p, int c, int gb) {
   using C = PassCfg<LOGN, kTileLogR>;
   if constexpr (I >= 1) {
     constexpr int PF = C::field(I), R = 1 << kTileLogR;
@@ -117,8 +129,8 @@ __device__ __noinline__ void tile_inv_mid(ulonglong2* sdat, const ulonglong2* sr
     dit_regs<kTileLogR, kTileLogR, true>(xr, xi, srad, p);
 #pragma unroll
     for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
-    __syncthreads();
-    tile_inv_mid<LOGN, I - 1>(sdat, srad, tab, L, p, c);
+    group_sync(gb, (1 << LOGN) >> kTileLogR);
+    tile_inv_mid<LOGN, I - 1>(sdat, srad, tab, L, p, c, gb);
   }
 }
 
@@ -126,7 +138,7 @@ __device__ __noinline__ void tile_inv_mid(ulonglong2* sdat, const ulonglong2* sr
 template <int LOGN>
 __device__ __noinline__ void tile_fwd_first(ulonglong2* sdat, const ulonglong2* xs, const ulonglong2* srad,
                                                const ulonglong2* tab, const DgtTableLayout& L, uint64_t p, int c,
-                                               bool live) {
+                                               bool live, int gb) {
   using C = PassCfg<LOGN, kTileLogR>;
   constexpr int T = (1 << LOGN) >> kTileLogR, W = C::W0, PF = LOGN - C::W0, G = 1 << (kTileLogR - C::W0);
   uint64_t xr[1 << W], xi[1 << W];
@@ -158,7 +170,7 @@ __device__ __noinline__ void tile_fwd_first(ulonglong2* sdat, const ulonglong2* 
 #pragma unroll
     for (int v = 0; v < (1 << W); ++v) sdat[pad16(Lw + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
   }
-  __syncthreads();
+  group_sync(gb, T);
 }
 
 // Last forward pass of a (lowest index bits, positions c R + v): to the slot.
@@ -255,7 +267,12 @@ __device__ __forceinline__ void tile_polymul(const TileGroup& G, int row0, int c
   static_assert(C::NP >= 3, "at least one middle pass");
   const int u = threadIdx.x / T, c = threadIdx.x % T;
   const bool live = u < count;
-  const int row = row0 + (live ? u : 0);
+  const int gb = 1 + u;  // this residue's named barrier
+  if (!live) {  // a residue slot the tile does not fill: nothing to wait for but the tile's end
+    __syncthreads();
+    return;
+  }
+  const int row = row0 + u;
   const int rid = G.rid[row];
   const uint64_t p = G.A.mc[rid].p;
   const ulonglong2* tab = G.A.tab + (size_t)rid * G.A.stride;
@@ -263,24 +280,24 @@ __device__ __forceinline__ void tile_polymul(const TileGroup& G, int row0, int c
   ulonglong2* sdat = smem + u * (N + (N >> 4));
   ulonglong2* srad = smem + kTileElems + (kTileElems >> 4) + u * R;
   if (c < R) srad[c] = tab[L.off_rad + c];
-  __syncthreads();
+  group_sync(gb, T);
   const size_t off = (size_t)row * N;
   // element v of thread c (position c R + v of the last pass) at my[v T]
   ulonglong2* my = slot + (size_t)u * N + c;
 
   // 1. a: forward transform; its last pass's registers to the slot
-  tile_fwd_first<LOGN>(sdat, G.a + off, srad, tab, L, p, c, live);
-  tile_fwd_mid<LOGN, 1>(sdat, srad, tab, L, p, c);
+  tile_fwd_first<LOGN>(sdat, G.a + off, srad, tab, L, p, c, true, gb);
+  tile_fwd_mid<LOGN, 1>(sdat, srad, tab, L, p, c, gb);
   tile_last_a<LOGN>(sdat, srad, p, c, my);
-  __syncthreads();  // shared memory is reused for b
+  group_sync(gb, T);  // the residue's shared memory is reused for b
   // 2. b: forward transform, product, the inverse's first pass
-  tile_fwd_first<LOGN>(sdat, G.b + off, srad, tab, L, p, c, live);
-  tile_fwd_mid<LOGN, 1>(sdat, srad, tab, L, p, c);
+  tile_fwd_first<LOGN>(sdat, G.b + off, srad, tab, L, p, c, true, gb);
+  tile_fwd_mid<LOGN, 1>(sdat, srad, tab, L, p, c, gb);
   tile_last_b<LOGN>(sdat, srad, G.A.mc + rid, c, my);
-  __syncthreads();
+  __syncwarp();  // the next inverse pass (field 3) reads what the 8 threads sharing c >> 3 wrote
   // 3. the remaining inverse passes, untwist, c to HBM
-  tile_inv_mid<LOGN, C::NP - 2>(sdat, srad, tab, L, p, c);
-  tile_inv_last<LOGN>(sdat, srad, tab, L, p, c, live, G.c + off);
+  tile_inv_mid<LOGN, C::NP - 2>(sdat, srad, tab, L, p, c, gb);
+  tile_inv_last<LOGN>(sdat, srad, tab, L, p, c, true, G.c + off);
   __syncthreads();  // shared memory is rewritten by the next tile
 }
 
