@@ -60,6 +60,40 @@ __device__ __forceinline__ void group_sync(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
+// Threads per named-barrier group of the transition of field f (at least 128, so that a
+// tile's groups fit the 15 ids).
+constexpr int tile_group(int f) { return (1 << f) > 128 ? (1 << f) : 128; }
+
+// First id of the transition of field f in a tile of residues of 2^LOGN elements: after
+// the residues' own ids 1 .. 8192 / N and the ids of every larger field f + 3, f + 6, ...
+template <int LOGN>
+constexpr int tile_bar_base(int f) {
+  constexpr int T = (1 << LOGN) >> kTileLogR;
+  int b = 1 + kTileThreads / T;
+  for (int g = f + kTileLogR; (1 << g) < T; g += kTileLogR)
+    if ((1 << g) > 32 && tile_group(g) < T) b += kTileThreads / tile_group(g);
+  return b;
+}
+
+// Barrier between two passes of one residue whose exchange spans the 2^F threads that
+// share c >> F (F the larger of the two passes' bit fields): a warp barrier when those fit
+// in a warp, the residue's barrier when a group spans the residue, else a named barrier
+// per group.  Each transition has its own ids, so a thread released early never meets a
+// group of another transition at the same id.
+template <int LOGN, int F>
+__device__ __forceinline__ void tile_pass_sync(int gb) {
+  constexpr int T = (1 << LOGN) >> kTileLogR, G = tile_group(F);
+  if constexpr ((1 << F) <= 32) {
+    __syncwarp();
+  } else if constexpr (G >= T) {
+    group_sync(gb, T);
+  } else {
+    constexpr int B = tile_bar_base<LOGN>(F);
+    static_assert(B + kTileThreads / G - 1 <= 15, "named barrier ids 1..15");
+    group_sync(B + (int)threadIdx.x / G, G);
+  }
+}
+
 // Forward passes I .. NP - 2 of one residue in shared memory (no staged tables:
 // the pass twiddles are read through the read-only cache); thread c of the
 // residue's T threads.
@@ -90,11 +124,7 @@ __device__ __noinline__ void tile_fwd_mid(ulonglong2* sdat, const ulonglong2* sr
     }
 #pragma unroll
     for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
-    // the next pass reads what the 2^PF threads sharing c >> PF wrote
-    if constexpr ((1 << PF) <= 32)
-      __syncwarp();
-    else
-      group_sync(gb, (1 << LOGN) >> kTileLogR);
+    tile_pass_sync<LOGN, PF>(gb);  // the next pass reads what the threads sharing c >> PF wrote
     tile_fwd_mid<LOGN, I + 1>(sdat, srad, tab, L, p, c, gb);
   }
 }
@@ -129,7 +159,7 @@ __device__ __noinline__ void tile_inv_mid(ulonglong2* sdat, const ulonglong2* sr
     dit_regs<kTileLogR, kTileLogR, true>(xr, xi, srad, p);
 #pragma unroll
     for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
-    group_sync(gb, (1 << LOGN) >> kTileLogR);
+    tile_pass_sync<LOGN, C::field(I - 1)>(gb);  // the next pass reads across c >> field(I - 1)
     tile_inv_mid<LOGN, I - 1>(sdat, srad, tab, L, p, c, gb);
   }
 }
