@@ -420,7 +420,7 @@ INT_COUNTERS = {
                                                "fmaheavy_pct": 71.6, "alu_pct": 56.5, "issue_pct": 59.9,
                                                "busier_pipe_frac": 0.716},
         "k_polymul_tiles": {"workload": "mixed batch of 1024 products, one launch",
-                            "fmaheavy_pct": 60.3, "alu_pct": 45.9, "issue_pct": 51.0, "busier_pipe_frac": 0.603},
+                            "fmaheavy_pct": 67.0, "alu_pct": 49.6, "issue_pct": 52.3, "busier_pipe_frac": 0.670},
     },
 }
 
@@ -738,7 +738,7 @@ def run_ours(args, D: Dist):
                                   "source": "ncu capture (sequence: the fused polymul's kernels at nphi 4096)"}}
     torch.cuda.empty_cache()
 
-    # ---- north-star configuration: nphi = 16384 (N = 2^14 coefficients), |Q| = 10, batched vs plain ----
+    # ---- target configuration: nphi = 16384 (N = 2^14 coefficients), |Q| = 10, batched vs plain ----
     eT = Engine(10, 11, 16384, T_PLAIN)
     PT, PTp = 32, 4
     insT = []
