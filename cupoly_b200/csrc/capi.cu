@@ -86,14 +86,23 @@ int finish_engine(cp_engine** out, cp_engine* h, int log_radix) {
     }
     e.xi.push_back(canonical_xi(p, e.roots[i], (uint64_t)e.N));
   }
-  e.plan = make_plan(e.logN, log_radix ? log_radix : 3);
-  // Default small-launch plan (N >= 2048): radix 4 over 2^(log N - 2) elements per CTA, the
-  // top 2 bits in the split stage, for launches of at most 96 residue transforms.  On B200 it
-  // took a single BFV multiplication from 133 to 77 us at nphi 8192 and from 277 to 168 us at
-  // nphi 16384.  cp_engine_set_narrow_plan replaces or removes it.
+  // Default main plan, the fastest measured on B200 (forward + inverse of 2048 residues): the
+  // whole transform in one CTA up to N = 4096; from N = 8192 on, the top 2 bits in the split
+  // stage (nphi 16384: 0.969 ms against 1.030 ms whole; nphi 32768: 2.082 against 2.312 ms
+  // with 1 split bit).
+  e.plan = make_plan(e.logN, log_radix ? log_radix : 3, e.logN >= 13 ? e.logN - 2 : kMaxLogNc);
+  // Default small-launch plan: radix 4 over 2^(log N - 2) elements per CTA, the top 2 bits in
+  // the split stage.  Where the main plan keeps more of the transform in one CTA (N = 2048 and
+  // 4096) it takes launches of up to 96 residue transforms: a single BFV multiplication went
+  // from 133 to 77 us at nphi 8192.  At N = 8192, where the main plan has the same split, only
+  // launches of up to 16 (0.027 against 0.031 ms at 16, slower from 96 on); none above.
+  // cp_engine_set_narrow_plan replaces or removes it.
   if (e.logN >= 11 && e.logN - 2 < e.plan.logNc) {
     e.plan_narrow = make_plan(e.logN, 2, e.logN - 2);
     e.narrow_units = 96;
+  } else if (e.logN == 13 && e.plan.logR != 2) {
+    e.plan_narrow = make_plan(e.logN, 2, e.logN - 2);
+    e.narrow_units = 16;
   }
   int rc = build_tables_nothrow(e);
   if (rc) {

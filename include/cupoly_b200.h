@@ -71,7 +71,9 @@ const char* cp_last_error(void);
  *      (cuPoly's M), 4 <= nphi <= 65536 a power of two; kl <= 0 selects k + 1;
  *      any t >= 2 coprime to Q (cuPoly requires a power of two).  The engine is
  *      created on the current CUDA device.  log_radix in {3, 4} picks the DGT
- *      register radix (0 = default). */
+ *      register radix (0 = default).  The default plan keeps the whole transform in
+ *      one CTA up to nphi 8192 and puts the top 2 bits in the split stage from nphi
+ *      16384 on (log_cta = log2(nphi / 2) - 2), the fastest measured on B200. */
 int cp_engine_create(cp_engine** out, int k, int kl, int nphi, uint64_t t, int log_radix);
 /* CKKS-mode engine: replaces CUDAEngine::init(k, kl, M, prec) of cuPoly's CKKS build
  * (src/cuda/cudaengine.cu:1192-1290).  Q = the first 63-bit prime followed by k - 1
@@ -98,8 +100,9 @@ int cp_engine_get_plan(const cp_engine* e, int* log_radix, int* log_cta, int* sp
  * over 2-4 CTAs finishes sooner.  Results are identical.  Same limits as cp_engine_set_plan;
  * the split stage of this plan is always the separate kernel.  Rebuilds the engine's
  * tables (synchronises the device).  The autotuner picks the plan and the crossover.
- * Default for nphi >= 4096: radix 4 (log_radix 2), log_cta = log2(nphi / 2) - 2, up to 96
- * units, when that differs from the main plan.  get: zeros when there is no such plan. */
+ * Default: radix 4 (log_radix 2), log_cta = log2(nphi / 2) - 2, up to 96 units at nphi
+ * 4096 and 8192, up to 16 at nphi 16384, none otherwise.  get: zeros when there is no
+ * such plan. */
 int cp_engine_set_narrow_plan(cp_engine* e, int log_radix, int log_cta, long long max_units);
 int cp_engine_get_narrow_plan(const cp_engine* e, int* log_radix, int* log_cta, long long* max_units);
 /* Form of the split stage of transforms larger than one CTA (plans with split bits > 0; no

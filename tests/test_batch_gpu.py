@@ -258,17 +258,21 @@ def test_small_launch_plan_gives_the_same_bytes(gpu, nphi, k, t, narrow, main):
 
 
 def test_default_and_cached_small_launch_plans(gpu, tmp_path, monkeypatch):
-    """Engines start with the library's small-launch plan (radix 4, 2 split bits, up to 96
-    residue transforms) from nphi 4096 up while the main plan has fewer split bits; a tuned
-    cache entry replaces it, including by none."""
+    """Engines start with the library's small-launch plan (radix 4, 2 split bits: up to 96
+    residue transforms at nphi 4096 and 8192, up to 16 at nphi 16384, none above) and its
+    main plan (2 split bits from nphi 16384 on); a tuned cache entry replaces them,
+    including by none."""
     import json
     monkeypatch.setenv("CUPOLY_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     from cupoly_b200 import autotune
     from cupoly_b200.engine import Engine
-    for nphi, exp in ((2048, 0), (4096, 9), (8192, 10), (16384, 11), (32768, 12), (65536, 0)):
-        got = Engine(1, 1, nphi, 65537 if nphi >= 32768 else 256).get_narrow_plan()
+    for nphi, exp, units, main_cta in ((2048, 0, 0, 10), (4096, 9, 96, 11), (8192, 10, 96, 12),
+                                       (16384, 11, 16, 11), (32768, 0, 0, 12), (65536, 0, 0, 13)):
+        eng = Engine(1, 1, nphi, 65537 if nphi >= 32768 else 256)
+        got = eng.get_narrow_plan()
+        assert (eng.get_plan()["log_radix"], eng.get_plan()["log_cta"]) == (3, main_cta), nphi
         if exp:
-            assert got == {"log_radix": 2, "log_cta": exp, "max_units": 96}, nphi
+            assert got == {"log_radix": 2, "log_cta": exp, "max_units": units}, nphi
         else:
             assert got["max_units"] == 0, nphi
     wide = autotune.best_plan(8192, residues=128, reps=2)
