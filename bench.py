@@ -456,12 +456,14 @@ def cupoly_gpu_times():
 
 def dropin_percall_times():
     """This library's C++ drop-in layer (libcupoly.so, cuPoly's API) per call, the same two
-    call sequences as cupoly_gpu_times on the same sizes: cupoly_b200/host/bench/percall.cpp,
+    call sequences as cupoly_gpu_times on the same sizes, plus the BFV multiplication at
+    nphi 16384, k 10, kl 11 (the batched target's size): cupoly_b200/host/bench/percall.cpp,
     CUDA events on the Context's stream over 200 calls."""
     if not os.path.exists(PERCALL):
         return {"unavailable": "cupoly_b200/lib/cupoly_percall was not built"}
     out = {}
-    for name, (k, nphi) in {"polymul_nphi4096_k2": (2, 4096), "bfv_mul_nphi8192_k5_kl6": (5, 8192)}.items():
+    for name, (k, nphi) in {"polymul_nphi4096_k2": (2, 4096), "bfv_mul_nphi8192_k5_kl6": (5, 8192),
+                            "bfv_mul_nphi16384_k10_kl11": (10, 16384)}.items():
         r = subprocess.run([PERCALL, str(k), str(k + 1), str(nphi), "200"], capture_output=True, text=True,
                            timeout=300)
         if r.returncode != 0:
@@ -878,7 +880,11 @@ def run_ours(args, D: Dist):
                                        "multiply, inverse DGT; 4 calls)"}
                         if polymul_value else None),
             "mixed_polymul": mixed,
-            "target": target,
+            "target": dict(target, **({"plain_cxx_hom_mul_per_s": percall_cxx["bfv_mul_nphi16384_k10_kl11"]["per_s"],
+                                       "batched_over_plain_cxx": round(
+                                           target["batched_hom_mul_per_s"] /
+                                           percall_cxx["bfv_mul_nphi16384_k10_kl11"]["per_s"], 2)}
+                                      if percall_cxx and "bfv_mul_nphi16384_k10_kl11" in percall_cxx else {})),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(achieved / hbm_peak, 4),
                          # dram__bytes_read.sum + dram__bytes_write.sum of this launch (same
