@@ -710,13 +710,13 @@ def run_ours(args, D: Dist):
                 g["a"].random_(0, 1 << 62)
                 g["b"].random_(0, 1 << 62)
             mp.capture(branches=form == "branches")
-        mixed_batches(mps, 2)
+        mixed_batches(mps, 4)
         torch.cuda.synchronize()
-        ev0.record(stream)
-        mixed_batches(mps, 6)
+        ev0.record(stream)  # 40 batches: the steady state of two in flight, not its ramp
+        mixed_batches(mps, 40)
         ev1.record(stream)
         torch.cuda.synchronize()
-        mixed_forms[form] = ev0.elapsed_time(ev1) / 6
+        mixed_forms[form] = ev0.elapsed_time(ev1) / 40
         mixed_launches[form] = mps[0].launches_per_run()
         mixed_bytes = mps[0].algorithmic_bytes()
         del mps, mp
