@@ -854,6 +854,13 @@ def run_ours(args, D: Dist):
         rate, done, el, cores = cpu_bfv_rate(10.0)
         cpu = {"value": round(rate, 3), "unit": "hom-mul/s", "cores": cores, "kind": "port",
                "sample": "%d pairs in %.1f s (nphi=8192, k=5) through oracle/cpoly_oracle.c, OpenMP" % (done, el)}
+        # the same restatement on one core, on the same seeded inputs (one pair per call)
+        from oracle import coracle
+        coracle.set_threads(1)
+        rate1, done1, el1, _ = cpu_bfv_rate(4.0, pairs_per_call=1)
+        coracle.set_threads(cores)
+        cpu["single_core"] = {"value": round(rate1, 3), "unit": "hom-mul/s", "cores": 1,
+                              "sample": "%d pairs in %.1f s, one thread" % (done1, el1)}
 
     if D.rank == 0:
         line = {
