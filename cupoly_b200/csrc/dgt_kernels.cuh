@@ -378,6 +378,15 @@ constexpr int dgt_min_blocks() {
   return b < 1 ? 1 : (b > 16 ? 16 : b);
 }
 
+// Whether a kernel carries the next-unit L2 prefetch: only the configurations with one
+// resident CTA per SM, whose grids the host makes persistent.  Elsewhere the grid is the
+// unit count, the prefetch never fires, and its live values only cost registers (the
+// radix-8, 4096-element forward kernel spilled 28 bytes per thread with it, 4 without).
+template <int LOGNC, int LOGR, int CL>
+constexpr bool dgt_prefetches() {
+  return CL == 0 && dgt_min_blocks<LOGNC, LOGR>() == 1;
+}
+
 // CL > 0: the split stage of 2^CL chunks runs inside the kernel's thread-block
 // cluster (launched with cluster dimension 2^CL, one CTA per unit, S = CL); the
 // input is read untwisted and the twist applied here (cluster_split_fwd).
@@ -393,7 +402,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   ulonglong2* stw = srad + R;
   const int tid = threadIdx.x;
   // Persistent CTAs: unit ub = (poly * nres + r) * 2^S + h, strided by the grid; each
-  // iteration prefetches the next unit's input into L2 while this one is transformed.
+  // iteration of a one-CTA-per-SM configuration prefetches the next unit's input into L2.
   const ulonglong2* in_base = src_base ? src_base : data;  // out of place when src_base is set
   auto unit_off = [&](unsigned ub) {
     const int pr_ = (int)(ub >> S);
@@ -401,7 +410,8 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
            ((size_t)(ub & ((1u << S) - 1)) << LOGNC);
   };
   for (unsigned ub = blockIdx.x; ub < nunits; ub += gridDim.x) {
-  if (tid == 0 && ub + gridDim.x < nunits) prefetch_l2(in_base + unit_off(ub + gridDim.x), NC * 16u);
+  if (dgt_prefetches<LOGNC, LOGR, CL>() && tid == 0 && ub + gridDim.x < nunits)
+    prefetch_l2(in_base + unit_off(ub + gridDim.x), NC * 16u);
   const int pr = (int)(ub >> S);
   const int r = pr % nres;
   const int rid = A.rid_list ? A.rid_list[pr] : rid_off + r;
@@ -512,7 +522,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
     }
   };
   for (unsigned ub = blockIdx.x; ub < nunits; ub += gridDim.x) {
-  if (tid == 0 && ub + gridDim.x < nunits) {  // the next unit's operands into L2
+  if (dgt_prefetches<LOGNC, LOGR, CL>() && tid == 0 && ub + gridDim.x < nunits) {  // the next unit's operands into L2
     int rn, pn;
     coords(ub + gridDim.x, rn, pn);
     const size_t inner_n = ((size_t)rn << (LOGNC + S)) + ((size_t)((ub + gridDim.x) & ((1u << S) - 1)) << LOGNC);
