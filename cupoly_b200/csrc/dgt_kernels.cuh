@@ -474,6 +474,12 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   }
 }
 
+// src.p[i] by selects: indexing the by-value parameter with a run-time i would copy the
+// whole argument to local memory in every thread.
+__device__ __forceinline__ const ulonglong2* inv_src_ptr(const InvSrc& s, int i) {
+  return i == 0 ? s.p[0] : i == 1 ? s.p[1] : i == 2 ? s.p[2] : s.p[3];
+}
+
 __device__ __forceinline__ ulonglong2 tensor_load(const InvSrc& s, int j, size_t off, const ModConst& m) {
   const ulonglong2 a0 = s.p[0][off], a1 = s.p[1][off], b0 = s.p[2][off], b1 = s.p[3][off];
   uint64_t r, i;
@@ -530,7 +536,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
       prefetch_l2(src.p[0] + pn * poly_stride + inner_n, NC * 16u);
       if (src.mode == 3) prefetch_l2(src.p[1] + pn * poly_stride + inner_n, NC * 16u);
     } else if (src.mode == 2) {
-      prefetch_l2(src.p[pn / src.npairs] + (pn % src.npairs) * poly_stride + inner_n, NC * 16u);
+      prefetch_l2(inv_src_ptr(src, pn / src.npairs) + (pn % src.npairs) * poly_stride + inner_n, NC * 16u);
     } else {
       const int jt = pn / src.npairs;
       const size_t bo = (size_t)(pn % src.npairs) * poly_stride + inner_n;
@@ -565,7 +571,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
   } else if (src.mode != 1) {
     const ulonglong2* xs = src.mode == 0
                                ? src.p[0] + poly * poly_stride + inner
-                               : src.p[poly / src.npairs] + (poly % src.npairs) * poly_stride + inner;
+                               : inv_src_ptr(src, poly / src.npairs) + (poly % src.npairs) * poly_stride + inner;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
       const int idx = tid + j * T;
