@@ -23,6 +23,8 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "engine.cuh"
 
 namespace cpoly {
@@ -480,14 +482,18 @@ __device__ __forceinline__ const ulonglong2* inv_src_ptr(const InvSrc& s, int i)
   return i == 0 ? s.p[0] : i == 1 ? s.p[1] : i == 2 ? s.p[2] : s.p[3];
 }
 
+// Element `off` of tensor output j from the operands p = {a0, a1, b0, b1}: c0 = a0 b0,
+// c1 = a0 b1 + a1 b0, c2 = a1 b1.  Only the operands output j uses are loaded.
 __device__ __forceinline__ ulonglong2 tensor_load(const InvSrc& s, int j, size_t off, const ModConst& m) {
-  const ulonglong2 a0 = s.p[0][off], a1 = s.p[1][off], b0 = s.p[2][off], b1 = s.p[3][off];
   uint64_t r, i;
   if (j == 0) {
+    const ulonglong2 a0 = s.p[0][off], b0 = s.p[2][off];
     gi_mul(r, i, a0.x, a0.y, b0.x, b0.y, m);
   } else if (j == 2) {
+    const ulonglong2 a1 = s.p[1][off], b1 = s.p[3][off];
     gi_mul(r, i, a1.x, a1.y, b1.x, b1.y, m);
   } else {
+    const ulonglong2 a0 = s.p[0][off], a1 = s.p[1][off], b0 = s.p[2][off], b1 = s.p[3][off];
     uint64_t r1, i1, r2, i2;
     gi_mul(r1, i1, a0.x, a0.y, b1.x, b1.y, m);
     gi_mul(r2, i2, a1.x, a1.y, b0.x, b0.y, m);
@@ -540,10 +546,10 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
     } else {
       const int jt = pn / src.npairs;
       const size_t bo = (size_t)(pn % src.npairs) * poly_stride + inner_n;
-      if (jt != 2) prefetch_l2(src.p[0] + bo, NC * 16u);
-      if (jt != 0) prefetch_l2(src.p[1] + bo, NC * 16u);
-      if (jt != 2) prefetch_l2(src.p[3] + bo, NC * 16u);
-      if (jt != 0) prefetch_l2(src.p[2] + bo, NC * 16u);
+      if (jt != 2) prefetch_l2(src.p[0] + bo, NC * 16u);  // a0: c0, c1
+      if (jt != 0) prefetch_l2(src.p[1] + bo, NC * 16u);  // a1: c1, c2
+      if (jt != 2) prefetch_l2(src.p[2] + bo, NC * 16u);  // b0: c0, c1
+      if (jt != 0) prefetch_l2(src.p[3] + bo, NC * 16u);  // b1: c1, c2
     }
   }
   const int h = (int)(ub & ((1u << S) - 1));
@@ -581,11 +587,19 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
     const int jt = poly / src.npairs;  // which tensor output
     const size_t base = (size_t)(poly % src.npairs) * poly_stride + inner;
     const ModConst m = A.mc[rid];
+    auto load_all = [&](auto out) {  // the output index as a constant: one loop per output
 #pragma unroll 4
-    for (int j = 0; j < R; ++j) {
-      const int idx = tid + j * T;
-      sdat[pad16(idx)] = tensor_load(src, jt, base + idx, m);
-    }
+      for (int j = 0; j < R; ++j) {
+        const int idx = tid + j * T;
+        sdat[pad16(idx)] = tensor_load(src, decltype(out)::value, base + idx, m);
+      }
+    };
+    if (jt == 0)
+      load_all(std::integral_constant<int, 0>{});
+    else if (jt == 2)
+      load_all(std::integral_constant<int, 2>{});
+    else
+      load_all(std::integral_constant<int, 1>{});
   }
   __syncthreads();
   inv_passes<LOGNC, LOGR, C::NP - 1>(sdat, srad, stw, tab, A.L, p);
