@@ -430,3 +430,42 @@ def test_single_launch_polymul_rejects_other_plans(gpu):
     rc = _lib.lib().cp_polymul_tiles(eng, cc, aa, bb, rr, mt._tile_rows, C.c_void_p(mt.tiles.data_ptr()),
                                      mt.ntiles, C.c_void_p(mt.tile_ws.data_ptr()), mt.tile_ws.numel() * 8, None)
     assert rc == 1 and b"radix-8 plan" in _lib.lib().cp_last_error()
+
+
+def test_persistent_plan_in_the_fused_calls(gpu):
+    """Plan r3/c13 at nphi 16384 keeps each residue whole in one CTA: one CTA of 1024 threads
+    per SM, persistent, walking several units and prefetching the next into L2. Every launch of
+    the batched chain and of the fused polymul below has more units than the GPU has SMs, so the
+    gather, tensor and product-on-load sources all run with CTAs that walk several units. The
+    bytes equal those of the library's default plan (split stage, several CTAs per SM)."""
+    import torch
+
+    from cupoly_b200.engine import QBase, UNIFORM, Engine
+    nphi, k, t, P, PM = 16384, 4, 256, 16, 48
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert min(3 * P * k, PM * k) > sms  # the smallest transform launches of the two calls
+    out = []
+    for plan in ((3, 0), (3, 13)):
+        e = Engine(k, 0, nphi, t, log_radix=3)
+        e.set_narrow_plan(0, 0, 0)
+        if plan[1]:
+            e.set_plan(*plan)
+            assert e.get_plan() == {"log_radix": 3, "log_cta": 13, "split_bits": 0}
+        else:
+            assert e.get_plan()["split_bits"] > 0
+        ins = []
+        for j in range(4):
+            v = e.empty(QBase, P)
+            e.sample(v, QBase, UNIFORM, 21, 16 * j, npolys=P, to_dgt=True)
+            ins.append(v)
+        c3 = e.empty(QBase, 3 * P)
+        e.bfv_mul_batch(c3, *ins, P, e.bfv_mul_batch_workspace(P))
+        a, b, c = e.empty(QBase, PM), e.empty(QBase, PM), e.empty(QBase, PM)
+        e.sample(a, QBase, UNIFORM, 22, 0, npolys=PM, to_dgt=False)
+        e.sample(b, QBase, UNIFORM, 22, PM, npolys=PM, to_dgt=False)
+        e.polymul(c, a, b, QBase, e.polymul_workspace(QBase, PM), PM)
+        torch.cuda.synchronize()
+        out.append((c3.clone(), c.clone()))
+        del e
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1])
