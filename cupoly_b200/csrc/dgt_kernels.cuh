@@ -31,6 +31,14 @@ namespace cpoly {
 
 __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 
+// pad16(b + (v << F)) = pad16(b) + pad_off<F>(v) whenever the bits of v << F are clear in b
+// (the sum is then a bitwise or, and so is its shift right by 4): every unrolled access of a
+// pass addresses shared memory at one per-thread base plus a constant.
+template <int F>
+__host__ __device__ constexpr int pad_off(int v) {
+  return (v << F) + ((v << F) >> 4);
+}
+
 template <int LOGNC, int LOGR>
 struct PassCfg {
   static constexpr int NP = (LOGNC + LOGR - 1) / LOGR;
@@ -177,10 +185,11 @@ __device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* s
     const int c = threadIdx.x;
     const int Lw = c & ((1 << PF) - 1);
     const int base = ((c >> PF) << (PF + LOGR)) + Lw;
+    const int pb = pad16(base);
     uint64_t xr[R], xi[R];
 #pragma unroll
     for (int v = 0; v < R; ++v) {
-      const ulonglong2 a = sdat[pad16(base + (v << PF))];
+      const ulonglong2 a = sdat[pb + pad_off<PF>(v)];
       xr[v] = a.x;
       xi[v] = a.y;
     }
@@ -195,7 +204,7 @@ __device__ __forceinline__ void fwd_passes(ulonglong2* sdat, const ulonglong2* s
       }
     }
 #pragma unroll
-    for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
+    for (int v = 0; v < R; ++v) sdat[pb + pad_off<PF>(v)] = make_ulonglong2(xr[v], xi[v]);
     __syncthreads();
     fwd_passes<LOGNC, LOGR, I + 1>(sdat, srad, stw, tab, L, p);
   }
@@ -462,7 +471,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
       }
 #pragma unroll
       for (int v = 0; v < (1 << W); ++v)
-        sdat[pad16(Lw + (v << PF))] = make_ulonglong2(xr[g * (1 << W) + v], xi[g * (1 << W) + v]);
+        sdat[pad16(Lw) + pad_off<PF>(v)] = make_ulonglong2(xr[g * (1 << W) + v], xi[g * (1 << W) + v]);
     }
     __syncthreads();
   }
@@ -470,7 +479,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
 #pragma unroll
   for (int j = 0; j < R; ++j) {
     const int idx = tid + j * T;
-    x[idx] = sdat[pad16(idx)];
+    x[idx] = sdat[pad16(tid) + pad_off<LOGNC - LOGR>(j)];
   }
   __syncthreads();  // shared memory is rewritten by the next unit
   }
