@@ -406,9 +406,9 @@ INT_COUNTERS = {
     "source": "ncu capture",
     "kernels": {
         "k_dgt_fwd<12,3,0>": {"workload": "forward DGT, nphi 8192, 3072 residues",
-                              "fmaheavy_pct": 69.0, "alu_pct": 51.4, "issue_pct": 55.0, "busier_pipe_frac": 0.690},
+                              "fmaheavy_pct": 69.9, "alu_pct": 51.9, "issue_pct": 54.9, "busier_pipe_frac": 0.699},
         "k_dgt_inv<12,3,0>": {"workload": "inverse DGT, nphi 8192, 3072 residues",
-                              "fmaheavy_pct": 73.5, "alu_pct": 54.7, "issue_pct": 58.0, "busier_pipe_frac": 0.735},
+                              "fmaheavy_pct": 73.8, "alu_pct": 54.6, "issue_pct": 58.0, "busier_pipe_frac": 0.738},
         "k_basis_ext_pre<5>": {"workload": "the chain's Q -> B conversion, 512 polynomials",
                                "fmaheavy_pct": 70.5, "alu_pct": 65.1, "issue_pct": 63.5, "busier_pipe_frac": 0.705},
         "k_complex_scaling_pre<5>": {"workload": "the chain's complex scaling, 384 polynomials",
@@ -897,7 +897,7 @@ def run_ours(args, D: Dist):
                          # dram__bytes_read.sum + dram__bytes_write.sum of this launch (same
                          # kernel, 3072 residues of N = 4096) from one ncu capture; writes read low
                          # because dirty lines are still in L2 when the kernel ends
-                         "traffic": 347079168 if (e.N == 4096 and 4 * P * K_B == 3072) else None,
+                         "traffic": 346929920 if (e.N == 4096 and 4 * P * K_B == 3072) else None,
                          "traffic_source": "ncu capture",
                          "kernel": "k_dgt_fwd (forward DGT, %d residues of N=%d per launch, timed alone)" %
                                    (4 * P * K_B, e.N),
