@@ -581,7 +581,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
       const ulonglong2 a = src.p[0][base + idx], b = src.p[1][base + idx];
       uint64_t cr, ci;
       gi_mul(cr, ci, a.x, a.y, b.x, b.y, m);
-      sdat[pad16(idx)] = make_ulonglong2(cr, ci);
+      sdat[pad16(tid) + pad_off<LOGNC - LOGR>(j)] = make_ulonglong2(cr, ci);
     }
   } else if (src.mode != 1) {
     const ulonglong2* xs = src.mode == 0
@@ -590,7 +590,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
 #pragma unroll
     for (int j = 0; j < R; ++j) {
       const int idx = tid + j * T;
-      sdat[pad16(idx)] = xs[idx];
+      sdat[pad16(tid) + pad_off<LOGNC - LOGR>(j)] = xs[idx];
     }
   } else {
     const int jt = poly / src.npairs;  // which tensor output
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
 #pragma unroll 4
       for (int j = 0; j < R; ++j) {
         const int idx = tid + j * T;
-        sdat[pad16(idx)] = tensor_load(src, decltype(out)::value, base + idx, m);
+        sdat[pad16(tid) + pad_off<LOGNC - LOGR>(j)] = tensor_load(src, decltype(out)::value, base + idx, m);
       }
     };
     if (jt == 0)
@@ -620,7 +620,7 @@ __global__ void __launch_bounds__((1 << LOGNC) >> LOGR, (dgt_min_blocks<LOGNC, L
       const int Lw = tid + g * T;
 #pragma unroll
       for (int v = 0; v < (1 << W); ++v) {
-        const ulonglong2 a = sdat[pad16(Lw + (v << PF))];
+        const ulonglong2 a = sdat[pad16(Lw) + pad_off<PF>(v)];
         xr[v] = a.x;
         xi[v] = a.y;
       }
