@@ -107,10 +107,11 @@ __device__ __noinline__ void tile_fwd_mid(ulonglong2* sdat, const ulonglong2* sr
     constexpr int PF = C::field(I), R = 1 << kTileLogR;
     const int Lw = c & ((1 << PF) - 1);
     const int base = ((c >> PF) << (PF + kTileLogR)) + Lw;
+    const int pb = pad16(base);
     uint64_t xr[R], xi[R];
 #pragma unroll
     for (int v = 0; v < R; ++v) {
-      const ulonglong2 x = sdat[pad16(base + (v << PF))];
+      const ulonglong2 x = sdat[pb + pad_off<PF>(v)];
       xr[v] = x.x;
       xi[v] = x.y;
     }
@@ -123,7 +124,7 @@ __device__ __noinline__ void tile_fwd_mid(ulonglong2* sdat, const ulonglong2* sr
       xi[v] = shoup_mul(xi[v], w.x, w.y, p);
     }
 #pragma unroll
-    for (int v = 0; v < R; ++v) sdat[pad16(base + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
+    for (int v = 0; v < R; ++v) sdat[pb + pad_off<PF>(v)] = make_ulonglong2(xr[v], xi[v]);
     tile_pass_sync<LOGN, PF>(gb);  // the next pass reads what the threads sharing c >> PF wrote
     tile_fwd_mid<LOGN, I + 1>(sdat, srad, tab, L, p, c, gb);
   }
@@ -198,7 +199,7 @@ __device__ __noinline__ void tile_fwd_first(ulonglong2* sdat, const ulonglong2* 
       xi[v] = shoup_mul(xi[v], w.x, w.y, p);
     }
 #pragma unroll
-    for (int v = 0; v < (1 << W); ++v) sdat[pad16(Lw + (v << PF))] = make_ulonglong2(xr[v], xi[v]);
+    for (int v = 0; v < (1 << W); ++v) sdat[pad16(Lw) + pad_off<PF>(v)] = make_ulonglong2(xr[v], xi[v]);
   }
   group_sync(gb, T);
 }
@@ -211,7 +212,7 @@ __device__ __noinline__ void tile_last_a(const ulonglong2* sdat, const ulonglong
   uint64_t xr[R], xi[R];
 #pragma unroll
   for (int v = 0; v < R; ++v) {
-    const ulonglong2 x = sdat[pad16(c * R + v)];
+    const ulonglong2 x = sdat[pad16(c * R) + v];
     xr[v] = x.x;
     xi[v] = x.y;
   }
@@ -230,7 +231,7 @@ __device__ __noinline__ void tile_last_b(ulonglong2* sdat, const ulonglong2* sra
   uint64_t xr[R], xi[R];
 #pragma unroll
   for (int v = 0; v < R; ++v) {
-    const ulonglong2 x = sdat[pad16(c * R + v)];
+    const ulonglong2 x = sdat[pad16(c * R) + v];
     xr[v] = x.x;
     xi[v] = x.y;
   }
@@ -246,7 +247,7 @@ __device__ __noinline__ void tile_last_b(ulonglong2* sdat, const ulonglong2* sra
   dit_regs<kTileLogR, kTileLogR, true>(xr, xi, srad, m.p);  // the next inverse pass reduces
   // each thread rewrites only the positions it read
 #pragma unroll
-  for (int v = 0; v < R; ++v) sdat[pad16(c * R + v)] = make_ulonglong2(xr[v], xi[v]);
+  for (int v = 0; v < R; ++v) sdat[pad16(c * R) + v] = make_ulonglong2(xr[v], xi[v]);
 }
 
 // Inverse pass 0 (the top W0 bits), untwist with N^-1, c to HBM.
@@ -262,7 +263,7 @@ __device__ __noinline__ void tile_inv_last(const ulonglong2* sdat, const ulonglo
     const int Lw = c + g * T;
 #pragma unroll
     for (int v = 0; v < (1 << W); ++v) {
-      const ulonglong2 x = sdat[pad16(Lw + (v << PF))];
+      const ulonglong2 x = sdat[pad16(Lw) + pad_off<PF>(v)];
       xr[v] = x.x;
       xi[v] = x.y;
     }
