@@ -408,7 +408,7 @@ INT_COUNTERS = {
         "k_dgt_fwd<12,3,0>": {"workload": "forward DGT, nphi 8192, 3072 residues",
                               "fmaheavy_pct": 69.9, "alu_pct": 51.9, "issue_pct": 54.9, "busier_pipe_frac": 0.699},
         "k_dgt_inv<12,3,0>": {"workload": "inverse DGT, nphi 8192, 3072 residues",
-                              "fmaheavy_pct": 73.8, "alu_pct": 54.6, "issue_pct": 58.0, "busier_pipe_frac": 0.738},
+                              "fmaheavy_pct": 74.0, "alu_pct": 54.5, "issue_pct": 58.1, "busier_pipe_frac": 0.740},
         "k_basis_ext_pre<5>": {"workload": "the chain's Q -> B conversion, 512 polynomials",
                                "fmaheavy_pct": 70.5, "alu_pct": 65.1, "issue_pct": 63.5, "busier_pipe_frac": 0.705},
         "k_complex_scaling_pre<5>": {"workload": "the chain's complex scaling, 384 polynomials",
@@ -417,10 +417,10 @@ INT_COUNTERS = {
         "k_basis_ext_pre<6>": {"workload": "the chain's B -> Q conversion, 384 polynomials",
                                "fmaheavy_pct": 67.8, "alu_pct": 64.4, "issue_pct": 62.1, "busier_pipe_frac": 0.678},
         "k_dgt_inv<11,3,0> products on load": {"workload": "fused polymul, nphi 4096, k 2, 2048 products",
-                                               "fmaheavy_pct": 71.6, "alu_pct": 56.5, "issue_pct": 59.9,
-                                               "busier_pipe_frac": 0.716},
+                                               "fmaheavy_pct": 74.7, "alu_pct": 58.3, "issue_pct": 60.1,
+                                               "busier_pipe_frac": 0.747},
         "k_polymul_tiles": {"workload": "mixed batch of 1024 products, one launch",
-                            "fmaheavy_pct": 67.0, "alu_pct": 49.6, "issue_pct": 52.3, "busier_pipe_frac": 0.670},
+                            "fmaheavy_pct": 67.7, "alu_pct": 49.8, "issue_pct": 52.6, "busier_pipe_frac": 0.677},
     },
 }
 
